@@ -1,0 +1,115 @@
+"""Seeded synthetic RGB24 video (ctypes binding of ``synth/synth.c``).
+
+The generator stands in for the lossless rawvideo/ffv1 inputs of the
+benchmark workloads; every frame is a pure function of (params, index).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _build
+
+MAX_DISCS = 4
+
+
+class _Params(C.Structure):
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("fps", C.c_float),
+                ("seed", C.c_uint64), ("n_discs", C.c_int),
+                ("disc_freq", C.c_float * MAX_DISCS), ("disc_amp", C.c_float * MAX_DISCS),
+                ("disc_radius", C.c_float), ("noise_sigma", C.c_float),
+                ("flicker_amp", C.c_float), ("flicker_freq", C.c_float)]
+
+
+@dataclass
+class SynthSpec:
+    width: int
+    height: int
+    fps: float = 30.0
+    seed: int = 1
+    disc_freq: list = field(default_factory=lambda: [1.2])
+    disc_amp: list = field(default_factory=lambda: [0.3])
+    disc_radius: float = 30.0
+    noise_sigma: float = 2.0
+    flicker_amp: float = 0.0
+    flicker_freq: float = 0.1
+
+
+_lib = None
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        path = _build.synth_lib_path()
+        if not os.path.exists(path):
+            _build.build_synth()
+        L = C.CDLL(path)
+        L.synth_new.argtypes = [C.POINTER(_Params)]
+        L.synth_new.restype = C.c_void_p
+        L.synth_free.argtypes = [C.c_void_p]
+        L.synth_frame.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.synth_frames.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        _lib = L
+    return _lib
+
+
+class SynthVideo:
+    def __init__(self, spec: SynthSpec):
+        if len(spec.disc_freq) != len(spec.disc_amp) or len(spec.disc_freq) > MAX_DISCS:
+            raise ValueError("disc_freq/disc_amp must have equal length <= 4")
+        self.spec = spec
+        p = _Params()
+        p.width, p.height, p.fps, p.seed = spec.width, spec.height, spec.fps, spec.seed
+        p.n_discs = len(spec.disc_freq)
+        for i, (f, a) in enumerate(zip(spec.disc_freq, spec.disc_amp)):
+            p.disc_freq[i], p.disc_amp[i] = f, a
+        p.disc_radius, p.noise_sigma = spec.disc_radius, spec.noise_sigma
+        p.flicker_amp, p.flicker_freq = spec.flicker_amp, spec.flicker_freq
+        self._lib = _load()
+        self._h = self._lib.synth_new(C.byref(p))
+        if not self._h:
+            raise ValueError("invalid synthetic video parameters")
+
+    def frames(self, t0: int, count: int, out: np.ndarray | None = None) -> np.ndarray:
+        s = self.spec
+        if out is None:
+            out = np.empty((count, s.height, s.width, 3), np.uint8)
+        assert out.dtype == np.uint8 and out.flags.c_contiguous and out.size == count * s.height * s.width * 3
+        self._lib.synth_frames(self._h, t0, count, out.ctypes.data)
+        return out
+
+    def frame(self, t: int) -> np.ndarray:
+        return self.frames(t, 1)[0]
+
+    def close(self):
+        if self._h:
+            self._lib.synth_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# --- the benchmark workloads' generators -----------------------------------
+
+def plain_qvga(seed: int = 1) -> SynthSpec:
+    """320x240 @30, one disc 1.2 Hz / 0.3 px, noise 2 LSB."""
+    return SynthSpec(320, 240, 30.0, seed, [1.2], [0.3], 30.0, 2.0)
+
+
+def plain_fullhd(seed: int = 2) -> SynthSpec:
+    """1920x1080 @30, discs 0.8/1.5/2.5 Hz (0.2-0.5 px), +-1 LSB flicker 0.1 Hz."""
+    return SynthSpec(1920, 1080, 30.0, seed, [0.8, 1.5, 2.5], [0.5, 0.35, 0.2], 30.0, 2.0,
+                     flicker_amp=1.0, flicker_freq=0.1)
+
+
+def precision_720p(seed: int = 3) -> SynthSpec:
+    """1280x720 @240, one disc 0.4 Hz / 0.15 px, noise 3 LSB."""
+    return SynthSpec(1280, 720, 240.0, seed, [0.4], [0.15], 30.0, 3.0)
