@@ -1,0 +1,376 @@
+"""Benchmark: WEMA per-frame amplification on B200.
+
+Workload (default): one 1920x1080 RGB24 stream at 30 fps - the reference's
+plain full-HD configuration: amp 120, band 0.5-3.0 Hz, colour mode (IIR
+band-pass on Y, Cb and Cr; the reference routes --color through
+wema_process_frame, so bilateral and edge-aware are inert there), FP32.
+Seeded synthetic frames with that configuration's content (three discs at
+0.8/1.5/2.5 Hz, +-1 LSB flicker at 0.1 Hz, 2 LSB noise) stand in for the
+600-frame lossless input file.
+
+A step is one frame of the stream through the whole path (RGB24 in ->
+forward DWT -> exact threshold -> IIR + amplify -> inverse DWT -> RGB24 out).
+* value: Mpix-frames/s with the input frames already resident in HBM,
+  device-timed with CUDA events on the session's stream.
+* e2e:   same through the C ABI from pinned host frames: every step copies
+  its RGB24 frame host->device and the output frame device->host.
+* roofline: the dominant stage's algorithmic bytes per frame over its mean
+  duration (CUDA events around each stage on the launching stream) against
+  the measured HBM copy bandwidth.
+* cpu_baseline: the reference's own C path (compiled from its sources with
+  its Makefile flags, oracle/_ref) on this host, a bounded sample of frames.
+
+Multi-GPU (torchrun): every rank runs an independent stream (replicas; the
+path has no cross-stream exchange), value = all ranks' pixels / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+WORKLOADS = {
+    # name: (synth factory, session kwargs)
+    "plain_fullhd_color": ("plain_fullhd", dict(fps=30.0, amp=120.0, f_low=0.5, f_high=3.0,
+                                                color=True, edge_aware=True, bilateral=True)),
+    "plain_fullhd_luma": ("plain_fullhd", dict(fps=30.0, amp=120.0, f_low=0.5, f_high=3.0,
+                                               color=False, edge_aware=True)),
+    "plain_qvga_luma": ("plain_qvga", dict(fps=30.0, amp=50.0, f_low=0.5, f_high=3.0,
+                                           color=False, edge_aware=True)),
+    "precision_720p_240fps": ("precision_720p", dict(fps=240.0, amp=200.0, f_low=0.2,
+                                                     f_high=0.6, color=False, edge_aware=True)),
+}
+METRIC = "Mpix-frames/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=8)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="plain_fullhd_color", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-frames", type=int, default=12, help="reference frames timed on the host")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def stage_bytes(w, h, channels, levels_dims, pu):
+    """Algorithmic HBM bytes per frame of each stage (each plane read or
+    written once by its stage)."""
+    P = w * h
+    C = channels
+    n0 = levels_dims[0][0] * levels_dims[0][1]
+    fwd0 = 3 * P + C * 4 * 4 * n0                      # RGB24 in; LL + 3 bands out
+    rest = 0
+    for l in range(1, len(levels_dims)):
+        pw, ph = levels_dims[l - 1]
+        sw, sh = levels_dims[l]
+        rest += C * 4 * (pw * ph + 4 * sw * sh)
+    thr = C * 2 * 4 * pu                               # two passes over |x|
+    temporal = C * (4 + 32 + 4) * pu                   # coef in, state in/out, amplified out
+    inv = 0
+    for l in range(len(levels_dims)):
+        sw, sh = levels_dims[l]
+        iw = (w if l == 0 else levels_dims[l - 1][0])
+        ih = (h if l == 0 else levels_dims[l - 1][1])
+        inv += C * 4 * 4 * sw * sh                     # LL + 3 bands in
+        inv += (3 * P if (l == 0 and C == 3) else C * 4 * iw * ih)
+    xfer = 0 if C == 3 else 3 * P + 4 * P + 3 * P      # RGB in, Y in, RGB out
+    return {"fwd_dwt_level0": fwd0, "fwd_dwt_levels": rest, "threshold": thr,
+            "temporal_amplify": temporal, "inv_dwt": inv, "luma_transfer": xfer}
+
+
+def dims_of(w, h):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    L = 0
+    m = min(w, h)
+    while m >= 16 and L < 4:
+        m //= 2
+        L += 1
+    L = max(L, 1)
+    dims = []
+    for _ in range(L):
+        w, h = (w + 1) // 2, (h + 1) // 2
+        dims.append((w, h))
+    return dims
+
+
+def cpu_reference_rate(name, frames_u8, kw, nframes):
+    """The reference's C path on this host: Mpix-frames/s over nframes."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Oracle, Reference
+    O = Oracle()
+    h, w = frames_u8.shape[1:3]
+    cfg = dict(width=w, height=h, fps=kw["fps"], amp=kw["amp"], f_low=kw["f_low"],
+               f_high=kw["f_high"], color=kw.get("color", False),
+               edge_aware=kw.get("edge_aware", True), bilateral=kw.get("bilateral", False))
+    rgb = O.u8_to_float(frames_u8[:nframes])
+    if Reference.available():
+        R = Reference()
+        cores = os.cpu_count() or 1
+        R.set_threads(cores)
+        kind = "reference"
+        if cfg["color"]:
+            s = R.stream(**cfg)
+            cores_used = 1      # wema_process_frame is single-threaded
+            t0 = time.perf_counter()
+            for t in range(nframes):
+                s.process(rgb[t])
+            dt = time.perf_counter() - t0
+        else:
+            s = R.stream(batch_size=nframes, threads=cores, **cfg)
+            cores_used = cores
+            t0 = time.perf_counter()
+            s.batch(rgb)
+            dt = time.perf_counter() - t0
+    else:
+        kind = "port"
+        cores_used = 1
+        s = O.stream(**cfg)
+        t0 = time.perf_counter()
+        for t in range(nframes):
+            s.process(rgb[t])
+        dt = time.perf_counter() - t0
+    value = w * h * nframes / dt / 1e6
+    return {"value": round(value, 4), "unit": METRIC, "cores": cores_used, "kind": kind,
+            "sample": f"{nframes} frames of {name} ({w}x{h}), first-frame preseed included"}
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    synth_name, kw = WORKLOADS[a.workload]
+
+    from wema_b200 import synth as S
+    spec = getattr(S, synth_name)(seed=1 + rank)
+    w, h = spec.width, spec.height
+
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        vid = S.SynthVideo(spec)
+        nf = max(1, a.steps)
+        frames = vid.frames(0, min(nf, 600))
+        r = cpu_reference_rate(a.workload, frames, kw, min(nf, 600))
+        line = {"metric": METRIC, "value": r["value"], "unit": METRIC, "n_gpus": a.gpus,
+                "steps": min(nf, 600), "warmup": 0, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "impl": "reference",
+                "config": {"workload": a.workload, "width": w, "height": h, "fps": kw["fps"]},
+                "cpu_baseline": r,
+                "e2e": {"value": r["value"], "unit": METRIC, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    from wema_b200 import cuda as wc
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    total = a.warmup + 3 * a.steps
+    nuniq = min(600, max(total, 1))
+    host = torch.empty((nuniq, h, w, 3), dtype=torch.uint8).pin_memory()
+    S.SynthVideo(spec).frames(0, nuniq, out=host.numpy())
+    d_frames = host.to(dev)
+    d_out = torch.empty((h, w, 3), dtype=torch.uint8, device=dev)
+    h_out = torch.empty((h, w, 3), dtype=torch.uint8).pin_memory()
+
+    sess = wc.Session(width=w, height=h, device=local, **kw)
+    sess.keep_deltas(False)
+    stream = torch.cuda.ExternalStream  # noqa: F841  (the session has its own stream)
+    t_stream = torch.cuda.Stream(device=dev)
+
+    def frame(i):
+        return d_frames[i % nuniq]
+
+    # warm-up (includes the first frame's IIR preseed)
+    for i in range(a.warmup):
+        sess.process_u8(frame(i), d_out, stream=t_stream)
+    torch.cuda.synchronize(dev)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    # ---- value: inputs resident in HBM
+    k0 = a.warmup
+    barrier()
+    with ClockSampler(local) as clk:
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(t_stream)
+        for i in range(a.steps):
+            sess.process_u8(frame(k0 + i), d_out, stream=t_stream)
+        ev1.record(t_stream)
+        ev1.synchronize()
+        ms = ev0.elapsed_time(ev1)
+    barrier()
+    clocks = clk.summary()
+
+    # ---- per-stage timing pass (same workload, continuing the stream)
+    sess.set_timing(True)
+    k1 = k0 + a.steps
+    for i in range(a.steps):
+        sess.process_u8(frame(k1 + i), d_out, stream=t_stream)
+    stages, nst = sess.stage_times()
+    sess.set_timing(False)
+    torch.cuda.synchronize(dev)
+
+    # ---- e2e through the C ABI from pinned host buffers
+    k2 = k1 + a.steps
+    d_in = torch.empty((h, w, 3), dtype=torch.uint8, device=dev)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(t_stream):
+        e0.record(t_stream)
+        for i in range(a.steps):
+            d_in.copy_(host[(k2 + i) % nuniq], non_blocking=True)
+            sess.process_u8(d_in, d_out, stream=t_stream)
+            h_out.copy_(d_out, non_blocking=True)
+        e1.record(t_stream)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    barrier()
+
+    if dist:
+        t = torch.tensor([ms, e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+
+    pix = w * h
+    value = pix * a.steps * world / (ms * 1e-3) / 1e6
+    e2e = pix * a.steps * world / (e2e_ms * 1e-3) / 1e6
+
+    dims = dims_of(w, h)
+    pu = sum(3 * sw * sh for sw, sh in dims)
+    C = 3 if kw.get("color") else 1
+    sb = stage_bytes(w, h, C, dims, pu)
+    per_frame = {k: v / max(nst, 1) for k, v in stages.items()}
+    dom = max(per_frame, key=per_frame.get)
+    peak, peak_kind = peaks()
+    achieved = sb[dom] / (per_frame[dom] * 1e-3) / 1e9
+    total_bytes = sum(sb.values())
+    total_ms = sum(per_frame.values())
+    launches_per_frame = (len(dims) + 4 + C + len(dims) + (0 if C == 3 else 1))
+
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": METRIC, "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms / a.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": a.workload, "width": w, "height": h, "fps": kw["fps"],
+                   "amp": kw["amp"], "band_hz": [kw["f_low"], kw["f_high"]],
+                   "color": bool(kw.get("color")), "parallelism": f"replicas x{world}",
+                   "l2": "per-frame working set > 126 MB L2 (no flush)"
+                         if total_bytes > 126e6 else "working set fits L2 (no flush)"},
+        "e2e": {"value": round(e2e, 2), "unit": METRIC, "h2d_bytes_per_step": 3 * pix,
+                "d2h_bytes_per_step": 3 * pix},
+        "gpu_launches": launches_per_frame * a.steps,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
+                     "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "peak_source": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": sb[dom]},
+        "pipeline": {"algorithmic_bytes_per_frame": total_bytes,
+                     "stage_ms_per_frame": {k: round(v, 5) for k, v in per_frame.items()},
+                     "frac_of_hbm_roofline": round(total_bytes / (ms / a.steps * 1e-3) / 1e9 / peak, 4)},
+        "clocks": clocks,
+    }
+    if rank == 0 and not a.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_reference_rate(a.workload, host[:a.cpu_frames].numpy(), kw,
+                                                      a.cpu_frames)
+        except Exception as ex:   # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "error": str(ex)[:200]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sess.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

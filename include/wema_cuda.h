@@ -1,0 +1,118 @@
+/*
+ * wema_cuda.h - extensions of libwema_cuda beyond the reference's C API.
+ *
+ * The reference API (dwt.h, iir_filter.h, temporal_filter.h, phase_amp.h,
+ * wema.h) keeps host-memory semantics so existing C11 callers drop in
+ * unchanged.  These entry points expose what the GPU adds: sessions whose
+ * state stays resident in device memory, u8 RGB24 frames on the device (no
+ * float frames over PCIe), explicit CUDA streams, inspection of the
+ * per-frame stages, and the HBM footprint used for admission control.
+ *
+ * All functions return 0 on success and -1 on error (the reference's
+ * convention, wema.c:437-439); wema_cuda_last_error() then describes the
+ * failure.  A session is not thread-safe: one host thread drives it.
+ */
+#ifndef WEMA_CUDA_H
+#define WEMA_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WEMA_CUDA_ABI_VERSION 1
+
+typedef struct wema_cuda_session wema_cuda_session;
+
+/* Threshold evaluation order: the reference's single-frame route computes
+ * (sum/N)*0.2 (wema.c:723), its batch route (0.2/N)*sum (wema_batch.c:276).
+ * They differ in the last bit and so can flip a mask. */
+enum { WEMA_CUDA_THR_SINGLE = 0, WEMA_CUDA_THR_BATCH = 1 };
+
+typedef struct {
+    int   width, height;
+    float fps;
+    float amp_factor;        /* alpha (wema.h WemaContext.amp_factor) */
+    float f_low, f_high;     /* Hz; IIR band, as wema_init */
+    int   temporal_window;   /* window mode: ws (4..256) */
+    int   edge_aware;        /* guided filter (1) or 5-tap Gaussian (0), luma only */
+    int   bilateral_temp;    /* window mode: bilateral weighting */
+    int   color_mode;        /* YCbCr, three pyramids, no luma transfer */
+    int   use_iir;           /* 1: IIR band-pass (default), 0: window ("--haar") mode */
+    int   threshold_form;    /* WEMA_CUDA_THR_SINGLE or WEMA_CUDA_THR_BATCH */
+    int   device;            /* CUDA device ordinal */
+} wema_cuda_config;
+
+/* Fills *cfg with the reference CLI's defaults for a stream of the given
+ * size and rate (main.c:66-75: amp 120, 0.5 Hz .. Nyquist-1e-4, window 32,
+ * edge-aware on, bilateral off, IIR, luma). */
+void wema_cuda_config_default(wema_cuda_config *cfg, int width, int height, float fps);
+
+int  wema_cuda_session_create(const wema_cuda_config *cfg, wema_cuda_session **out);
+void wema_cuda_session_destroy(wema_cuda_session *s);
+
+/* Device bytes a session of this configuration holds (pyramid, IIR state or
+ * window ring, threshold scratch, staging): the admission footprint. */
+size_t wema_cuda_session_bytes(const wema_cuda_config *cfg);
+
+/* One frame, device pointers, asynchronous on `cuda_stream` (a
+ * cudaStream_t; NULL = the session's own stream).  in/out are RGB24
+ * [height][width][3]; out may not alias in. */
+int wema_cuda_process_u8(wema_cuda_session *s, const uint8_t *d_in, uint8_t *d_out,
+                         void *cuda_stream);
+/* Same with float RGB in [0,1] (the reference's Frame layout); either output
+ * pointer may be NULL. */
+int wema_cuda_process_f32(wema_cuda_session *s, const float *d_in, float *d_out_f32,
+                          uint8_t *d_out_u8, void *cuda_stream);
+/* Host RGB24 in/out; copies in, processes, copies out, synchronises. */
+int wema_cuda_process_host_u8(wema_cuda_session *s, const uint8_t *h_in, uint8_t *h_out);
+
+/* Waits for the session's queued work. */
+int wema_cuda_session_sync(wema_cuda_session *s);
+
+/* Frames seen by the temporal filter (the reference's frames_processed,
+ * which jumps to the warm-up count at the first frame's preseed). */
+int wema_cuda_session_frames_processed(const wema_cuda_session *s);
+
+/* Copies a stage of the last processed frame to host memory, in the
+ * reference's layouts (synchronises first).  Returns the element count, or
+ * -1.  `what`: */
+enum {
+    WEMA_CUDA_READ_GRAY_IN = 0,   /* Y plane [P] (colour: Y) */
+    WEMA_CUDA_READ_GRAY_OUT = 1,  /* reconstructed Y [P] */
+    WEMA_CUDA_READ_ORIG6 = 2,     /* original coefficients, 6-slot flat [N6] */
+    WEMA_CUDA_READ_DELTA6 = 3,    /* band-passed deltas, 6-slot [N6] (slots 3-5 mirrored) */
+    WEMA_CUDA_READ_AMP6 = 4,      /* amplified coefficients, 6-slot [N6] */
+    WEMA_CUDA_READ_LOWPASS = 5,   /* coarsest LL */
+    WEMA_CUDA_READ_THRESHOLD = 6, /* per-channel thresholds [channels] */
+    WEMA_CUDA_READ_MAGSUM = 7     /* per-channel sum |x| [channels] */
+};
+long wema_cuda_session_read(wema_cuda_session *s, int what, int channel, float *h_dst, size_t cap);
+
+/* Per-stage device timing with CUDA events on the session's stream:
+ * stages are forward DWT level 0, forward DWT levels >= 1, threshold,
+ * temporal filter + amplification, inverse DWT, luma transfer.  times_ms[6]
+ * receives the accumulated milliseconds, *frames the frames timed. */
+enum { WEMA_CUDA_STAGES = 6 };
+int wema_cuda_set_timing(wema_cuda_session *s, int enable);
+int wema_cuda_stage_times(wema_cuda_session *s, double *times_ms, long long *frames);
+
+/* Whether each frame's band-passed deltas are stored for
+ * WEMA_CUDA_READ_DELTA6 (default 1; 0 saves one plane write per frame). */
+int wema_cuda_set_keep_deltas(wema_cuda_session *s, int keep);
+
+/* Exact reference threshold of a device array of n floats (plain flat
+ * order), written to *d_thr; d_sum optional.  Allocates its scratch. */
+int wema_cuda_threshold_flat(const float *d_x, size_t n, int threshold_form, float *d_thr,
+                             float *d_sum, void *cuda_stream);
+
+/* Message of the last failure on this thread ("" if none). */
+const char *wema_cuda_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WEMA_CUDA_H */

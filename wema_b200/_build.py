@@ -66,7 +66,7 @@ def build_cuda(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(objdir, exist_ok=True)
     nvcc = _nvcc()
     common = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
-              "-I", INCLUDE, "-I", CSRC, "-lineinfo"]
+              "-Xcompiler", "-ffp-contract=off", "-I", INCLUDE, "-I", CSRC, "-lineinfo"]
     objs = []
     for src in cu + cpp:
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
@@ -78,8 +78,6 @@ def build_cuda(force: bool = False, verbose: bool = False) -> str:
             cmd += ["--expt-relaxed-constexpr", "-Xptxas", "-O3"]
             if verbose:
                 cmd += ["-Xptxas", "-v"]
-        else:
-            cmd[1:1] = ["-x", "cu"] if False else []
         subprocess.run(cmd, check=True)
     subprocess.run([nvcc, *NVCC_ARCH, "-shared", *objs, "-o", out, "-lcudart", "-lpthread"],
                    check=True)

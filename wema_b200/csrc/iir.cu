@@ -1,0 +1,166 @@
+// iir.cu - per-coefficient temporal band-pass (Butterworth HP + LP biquads,
+// DF-II transposed) fused with the adaptive-threshold amplification.
+//
+// One thread per unique detail coefficient.  The reference filters all six
+// slots, but slots 3-5 carry the same input sequence as slots 2-0 and their
+// deltas are never read back (dwt.c:749-751), so the unique three suffice.
+// State is one float4 per coefficient {w1_hp, w2_hp, w1_lp, w2_lp}.
+// Arithmetic is the AVX-512 path's (iir_filter.c:210-224):
+//   y = fma(b0, x, w1); w1 = fnma(a1, y, fma(b1, x, w2)); w2 = fnma(a2, y, b2*x)
+// except for positions at or past the last full 16-wide block of the 6-slot
+// array, which the reference runs in its scalar loop: w2 = fms(b2, x, a2*y)
+// (iir_filter.c:231-246).  Amplification (wema.c:726-743):
+//   out = |x| > thr ? fma(delta, alpha_l, x) : x,  alpha_0 = alpha/2.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace wema {
+
+constexpr int IIR_THREADS = 256;
+
+struct IirDev {
+    IirParams p;
+    const float* coef;
+    long long frame_stride;
+    int frames;
+    float4* state;
+    float* amplified;
+    float* delta_out;
+    const float* thr;
+    const float* amp;      // batch route: per-frame alphas (device)
+    float alpha;           // single frame: the channel's alpha
+    int warmup;
+};
+
+__device__ __forceinline__ float cascade(const float* c, float4& st, float x, bool tail) {
+    // high-pass section
+    float y = __fmaf_rn(c[0], x, st.x);
+    float w1 = __fmaf_rn(-c[3], y, __fmaf_rn(c[1], x, st.y));
+    float w2 = tail ? __fmaf_rn(c[2], x, -__fmul_rn(c[4], y)) : __fmaf_rn(-c[4], y, __fmul_rn(c[2], x));
+    st.x = w1;
+    st.y = w2;
+    x = y;
+    // low-pass section
+    y = __fmaf_rn(c[5], x, st.z);
+    w1 = __fmaf_rn(-c[8], y, __fmaf_rn(c[6], x, st.w));
+    w2 = tail ? __fmaf_rn(c[7], x, -__fmul_rn(c[9], y)) : __fmaf_rn(-c[9], y, __fmul_rn(c[7], x));
+    st.z = w1;
+    st.w = w2;
+    return y;
+}
+
+// level of unique position u, and whether its 6-slot index is in the
+// reference's scalar tail
+__device__ __forceinline__ int level_of(const IirParams& p, long long u, bool& tail) {
+    int l = 0;
+#pragma unroll
+    for (int k = 1; k < 4; k++)
+        if (k < p.levels && u >= p.uoff[k]) l = k;
+    const long long r = u - p.uoff[l];             // band * n + k, band in 0..2 = slot
+    tail = p.off6[l] + r >= p.simd_end;
+    return l;
+}
+
+__global__ void __launch_bounds__(IIR_THREADS) k_iir_preseed(IirDev a) {
+    const long long pu = a.p.uoff[a.p.levels];
+    for (long long u = blockIdx.x * (long long)IIR_THREADS + threadIdx.x; u < pu;
+         u += (long long)gridDim.x * IIR_THREADS) {
+        bool tail;
+        level_of(a.p, u, tail);
+        const float x = a.coef[u];
+        float4 st = a.state[u];
+        for (int it = 0; it < a.warmup; it++) cascade(a.p.c, st, x, tail);
+        a.state[u] = st;
+    }
+}
+
+__global__ void __launch_bounds__(IIR_THREADS) k_iir_amp(IirDev a) {
+    const long long pu = a.p.uoff[a.p.levels];
+    const float thr = *a.thr;
+    const float alpha = a.alpha;
+    const float alpha0 = __fmul_rn(alpha, 0.5f);
+    for (long long u = blockIdx.x * (long long)IIR_THREADS + threadIdx.x; u < pu;
+         u += (long long)gridDim.x * IIR_THREADS) {
+        bool tail;
+        const int l = level_of(a.p, u, tail);
+        float4 st = a.state[u];
+        const float x = a.coef[u];
+        const float d = cascade(a.p.c, st, x, tail);
+        const float al = l == 0 ? alpha0 : alpha;
+        if (a.delta_out) a.delta_out[u] = d;
+        a.amplified[u] = fabsf(x) > thr ? __fmaf_rn(d, al, x) : x;
+        a.state[u] = st;
+    }
+}
+
+// batch route: per-frame thresholds and alphas
+__global__ void __launch_bounds__(IIR_THREADS) k_iir_amp_frames(IirDev a) {
+    const long long pu = a.p.uoff[a.p.levels];
+    for (long long u = blockIdx.x * (long long)IIR_THREADS + threadIdx.x; u < pu;
+         u += (long long)gridDim.x * IIR_THREADS) {
+        bool tail;
+        const int l = level_of(a.p, u, tail);
+        float4 st = a.state[u];
+        for (int f = 0; f < a.frames; f++) {
+            const long long o = f * a.frame_stride + u;
+            const float x = a.coef[o];
+            const float d = cascade(a.p.c, st, x, tail);
+            const float alpha = a.amp[f];
+            const float al = l == 0 ? __fmul_rn(alpha, 0.5f) : alpha;
+            if (a.delta_out) a.delta_out[o] = d;
+            a.amplified[o] = fabsf(x) > a.thr[f] ? __fmaf_rn(d, al, x) : x;
+        }
+        a.state[u] = st;
+    }
+}
+
+static int grid_for(long long n) {
+    long long b = (n + IIR_THREADS - 1) / IIR_THREADS;
+    return (int)(b < 148 * 16 ? (b > 0 ? b : 1) : 148 * 16);
+}
+
+cudaError_t launch_iir_preseed(const IirParams& p, const float* coef, float4* state, int warmup,
+                               cudaStream_t st) {
+    IirDev a{};
+    a.p = p;
+    a.coef = coef;
+    a.state = state;
+    a.warmup = warmup;
+    k_iir_preseed<<<grid_for(p.uoff[p.levels]), IIR_THREADS, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_iir_amp(const IirParams& p, const float* coef, float4* state, float* amplified,
+                           float* delta_out, const float* thr, float alpha, cudaStream_t st) {
+    IirDev a{};
+    a.p = p;
+    a.coef = coef;
+    a.frames = 1;
+    a.frame_stride = 0;
+    a.state = state;
+    a.amplified = amplified;
+    a.delta_out = delta_out;
+    a.thr = thr;
+    a.alpha = alpha;
+    k_iir_amp<<<grid_for(p.uoff[p.levels]), IIR_THREADS, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_iir_amp_frames(const IirParams& p, const float* coef, long long frame_stride,
+                                  int frames, float4* state, float* amplified, float* delta_out,
+                                  const float* thr, const float* amp, cudaStream_t st) {
+    IirDev a{};
+    a.p = p;
+    a.coef = coef;
+    a.frames = frames;
+    a.frame_stride = frame_stride;
+    a.state = state;
+    a.amplified = amplified;
+    a.delta_out = delta_out;
+    a.thr = thr;
+    a.amp = amp;
+    k_iir_amp_frames<<<grid_for(p.uoff[p.levels]), IIR_THREADS, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace wema

@@ -1,0 +1,117 @@
+// kernels.h - launch interface of the sm_100a kernels (host side of csrc/).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace wema {
+
+// ---- DWT (dwt.cu) --------------------------------------------------------
+enum { kSrcPlanes = 0, kSrcRgbU8 = 1, kSrcRgbF32 = 2 };
+enum { kOutPlanes = 0, kOutRgb = 1 };
+
+struct FwdLevelParams {
+    int iw, ih;                 // level input size
+    int sw, sh;                 // subband size
+    long long n;                // sw*sh
+    long long vec_end;          // level 0: pixels below use the vector-body luma form
+    const float* src_planes[3]; // levels >= 1: input planes (previous LL)
+    const uint8_t* src_u8;      // level 0: interleaved RGB24
+    const float* src_f32;       // level 0: interleaved float RGB
+    float* plane_out[3];        // level 0, optional: converted Y / Cb / Cr planes
+    float* coef[3];             // this level's bands LH, HH, HL (n each)
+    const float* prev[3];       // previous level's bands (stale entries), or null
+    long long prev_n;
+    float* ll_out[3];           // LL (next level's input or the lowpass)
+};
+
+struct InvLevelParams {
+    int ow, oh;                 // level canvas size (reconstructed image)
+    int sw, sh;
+    long long n;
+    const float* ll[3];         // coarser reconstruction / lowpass (sw x sh)
+    const float* coef[3];       // bands LH, HH, HL
+    float* out_planes[3];       // reconstructed planes (kOutPlanes), optional for kOutRgb
+    uint8_t* out_u8;            // kOutRgb: RGB24 output (optional)
+    float* out_f32;             // kOutRgb: float RGB output (optional)
+};
+
+cudaError_t dwt_prepare_device();
+size_t dwt_smem_bytes(int channels);
+cudaError_t launch_dwt_fwd(int src_mode, int channels, const FwdLevelParams& p, cudaStream_t st);
+cudaError_t launch_dwt_inv(int channels, int out_mode, const InvLevelParams& p, cudaStream_t st);
+
+// ---- exact threshold (threshold.cu) ---------------------------------------
+// Views the unique detail planes of one channel as the reference's 6-slot
+// flat array and reproduces its vectorised FP32 sum of |x| bit for bit.
+struct PyrView {
+    const float* coef;          // unique planes (uoff layout); levels == 0: flat array of off6[0]
+    int levels;
+    long long n[4], uoff[4], off6[5];   // off6[levels] = N6
+};
+
+struct ThrScratch {             // device scratch, sized by thr_scratch_bytes
+    double* part;               // [n_sub][8] exact-ish lane partial sums
+    double* prefix;             // [n_sub][8] exclusive prefixes
+    int4* cand;                 // [n_sub][8][2] binade top and monoids of 3 candidates
+    int2* cand1;                // unused
+};
+size_t thr_scratch_bytes(long long n6);
+void thr_scratch_bind(ThrScratch& s, void* base, long long n6);
+// Writes thr[chan] = threshold of each of `nch` channels (single-frame form
+// (sum/N)*0.2, or batch form (0.2/N)*sum); optionally the raw sums.
+cudaError_t launch_threshold(const PyrView* views, int nch, ThrScratch* scratch, float* thr,
+                             float* sums, int batch_form, cudaStream_t st);
+
+// ---- IIR + amplification (iir.cu) ------------------------------------------
+struct IirParams {
+    float c[10];                // {b0,b1,b2,a1,a2} high-pass, then low-pass
+    int levels;
+    long long uoff[5];          // unique-plane level offsets
+    long long n[4];
+    long long off6[5];
+    long long simd_end;         // 6-slot positions >= simd_end take the scalar-tail form
+};
+// preseed: run `warmup` iterations with the current coefficients as input
+cudaError_t launch_iir_preseed(const IirParams& p, const float* coef, float4* state, int warmup,
+                               cudaStream_t st);
+// one frame: delta = cascade(coef), amplified = |coef| > thr ? fma(delta, a_l, coef) : coef
+// alpha: the channel's amplification (fade-in applied); thr: device scalar
+cudaError_t launch_iir_amp(const IirParams& p, const float* coef, float4* state, float* amplified,
+                           float* delta_out, const float* thr, float alpha, cudaStream_t st);
+// frames [0, F) of one stream: coefficients [F][Pu] frame-major, state kept
+// in registers across the frames (batch route)
+cudaError_t launch_iir_amp_frames(const IirParams& p, const float* coef, long long frame_stride,
+                                  int frames, float4* state, float* amplified, float* delta_out,
+                                  const float* thr, const float* amp, cudaStream_t st);
+
+// ---- spatial filter + luma transfer (spatial.cu) ----------------------------
+struct TransferParams {
+    int w, h;
+    long long vec_end;          // guide luma form switch (vector body / tail)
+    const uint8_t* src_u8;      // input RGB24 (or null)
+    const float* src_f32;       // input float RGB (or null)
+    const float* gray_out;      // reconstructed luma
+    uint8_t* out_u8;            // output RGB24 (optional)
+    float* out_f32;             // output float RGB (optional)
+    int edge_aware;             // 1: guided filter r=4 eps=0.01; 0: 5-tap Gaussian
+};
+cudaError_t launch_transfer(const TransferParams& p, cudaStream_t st);
+cudaError_t spatial_prepare_device();
+
+// copy-through (window mode before the ring is full): out = in
+cudaError_t launch_passthrough(const TransferParams& p, cudaStream_t st);
+
+// ---- window (--haar) temporal filter (window.cu) ----------------------------
+struct WindowParams {
+    long long pu;               // unique positions
+    int ws, head;               // window size, ring slot of the oldest sample
+    int bilateral;
+    float time_w[256];
+};
+cudaError_t launch_ring_push(const float* coef, float* ring, long long pu, int slot, cudaStream_t st);
+cudaError_t launch_window_amp(const WindowParams& wp, const IirParams& geo, const float* ring,
+                              const float* coef, float* amplified, float* delta_out,
+                              const float* thr, float alpha, cudaStream_t st);
+
+}  // namespace wema

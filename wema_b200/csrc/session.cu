@@ -1,0 +1,566 @@
+// session.cu - per-stream pipeline and the wema_cuda_* entry points.
+//
+// A Session owns every device buffer of one video stream in a single
+// allocation: the unique detail planes (orig, amplified, deltas), the IIR
+// state (float4 per coefficient) or the window ring, the LL / reconstruction
+// planes of each level, the threshold scratch and a few scalars.  A frame is
+// a fixed sequence of launches on one stream:
+//   forward DWT (L launches, level 0 reads RGB and converts on the fly)
+//   exact threshold (4 launches, all channels together)
+//   [first frame: preseed]  IIR + amplify  |  ring push + window amplify
+//   inverse DWT (L launches; colour writes RGB at level 0)
+//   luma: guided filter / Gaussian + RGB transfer + u8 quantisation
+// mirroring wema_process_frame (wema.c:746-952).
+#include "session.h"
+
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <mutex>
+#include <new>
+#include <vector>
+
+namespace wema {
+
+static thread_local std::string g_err;
+
+void set_error(const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+}
+void clear_error() { g_err.clear(); }
+const char* last_error() { return g_err.c_str(); }
+
+bool cuda_ok(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return true;
+    set_error("%s: %s", what, cudaGetErrorString(e));
+    return false;
+}
+
+bool ensure_device(int dev) {
+    static std::mutex mu;
+    static std::vector<char> ready;
+    if (!cuda_ok(cudaSetDevice(dev), "cudaSetDevice")) return false;
+    std::lock_guard<std::mutex> lk(mu);
+    if ((int)ready.size() <= dev) ready.resize(dev + 1, 0);
+    if (ready[dev]) return true;
+    if (!cuda_ok(dwt_prepare_device(), "DWT kernel setup")) return false;
+    if (!cuda_ok(spatial_prepare_device(), "spatial kernel setup")) return false;
+    ready[dev] = 1;
+    return true;
+}
+
+// ---------------------------------------------------------------- IIR design
+#define WEMA_PI_F ((float)3.14159265358979323846)
+
+// iir_design_bandpass / iir_temporal_init (iir_filter.c:36-154), evaluated
+// the way the reference's -Ofast build evaluates it (FMA placement read
+// from GCC's optimised-tree dump of that build).
+int design_bandpass(float f_low, float f_high, float fs, float c[10], int* warmup) {
+    if (f_low >= f_high || f_low <= 0 || fs * 0.5f <= f_high) return -1;
+    const float s2 = 1.41421356237f;
+    float wc = tanf((f_low * WEMA_PI_F) / fs);
+    float ws2 = wc * s2;
+    float norm = 1.0f / (fmaf(wc, wc, ws2) + 1.0f);
+    c[0] = norm;
+    c[1] = norm * -2.0f;
+    c[2] = norm;
+    c[3] = (fmaf(wc, wc, -1.0f) * 2.0f) * norm;
+    c[4] = (fmaf(wc, wc, 1.0f) - ws2) * norm;
+    wc = tanf((f_high * WEMA_PI_F) / fs);
+    float wc2 = wc * wc;
+    norm = 1.0f / (fmaf(wc, s2, wc2) + 1.0f);
+    c[5] = wc2 * norm;
+    c[6] = c[5] * 2.0f;
+    c[7] = c[5];
+    c[8] = ((wc2 - 1.0f) * 2.0f) * norm;
+    c[9] = norm * fmaf(-wc, s2, wc2 + 1.0f);
+    if (warmup) {
+        int w = (int)(7.0f * fs / (2.0f * WEMA_PI_F * f_low));
+        *warmup = w < 30 ? 30 : w;
+    }
+    return 0;
+}
+
+// quadratic 15-frame fade-in after the preseed (wema.c:831-839)
+float fade_amp(float amp_factor, int frames_before, int warmup) {
+    const int g = frames_before - warmup;
+    if (g < 0) return 0.0f;
+    if (g >= 15) return amp_factor;
+    const float t = (float)(g + 1) * (1.0f / 15.0f);
+    return (t * t) * amp_factor;
+}
+
+// ------------------------------------------------------------------- arena
+
+namespace {
+struct Arena {
+    size_t off = 0;
+    char* base = nullptr;
+    template <class T>
+    T* take(size_t count) {
+        off = (off + 255) & ~(size_t)255;
+        T* p = base ? (T*)(base + off) : nullptr;
+        off += count * sizeof(T);
+        return p;
+    }
+};
+}  // namespace
+
+static void layout(Arena& A, Session& s) {
+    const Geom& g = s.g;
+    const long long pu = g.uoff[g.levels];
+    const long long n6 = g.off6[g.levels];
+    for (int c = 0; c < s.nch; c++) {
+        s.coef[c] = A.take<float>(pu);
+        s.ampl[c] = A.take<float>(pu);
+        s.delta[c] = A.take<float>(pu);
+        if (s.cfg.use_iir) s.state[c] = A.take<float4>(pu);
+        else s.ring[c] = A.take<float>((size_t)pu * s.cfg.temporal_window);
+        for (int l = 0; l < g.levels; l++) s.ll[c][l] = A.take<float>(g.n[l]);
+        for (int l = 0; l < g.levels; l++)
+            s.rec[c][l] = A.take<float>((size_t)g.in_w[l] * g.in_h[l]);
+        s.gray_in[c] = A.take<float>(g.pixels);
+        void* t = A.take<char>(thr_scratch_bytes(n6));
+        if (A.base) thr_scratch_bind(s.thr_s[c], t, n6);
+    }
+    s.d_small = A.take<float>(16);
+}
+
+static bool valid_config(const wema_cuda_config& c) {
+    if (c.width < 1 || c.height < 1) { set_error("frame size must be positive"); return false; }
+    if ((long long)c.width * c.height > (1LL << 28)) { set_error("frame too large"); return false; }
+    if (!(c.fps > 0)) { set_error("fps must be positive"); return false; }
+    if (!c.use_iir && (c.temporal_window < 4 || c.temporal_window > 256)) {
+        set_error("temporal window must be in [4, 256]");
+        return false;
+    }
+    return true;
+}
+
+size_t Session::bytes_for(const wema_cuda_config& c) {
+    if (!valid_config(c)) return 0;
+    Session s;
+    s.cfg = c;
+    s.g = make_geom(c.width, c.height);
+    s.nch = c.color_mode ? 3 : 1;
+    Arena A;
+    layout(A, s);
+    return A.off + 6 * (size_t)s.g.pixels * (1 + sizeof(float));   // + host-API staging
+}
+
+Session::~Session() {
+    if (stream) {
+        cudaStreamSynchronize(stream);
+        cudaStreamDestroy(stream);
+    }
+    if (arena) cudaFree(arena);
+    if (stage_u8) cudaFree(stage_u8);
+    if (stage_f32) cudaFree(stage_f32);
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+}
+
+// adds the last timed frame's per-stage durations (waits for it)
+bool Session::collect_timing() {
+    if (!ev_pending) return true;
+    ev_pending = false;
+    if (!cuda_ok(cudaEventSynchronize(ev[N_STAGE]), "event sync")) return false;
+    for (int k = 0; k < N_STAGE; k++) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, ev[k], ev[k + 1]) == cudaSuccess) stage_ms[k] += ms;
+    }
+    stage_frames++;
+    return true;
+}
+
+bool Session::init(const wema_cuda_config& c) {
+    if (!valid_config(c)) return false;
+    cfg = c;
+    if (!ensure_device(c.device)) return false;
+    g = make_geom(c.width, c.height);
+    nch = c.color_mode ? 3 : 1;
+    if (c.use_iir) {
+        if (design_bandpass(c.f_low, c.f_high, c.fps, coef10, &warmup) < 0) {
+            set_error("invalid band: need 0 < f_low < f_high < fps/2 (iir_filter.c:74)");
+            return false;
+        }
+    }
+    memcpy(ip.c, coef10, sizeof coef10);
+    ip.levels = g.levels;
+    for (int l = 0; l <= g.levels; l++) { ip.uoff[l] = g.uoff[l]; ip.off6[l] = g.off6[l]; }
+    for (int l = 0; l < g.levels; l++) ip.n[l] = g.n[l];
+    ip.simd_end = g.off6[g.levels] & ~15LL;
+
+    Arena A;
+    layout(A, *this);
+    arena_bytes = A.off;
+    if (!cuda_ok(cudaMalloc(&arena, arena_bytes), "cudaMalloc(session)")) return false;
+    if (!cuda_ok(cudaMemset(arena, 0, arena_bytes), "cudaMemset")) return false;
+    A = Arena();
+    A.base = (char*)arena;
+    layout(A, *this);
+    if (!cuda_ok(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate"))
+        return false;
+    return true;
+}
+
+bool Session::ensure_staging() {
+    if (stage_u8) return true;
+    const size_t P3 = 3 * (size_t)g.pixels;
+    if (!cuda_ok(cudaMalloc(&stage_u8, 2 * P3), "cudaMalloc(staging)")) return false;
+    if (!cuda_ok(cudaMalloc(&stage_f32, 2 * P3 * sizeof(float)), "cudaMalloc(staging)")) return false;
+    return true;
+}
+
+PyrView Session::view(int c) const {
+    PyrView v{};
+    v.coef = coef[c];
+    v.levels = g.levels;
+    for (int l = 0; l < g.levels; l++) { v.n[l] = g.n[l]; v.uoff[l] = g.uoff[l]; }
+    for (int l = 0; l <= g.levels; l++) v.off6[l] = g.off6[l];
+    return v;
+}
+
+bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, float* out_f32,
+                  cudaStream_t st) {
+    const int L = g.levels;
+    float* d_thr = d_small;
+    float* d_sum = d_small + 4;
+    last_passthrough = false;
+    if (timing) {
+        if (!collect_timing()) return false;
+        if (!ev[0])
+            for (auto& e : ev)
+                if (!cuda_ok(cudaEventCreate(&e), "cudaEventCreate")) return false;
+    }
+    mark(ST_FWD0, st);
+
+    // forward DWT
+    for (int l = 0; l < L; l++) {
+        FwdLevelParams p{};
+        p.iw = g.in_w[l];
+        p.ih = g.in_h[l];
+        p.sw = g.sw[l];
+        p.sh = g.sh[l];
+        p.n = g.n[l];
+        p.vec_end = vec_cover(g.pixels);
+        int mode = kSrcPlanes;
+        if (l == 0) {
+            mode = in_u8 ? kSrcRgbU8 : kSrcRgbF32;
+            p.src_u8 = in_u8;
+            p.src_f32 = in_f32;
+            for (int c = 0; c < nch; c++) p.plane_out[c] = gray_in[c];
+        } else {
+            for (int c = 0; c < nch; c++) p.src_planes[c] = ll[c][l - 1];
+        }
+        for (int c = 0; c < nch; c++) {
+            p.coef[c] = coef[c] + g.uoff[l];
+            p.prev[c] = l > 0 ? coef[c] + g.uoff[l - 1] : nullptr;
+            p.ll_out[c] = ll[c][l];
+        }
+        p.prev_n = l > 0 ? g.n[l - 1] : 0;
+        if (!cuda_ok(launch_dwt_fwd(mode, nch, p, st), "forward DWT")) return false;
+        if (l == 0) mark(ST_FWD, st);
+    }
+    mark(ST_THR, st);
+
+    PyrView views[3];
+    for (int c = 0; c < nch; c++) views[c] = view(c);
+
+    if (cfg.use_iir) {
+        if (!cuda_ok(launch_threshold(views, nch, thr_s, d_thr, d_sum, cfg.threshold_form, st),
+                     "threshold"))
+            return false;
+        mark(ST_TEMPORAL, st);
+        if (frames_processed == 0) {   // iir_temporal_preseed on the first frame
+            for (int c = 0; c < nch; c++)
+                if (!cuda_ok(launch_iir_preseed(ip, coef[c], state[c], warmup, st), "preseed"))
+                    return false;
+            frames_processed = warmup;
+        }
+        const float amp = fade_amp(cfg.amp_factor, frames_processed, warmup);
+        frames_processed++;
+        for (int c = 0; c < nch; c++)
+            if (!cuda_ok(launch_iir_amp(ip, coef[c], state[c], ampl[c], write_delta ? delta[c] : nullptr,
+                                        d_thr + c, c == 0 ? amp : amp * 0.5f, st),
+                         "IIR"))
+                return false;
+    } else {
+        const long long pu = g.uoff[L];
+        for (int c = 0; c < nch; c++)
+            if (!cuda_ok(launch_ring_push(coef[c], ring[c], pu, head, st), "ring push")) return false;
+        head = (head + 1) % cfg.temporal_window;
+        if (filled < cfg.temporal_window) filled++;
+        if (filled < cfg.temporal_window) {   // wema.c:924-929: pass the input through
+            TransferParams tp{};
+            tp.w = g.w;
+            tp.h = g.h;
+            tp.src_u8 = in_u8;
+            tp.src_f32 = in_f32;
+            tp.out_u8 = out_u8;
+            tp.out_f32 = out_f32;
+            last_passthrough = true;
+            return cuda_ok(launch_passthrough(tp, st), "passthrough");
+        }
+        if (!cuda_ok(launch_threshold(views, nch, thr_s, d_thr, d_sum, cfg.threshold_form, st),
+                     "threshold"))
+            return false;
+        mark(ST_TEMPORAL, st);
+        WindowParams wp{};
+        wp.pu = pu;
+        wp.ws = cfg.temporal_window;
+        wp.head = head;   // oldest sample (temporal_filter.c:221)
+        wp.bilateral = cfg.bilateral_temp;
+        const int ws = cfg.temporal_window, center = ws / 2;
+        const float ts = (float)ws * 0.15f;
+        const float inv2 = 0.5f / (ts * ts);
+        for (int t = 0; t < ws; t++) {
+            const float d = (float)(t - center);
+            wp.time_w[t] = expf(-(d * d) * inv2);
+        }
+        for (int c = 0; c < nch; c++)
+            if (!cuda_ok(launch_window_amp(wp, ip, ring[c], coef[c], ampl[c],
+                                           write_delta ? delta[c] : nullptr, d_thr + c,
+                                           c == 0 ? cfg.amp_factor : cfg.amp_factor * 0.5f, st),
+                         "window filter"))
+                return false;
+    }
+
+    mark(ST_INV, st);
+    // inverse DWT, coarse to fine
+    for (int l = L - 1; l >= 0; l--) {
+        InvLevelParams q{};
+        q.ow = g.in_w[l];
+        q.oh = g.in_h[l];
+        q.sw = g.sw[l];
+        q.sh = g.sh[l];
+        q.n = g.n[l];
+        for (int c = 0; c < nch; c++) {
+            q.ll[c] = (l == L - 1) ? ll[c][L - 1] : rec[c][l + 1];
+            q.coef[c] = ampl[c] + g.uoff[l];
+            q.out_planes[c] = rec[c][l];
+        }
+        int mode = kOutPlanes;
+        if (l == 0 && nch == 3) {
+            mode = kOutRgb;
+            q.out_u8 = out_u8;
+            q.out_f32 = out_f32;
+        }
+        if (!cuda_ok(launch_dwt_inv(nch, mode, q, st), "inverse DWT")) return false;
+    }
+    mark(ST_XFER, st);
+    if (nch == 1) {
+        TransferParams tp{};
+        tp.w = g.w;
+        tp.h = g.h;
+        tp.vec_end = vec_cover(g.pixels);
+        tp.src_u8 = in_u8;
+        tp.src_f32 = in_f32;
+        tp.gray_out = rec[0][0];
+        tp.out_u8 = out_u8;
+        tp.out_f32 = out_f32;
+        tp.edge_aware = cfg.edge_aware;
+        if (!cuda_ok(launch_transfer(tp, st), "luma transfer")) return false;
+    }
+    mark(N_STAGE, st);
+    ev_pending = timing;
+    return true;
+}
+
+}  // namespace wema
+
+// ===================================================================== C ABI
+using namespace wema;
+
+struct wema_cuda_session {
+    Session s;
+};
+
+#define WEMA_API extern "C" __attribute__((visibility("default")))
+
+WEMA_API const char* wema_cuda_last_error(void) { return last_error(); }
+
+WEMA_API void wema_cuda_config_default(wema_cuda_config* cfg, int width, int height, float fps) {
+    memset(cfg, 0, sizeof *cfg);
+    cfg->width = width;
+    cfg->height = height;
+    cfg->fps = fps;
+    cfg->amp_factor = 120.0f;
+    cfg->f_low = 0.5f;
+    cfg->f_high = fps / 2.0f - 0.0001f;   // main.c:248-250
+    cfg->temporal_window = 32;
+    cfg->edge_aware = 1;
+    cfg->bilateral_temp = 0;
+    cfg->color_mode = 0;
+    cfg->use_iir = 1;
+    cfg->threshold_form = WEMA_CUDA_THR_SINGLE;
+    cfg->device = 0;
+}
+
+WEMA_API size_t wema_cuda_session_bytes(const wema_cuda_config* cfg) {
+    clear_error();
+    if (!cfg) { set_error("null config"); return 0; }
+    return Session::bytes_for(*cfg);
+}
+
+WEMA_API int wema_cuda_session_create(const wema_cuda_config* cfg, wema_cuda_session** out) {
+    clear_error();
+    if (!cfg || !out) { set_error("null argument"); return -1; }
+    *out = nullptr;
+    wema_cuda_session* s = new (std::nothrow) wema_cuda_session();
+    if (!s) { set_error("out of host memory"); return -1; }
+    if (!s->s.init(*cfg)) {
+        delete s;
+        return -1;
+    }
+    *out = s;
+    return 0;
+}
+
+WEMA_API void wema_cuda_session_destroy(wema_cuda_session* s) {
+    if (!s) return;
+    cudaSetDevice(s->s.cfg.device);
+    delete s;
+}
+
+WEMA_API int wema_cuda_process_u8(wema_cuda_session* s, const uint8_t* d_in, uint8_t* d_out,
+                                  void* cuda_stream) {
+    clear_error();
+    if (!s || !d_in || !d_out) { set_error("null argument"); return -1; }
+    if (!cuda_ok(cudaSetDevice(s->s.cfg.device), "cudaSetDevice")) return -1;
+    cudaStream_t st = cuda_stream ? (cudaStream_t)cuda_stream : s->s.stream;
+    return s->s.run(d_in, nullptr, d_out, nullptr, st) ? 0 : -1;
+}
+
+WEMA_API int wema_cuda_process_f32(wema_cuda_session* s, const float* d_in, float* d_out_f32,
+                                   uint8_t* d_out_u8, void* cuda_stream) {
+    clear_error();
+    if (!s || !d_in || (!d_out_f32 && !d_out_u8)) { set_error("null argument"); return -1; }
+    if (!cuda_ok(cudaSetDevice(s->s.cfg.device), "cudaSetDevice")) return -1;
+    cudaStream_t st = cuda_stream ? (cudaStream_t)cuda_stream : s->s.stream;
+    return s->s.run(nullptr, d_in, d_out_u8, d_out_f32, st) ? 0 : -1;
+}
+
+WEMA_API int wema_cuda_process_host_u8(wema_cuda_session* s, const uint8_t* h_in, uint8_t* h_out) {
+    clear_error();
+    if (!s || !h_in || !h_out) { set_error("null argument"); return -1; }
+    Session& S = s->s;
+    if (!cuda_ok(cudaSetDevice(S.cfg.device), "cudaSetDevice")) return -1;
+    if (!S.ensure_staging()) return -1;
+    const size_t P3 = 3 * (size_t)S.g.pixels;
+    if (!cuda_ok(cudaMemcpyAsync(S.stage_u8, h_in, P3, cudaMemcpyHostToDevice, S.stream), "H2D"))
+        return -1;
+    if (!S.run(S.stage_u8, nullptr, S.stage_u8 + P3, nullptr, S.stream)) return -1;
+    if (!cuda_ok(cudaMemcpyAsync(h_out, S.stage_u8 + P3, P3, cudaMemcpyDeviceToHost, S.stream), "D2H"))
+        return -1;
+    return cuda_ok(cudaStreamSynchronize(S.stream), "sync") ? 0 : -1;
+}
+
+WEMA_API int wema_cuda_session_sync(wema_cuda_session* s) {
+    clear_error();
+    if (!s) { set_error("null session"); return -1; }
+    if (!cuda_ok(cudaSetDevice(s->s.cfg.device), "cudaSetDevice")) return -1;
+    return cuda_ok(cudaStreamSynchronize(s->s.stream), "sync") ? 0 : -1;
+}
+
+WEMA_API int wema_cuda_session_frames_processed(const wema_cuda_session* s) {
+    return s ? s->s.frames_processed : -1;
+}
+
+WEMA_API long wema_cuda_session_read(wema_cuda_session* s, int what, int channel, float* h_dst,
+                                     size_t cap) {
+    clear_error();
+    if (!s || !h_dst) { set_error("null argument"); return -1; }
+    Session& S = s->s;
+    if (channel < 0 || channel >= S.nch) { set_error("bad channel"); return -1; }
+    if (!cuda_ok(cudaSetDevice(S.cfg.device), "cudaSetDevice")) return -1;
+    if (!cuda_ok(cudaDeviceSynchronize(), "sync")) return -1;
+    const Geom& g = S.g;
+    const long long pu = g.uoff[g.levels], n6 = g.off6[g.levels];
+    auto rd = [&](const float* src, size_t n) -> long {
+        if (n > cap) { set_error("buffer too small (%zu needed)", n); return -1; }
+        return cuda_ok(cudaMemcpy(h_dst, src, n * sizeof(float), cudaMemcpyDeviceToHost), "D2H")
+                   ? (long)n : -1;
+    };
+    auto rd6 = [&](const float* src) -> long {
+        if ((size_t)n6 > cap) { set_error("buffer too small (%lld needed)", n6); return -1; }
+        std::vector<float> u(pu);
+        if (!cuda_ok(cudaMemcpy(u.data(), src, pu * sizeof(float), cudaMemcpyDeviceToHost), "D2H"))
+            return -1;
+        for (int l = 0; l < g.levels; l++)
+            for (int slot = 0; slot < 6; slot++) {
+                const int band = slot < 3 ? slot : 5 - slot;
+                memcpy(h_dst + g.off6[l] + slot * g.n[l], u.data() + g.uoff[l] + band * g.n[l],
+                       g.n[l] * sizeof(float));
+            }
+        return (long)n6;
+    };
+    switch (what) {
+        case WEMA_CUDA_READ_GRAY_IN: return rd(S.gray_in[channel], g.pixels);
+        case WEMA_CUDA_READ_GRAY_OUT: return rd(S.rec[channel][0], g.pixels);
+        case WEMA_CUDA_READ_ORIG6: return rd6(S.coef[channel]);
+        case WEMA_CUDA_READ_DELTA6: return rd6(S.delta[channel]);
+        case WEMA_CUDA_READ_AMP6: return rd6(S.ampl[channel]);
+        case WEMA_CUDA_READ_LOWPASS: return rd(S.ll[channel][g.levels - 1], g.low_n);
+        case WEMA_CUDA_READ_THRESHOLD: return rd(S.d_small, S.nch);
+        case WEMA_CUDA_READ_MAGSUM: return rd(S.d_small + 4, S.nch);
+    }
+    set_error("unknown stage %d", what);
+    return -1;
+}
+
+WEMA_API int wema_cuda_set_timing(wema_cuda_session* s, int enable) {
+    clear_error();
+    if (!s) { set_error("null session"); return -1; }
+    Session& S = s->s;
+    if (!cuda_ok(cudaSetDevice(S.cfg.device), "cudaSetDevice")) return -1;
+    if (!S.collect_timing()) return -1;
+    S.timing = enable != 0;
+    for (double& v : S.stage_ms) v = 0.0;
+    S.stage_frames = 0;
+    return 0;
+}
+
+WEMA_API int wema_cuda_stage_times(wema_cuda_session* s, double* times_ms, long long* frames) {
+    clear_error();
+    if (!s || !times_ms) { set_error("null argument"); return -1; }
+    Session& S = s->s;
+    if (!cuda_ok(cudaSetDevice(S.cfg.device), "cudaSetDevice")) return -1;
+    if (!S.collect_timing()) return -1;
+    for (int k = 0; k < Session::N_STAGE; k++) times_ms[k] = S.stage_ms[k];
+    if (frames) *frames = S.stage_frames;
+    return 0;
+}
+
+WEMA_API int wema_cuda_set_keep_deltas(wema_cuda_session* s, int keep) {
+    clear_error();
+    if (!s) { set_error("null session"); return -1; }
+    s->s.write_delta = keep != 0;
+    return 0;
+}
+
+WEMA_API int wema_cuda_threshold_flat(const float* d_x, size_t n, int threshold_form, float* d_thr,
+                                      float* d_sum, void* cuda_stream) {
+    clear_error();
+    if (!d_x || !d_thr || n == 0) { set_error("bad argument"); return -1; }
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    void* scratch = nullptr;
+    const size_t bytes = thr_scratch_bytes((long long)n);
+    if (!cuda_ok(cudaMallocAsync(&scratch, bytes, st), "cudaMallocAsync")) return -1;
+    ThrScratch ts{};
+    thr_scratch_bind(ts, scratch, (long long)n);
+    PyrView v{};
+    v.coef = d_x;
+    v.levels = 0;
+    v.off6[0] = (long long)n;
+    bool ok = cuda_ok(launch_threshold(&v, 1, &ts, d_thr, d_sum, threshold_form, st), "threshold");
+    cudaFreeAsync(scratch, st);
+    return ok ? 0 : -1;
+}

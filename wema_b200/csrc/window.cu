@@ -1,0 +1,110 @@
+// window.cu - the window ("--haar") temporal filter (temporal_filter.c:139-319)
+// fused with the amplification (phase_amp.c:12-56).
+//
+// The ring holds the last ws frames of every unique coefficient, slot-major
+// ([ws][Pu]), so a push is one contiguous plane copy and each thread reads
+// its position's history with coalesced loads.  For position u, with the
+// window in chronological order x_0..x_{ws-1} (oldest first, centre c = ws/2):
+//   delta = x_c - mean(x);
+//   bilateral: sigma = max(0.5 * mean|x_t - x_c|, 1e-3),
+//              w_t = exp(-(x_t-x_c)^2 / (2 sigma^2)) * exp(-(t-c)^2 / (2 (0.15 ws)^2)),
+//              delta = sum w_t (x_t - mean) / sum w_t  (if sum w_t > 1e-8).
+// The reference's vectorised reductions and vector expf order these sums
+// differently; deltas agree to a few ulp, the bar for this stage.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace wema {
+
+constexpr int WIN_THREADS = 256;
+
+__global__ void k_ring_push(const float* coef, float* ring, long long pu, int slot) {
+    float* dst = ring + (long long)slot * pu;
+    for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < pu;
+         u += (long long)gridDim.x * blockDim.x)
+        dst[u] = coef[u];
+}
+
+struct WinDev {
+    WindowParams w;
+    IirParams g;
+    const float* ring;
+    const float* coef;
+    float* amplified;
+    float* delta_out;
+    const float* thr;
+    float alpha;
+};
+
+__device__ __forceinline__ int lvl(const IirParams& p, long long u) {
+    int l = 0;
+#pragma unroll
+    for (int k = 1; k < 4; k++)
+        if (k < p.levels && u >= p.uoff[k]) l = k;
+    return l;
+}
+
+__global__ void __launch_bounds__(WIN_THREADS) k_window_amp(WinDev a) {
+    const long long pu = a.w.pu;
+    const int ws = a.w.ws, head = a.w.head, center = ws / 2;
+    const float inv_ws = __fdiv_rn(1.0f, (float)ws);
+    const float thr = *a.thr;
+    const float alpha = a.alpha;
+    for (long long u = blockIdx.x * (long long)WIN_THREADS + threadIdx.x; u < pu;
+         u += (long long)gridDim.x * WIN_THREADS) {
+        float sum = 0.0f, cur = 0.0f;
+        for (int t = 0; t < ws; t++) {
+            int slot = head + t;
+            if (slot >= ws) slot -= ws;
+            const float v = a.ring[(long long)slot * pu + u];
+            sum = __fadd_rn(sum, v);
+            if (t == center) cur = v;
+        }
+        const float mean = __fmul_rn(inv_ws, sum);
+        float d = __fadd_rn(cur, -mean);
+        if (a.w.bilateral) {
+            float mad = 0.0f;
+            for (int t = 0; t < ws; t++) {
+                int slot = head + t;
+                if (slot >= ws) slot -= ws;
+                mad = __fadd_rn(mad, fabsf(__fadd_rn(a.ring[(long long)slot * pu + u], -cur)));
+            }
+            const float sigma = fmaxf(__fmul_rn(__fmul_rn(inv_ws, 0.5f), mad), 0.001f);
+            const float inv2 = __fdiv_rn(0.5f, __fmul_rn(sigma, sigma));
+            float wsum = 0.0f, res = 0.0f;
+            for (int t = 0; t < ws; t++) {
+                int slot = head + t;
+                if (slot >= ws) slot -= ws;
+                const float v = a.ring[(long long)slot * pu + u];
+                const float df = __fadd_rn(v, -cur);
+                const float wt = __fmul_rn(expf(-__fmul_rn(__fmul_rn(df, df), inv2)), a.w.time_w[t]);
+                wsum = __fadd_rn(wsum, wt);
+                res = __fmaf_rn(wt, __fadd_rn(v, -mean), res);
+            }
+            if (wsum > 1e-8f) d = __fmul_rn(res, __fdiv_rn(1.0f, wsum));
+        }
+        const float x = a.coef[u];
+        const int l = lvl(a.g, u);
+        const float al = l == 0 ? __fmul_rn(alpha, 0.5f) : alpha;
+        if (a.delta_out) a.delta_out[u] = d;
+        a.amplified[u] = fabsf(x) > thr ? __fmaf_rn(d, al, x) : x;
+    }
+}
+
+cudaError_t launch_ring_push(const float* coef, float* ring, long long pu, int slot,
+                             cudaStream_t st) {
+    long long b = (pu + 255) / 256;
+    k_ring_push<<<(int)(b < 148 * 8 ? (b > 0 ? b : 1) : 148 * 8), 256, 0, st>>>(coef, ring, pu, slot);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_window_amp(const WindowParams& wp, const IirParams& geo, const float* ring,
+                              const float* coef, float* amplified, float* delta_out,
+                              const float* thr, float alpha, cudaStream_t st) {
+    WinDev a{wp, geo, ring, coef, amplified, delta_out, thr, alpha};
+    long long b = (wp.pu + WIN_THREADS - 1) / WIN_THREADS;
+    k_window_amp<<<(int)(b < 148 * 16 ? (b > 0 ? b : 1) : 148 * 16), WIN_THREADS, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace wema

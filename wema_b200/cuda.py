@@ -1,0 +1,176 @@
+"""ctypes binding of libwema_cuda (the product library) for tests and the
+benchmark.  Device buffers are torch CUDA tensors (torch is plumbing only:
+allocation and streams); every computation runs in the library's kernels.
+
+There is no fallback: if the library or a GPU is missing, using it raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _build
+
+READ_GRAY_IN, READ_GRAY_OUT, READ_ORIG6, READ_DELTA6, READ_AMP6, READ_LOWPASS, \
+    READ_THRESHOLD, READ_MAGSUM = range(8)
+THR_SINGLE, THR_BATCH = 0, 1
+
+
+class Config(C.Structure):
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("fps", C.c_float),
+                ("amp_factor", C.c_float), ("f_low", C.c_float), ("f_high", C.c_float),
+                ("temporal_window", C.c_int), ("edge_aware", C.c_int),
+                ("bilateral_temp", C.c_int), ("color_mode", C.c_int), ("use_iir", C.c_int),
+                ("threshold_form", C.c_int), ("device", C.c_int)]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        path = _build.cuda_lib_path()
+        if not os.path.exists(path):
+            raise RuntimeError(f"libwema_cuda not built ({path}); run __graft_entry__.build()")
+        L = C.CDLL(path)
+        vp, i, f, sz = C.c_void_p, C.c_int, C.c_float, C.c_size_t
+        L.wema_cuda_last_error.restype = C.c_char_p
+        L.wema_cuda_config_default.argtypes = [C.POINTER(Config), i, i, f]
+        L.wema_cuda_session_bytes.argtypes = [C.POINTER(Config)]
+        L.wema_cuda_session_bytes.restype = sz
+        L.wema_cuda_session_create.argtypes = [C.POINTER(Config), C.POINTER(vp)]
+        L.wema_cuda_session_destroy.argtypes = [vp]
+        L.wema_cuda_process_u8.argtypes = [vp, vp, vp, vp]
+        L.wema_cuda_process_f32.argtypes = [vp, vp, vp, vp, vp]
+        L.wema_cuda_process_host_u8.argtypes = [vp, vp, vp]
+        L.wema_cuda_session_sync.argtypes = [vp]
+        L.wema_cuda_session_frames_processed.argtypes = [vp]
+        L.wema_cuda_session_read.argtypes = [vp, i, i, vp, sz]
+        L.wema_cuda_session_read.restype = C.c_long
+        L.wema_cuda_threshold_flat.argtypes = [vp, sz, i, vp, vp, vp]
+        L.wema_cuda_set_timing.argtypes = [vp, i]
+        L.wema_cuda_stage_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
+        L.wema_cuda_set_keep_deltas.argtypes = [vp, i]
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().wema_cuda_last_error().decode()
+
+
+def _check(rc: int, what: str):
+    if rc != 0:
+        raise RuntimeError(f"{what} failed: {last_error()}")
+
+
+def make_config(width, height, fps=30.0, amp=120.0, f_low=0.5, f_high=None, window=32,
+                edge_aware=True, bilateral=False, color=False, use_iir=True,
+                threshold_form=THR_SINGLE, device=0) -> Config:
+    c = Config()
+    lib().wema_cuda_config_default(C.byref(c), int(width), int(height), float(fps))
+    c.amp_factor = float(amp)
+    c.f_low = float(f_low)
+    if f_high is not None:
+        c.f_high = float(f_high)
+    c.temporal_window = int(window)
+    c.edge_aware, c.bilateral_temp = int(bool(edge_aware)), int(bool(bilateral))
+    c.color_mode, c.use_iir = int(bool(color)), int(bool(use_iir))
+    c.threshold_form, c.device = int(threshold_form), int(device)
+    return c
+
+
+def session_bytes(**kw) -> int:
+    c = make_config(**kw)
+    return int(lib().wema_cuda_session_bytes(C.byref(c)))
+
+
+def _ptr(t) -> int:
+    return t.data_ptr() if hasattr(t, "data_ptr") else t.ctypes.data
+
+
+class Session:
+    """One video stream with device-resident state."""
+
+    def __init__(self, **kw):
+        self.cfg = make_config(**kw)
+        h = C.c_void_p()
+        _check(lib().wema_cuda_session_create(C.byref(self.cfg), C.byref(h)), "session create")
+        self.h = h
+        self.w, self.hgt = self.cfg.width, self.cfg.height
+        self.channels = 3 if self.cfg.color_mode else 1
+
+    def process_u8(self, d_in, d_out, stream=None):
+        s = stream.cuda_stream if stream is not None else None
+        _check(lib().wema_cuda_process_u8(self.h, _ptr(d_in), _ptr(d_out), s), "process_u8")
+
+    def process_f32(self, d_in, d_out_f32=None, d_out_u8=None, stream=None):
+        s = stream.cuda_stream if stream is not None else None
+        _check(lib().wema_cuda_process_f32(
+            self.h, _ptr(d_in), _ptr(d_out_f32) if d_out_f32 is not None else None,
+            _ptr(d_out_u8) if d_out_u8 is not None else None, s), "process_f32")
+
+    def process_host_u8(self, frame: np.ndarray) -> np.ndarray:
+        frame = np.ascontiguousarray(frame, np.uint8)
+        out = np.empty_like(frame)
+        _check(lib().wema_cuda_process_host_u8(self.h, frame.ctypes.data, out.ctypes.data),
+               "process_host_u8")
+        return out
+
+    def sync(self):
+        _check(lib().wema_cuda_session_sync(self.h), "sync")
+
+    @property
+    def frames_processed(self) -> int:
+        return lib().wema_cuda_session_frames_processed(self.h)
+
+    def read(self, what: int, channel: int = 0, cap: int | None = None) -> np.ndarray:
+        if cap is None:
+            cap = max(8 * self.w * self.hgt + 64, 64)
+        buf = np.empty(cap, np.float32)
+        n = lib().wema_cuda_session_read(self.h, what, channel, buf.ctypes.data, cap)
+        if n < 0:
+            raise RuntimeError(f"read failed: {last_error()}")
+        return buf[:n].copy()
+
+    STAGES = ("fwd_dwt_level0", "fwd_dwt_levels", "threshold", "temporal_amplify",
+              "inv_dwt", "luma_transfer")
+
+    def set_timing(self, enable: bool):
+        _check(lib().wema_cuda_set_timing(self.h, int(bool(enable))), "set_timing")
+
+    def stage_times(self):
+        """-> (dict stage -> total ms, frames timed)"""
+        t = (C.c_double * 6)()
+        n = C.c_longlong()
+        _check(lib().wema_cuda_stage_times(self.h, t, C.byref(n)), "stage_times")
+        return dict(zip(self.STAGES, list(t))), n.value
+
+    def keep_deltas(self, keep: bool):
+        _check(lib().wema_cuda_set_keep_deltas(self.h, int(bool(keep))), "keep_deltas")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().wema_cuda_session_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def threshold_flat(d_x, threshold_form=THR_SINGLE, stream=None):
+    """Exact reference threshold of a flat device float32 tensor -> (thr, sum)."""
+    import torch
+    out = torch.empty(2, dtype=torch.float32, device=d_x.device)
+    s = stream.cuda_stream if stream is not None else None
+    _check(lib().wema_cuda_threshold_flat(d_x.data_ptr(), d_x.numel(), threshold_form,
+                                          out.data_ptr(), out.data_ptr() + 4, s), "threshold")
+    torch.cuda.synchronize()
+    v = out.cpu().numpy()
+    return np.float32(v[0]), np.float32(v[1])
