@@ -141,13 +141,13 @@ def stage_bytes(w, h, channels, levels_dims, pu):
         sw, sh = levels_dims[l]
         rest += C * 4 * (pw * ph + 4 * sw * sh)
     thr = C * 2 * 4 * pu                               # two passes over |x|
-    temporal = C * (4 + 32 + 4) * pu                   # coef in, state in/out, amplified out
+    temporal = C * (4 + 32 + 4) * pu                   # coef in, state in/out, delta out
     inv = 0
     for l in range(len(levels_dims)):
         sw, sh = levels_dims[l]
         iw = (w if l == 0 else levels_dims[l - 1][0])
         ih = (h if l == 0 else levels_dims[l - 1][1])
-        inv += C * 4 * 4 * sw * sh                     # LL + 3 bands in
+        inv += C * 4 * sw * sh + C * 8 * 3 * sw * sh   # LL in; 3 bands: coef + delta in
         inv += (3 * P if (l == 0 and C == 3) else C * 4 * iw * ih)
     xfer = 0 if C == 3 else 3 * P + 4 * P + 3 * P      # RGB in, Y in, RGB out
     return {"fwd_dwt_level0": fwd0, "fwd_dwt_levels": rest, "threshold": thr,
@@ -260,7 +260,6 @@ def main():
     h_out = torch.empty((h, w, 3), dtype=torch.uint8).pin_memory()
 
     sess = wc.Session(width=w, height=h, device=local, **kw)
-    sess.keep_deltas(False)
     stream = torch.cuda.ExternalStream  # noqa: F841  (the session has its own stream)
     t_stream = torch.cuda.Stream(device=dev)
 

@@ -99,10 +99,6 @@ enum { WEMA_CUDA_STAGES = 6 };
 int wema_cuda_set_timing(wema_cuda_session *s, int enable);
 int wema_cuda_stage_times(wema_cuda_session *s, double *times_ms, long long *frames);
 
-/* Whether each frame's band-passed deltas are stored for
- * WEMA_CUDA_READ_DELTA6 (default 1; 0 saves one plane write per frame). */
-int wema_cuda_set_keep_deltas(wema_cuda_session *s, int keep);
-
 /* Exact reference threshold of a device array of n floats (plain flat
  * order), written to *d_thr; d_sum optional.  Allocates its scratch. */
 int wema_cuda_threshold_flat(const float *d_x, size_t n, int threshold_form, float *d_thr,

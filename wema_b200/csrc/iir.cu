@@ -1,5 +1,5 @@
 // iir.cu - per-coefficient temporal band-pass (Butterworth HP + LP biquads,
-// DF-II transposed) fused with the adaptive-threshold amplification.
+// DF-II transposed), and the adaptive-threshold amplification.
 //
 // One thread per unique detail coefficient.  The reference filters all six
 // slots, but slots 3-5 carry the same input sequence as slots 2-0 and their
@@ -10,7 +10,9 @@
 // except for positions at or past the last full 16-wide block of the 6-slot
 // array, which the reference runs in its scalar loop: w2 = fms(b2, x, a2*y)
 // (iir_filter.c:231-246).  Amplification (wema.c:726-743):
-//   out = |x| > thr ? fma(delta, alpha_l, x) : x,  alpha_0 = alpha/2.
+//   out = |x| > thr ? fma(delta, alpha_l, x) : x,  alpha_0 = alpha/2;
+// the per-frame path applies it inside the inverse DWT's staging (dwt.cu), so
+// the filter need not wait for the threshold.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -74,43 +76,28 @@ __global__ void __launch_bounds__(IIR_THREADS) k_iir_preseed(IirDev a) {
     }
 }
 
-__global__ void __launch_bounds__(IIR_THREADS) k_iir_amp(IirDev a) {
+__global__ void __launch_bounds__(IIR_THREADS) k_iir(IirDev a) {
     const long long pu = a.p.uoff[a.p.levels];
-    const float thr = *a.thr;
-    const float alpha = a.alpha;
-    const float alpha0 = __fmul_rn(alpha, 0.5f);
     for (long long u = blockIdx.x * (long long)IIR_THREADS + threadIdx.x; u < pu;
          u += (long long)gridDim.x * IIR_THREADS) {
         bool tail;
-        const int l = level_of(a.p, u, tail);
+        level_of(a.p, u, tail);
         float4 st = a.state[u];
-        const float x = a.coef[u];
-        const float d = cascade(a.p.c, st, x, tail);
-        const float al = l == 0 ? alpha0 : alpha;
-        if (a.delta_out) a.delta_out[u] = d;
-        a.amplified[u] = fabsf(x) > thr ? __fmaf_rn(d, al, x) : x;
+        a.delta_out[u] = cascade(a.p.c, st, a.coef[u], tail);
         a.state[u] = st;
     }
 }
 
-// batch route: per-frame thresholds and alphas
-__global__ void __launch_bounds__(IIR_THREADS) k_iir_amp_frames(IirDev a) {
+__global__ void __launch_bounds__(IIR_THREADS) k_amplify(IirDev a) {
     const long long pu = a.p.uoff[a.p.levels];
+    const float thr = *a.thr;
+    const float alpha0 = __fmul_rn(a.alpha, 0.5f);
     for (long long u = blockIdx.x * (long long)IIR_THREADS + threadIdx.x; u < pu;
          u += (long long)gridDim.x * IIR_THREADS) {
         bool tail;
         const int l = level_of(a.p, u, tail);
-        float4 st = a.state[u];
-        for (int f = 0; f < a.frames; f++) {
-            const long long o = f * a.frame_stride + u;
-            const float x = a.coef[o];
-            const float d = cascade(a.p.c, st, x, tail);
-            const float alpha = a.amp[f];
-            const float al = l == 0 ? __fmul_rn(alpha, 0.5f) : alpha;
-            if (a.delta_out) a.delta_out[o] = d;
-            a.amplified[o] = fabsf(x) > a.thr[f] ? __fmaf_rn(d, al, x) : x;
-        }
-        a.state[u] = st;
+        const float x = a.coef[u];
+        a.amplified[u] = fabsf(x) > thr ? __fmaf_rn(a.delta_out[u], l == 0 ? alpha0 : a.alpha, x) : x;
     }
 }
 
@@ -130,36 +117,27 @@ cudaError_t launch_iir_preseed(const IirParams& p, const float* coef, float4* st
     return cudaGetLastError();
 }
 
-cudaError_t launch_iir_amp(const IirParams& p, const float* coef, float4* state, float* amplified,
-                           float* delta_out, const float* thr, float alpha, cudaStream_t st) {
+cudaError_t launch_iir(const IirParams& p, const float* coef, float4* state, float* delta,
+                       cudaStream_t st) {
     IirDev a{};
     a.p = p;
     a.coef = coef;
-    a.frames = 1;
-    a.frame_stride = 0;
     a.state = state;
-    a.amplified = amplified;
-    a.delta_out = delta_out;
-    a.thr = thr;
-    a.alpha = alpha;
-    k_iir_amp<<<grid_for(p.uoff[p.levels]), IIR_THREADS, 0, st>>>(a);
+    a.delta_out = delta;
+    k_iir<<<grid_for(p.uoff[p.levels]), IIR_THREADS, 0, st>>>(a);
     return cudaGetLastError();
 }
 
-cudaError_t launch_iir_amp_frames(const IirParams& p, const float* coef, long long frame_stride,
-                                  int frames, float4* state, float* amplified, float* delta_out,
-                                  const float* thr, const float* amp, cudaStream_t st) {
+cudaError_t launch_amplify(const IirParams& p, const float* coef, const float* delta,
+                           const float* thr, float alpha, float* amplified, cudaStream_t st) {
     IirDev a{};
     a.p = p;
     a.coef = coef;
-    a.frames = frames;
-    a.frame_stride = frame_stride;
-    a.state = state;
-    a.amplified = amplified;
-    a.delta_out = delta_out;
+    a.delta_out = const_cast<float*>(delta);
     a.thr = thr;
-    a.amp = amp;
-    k_iir_amp_frames<<<grid_for(p.uoff[p.levels]), IIR_THREADS, 0, st>>>(a);
+    a.alpha = alpha;
+    a.amplified = amplified;
+    k_amplify<<<grid_for(p.uoff[p.levels]), IIR_THREADS, 0, st>>>(a);
     return cudaGetLastError();
 }
 

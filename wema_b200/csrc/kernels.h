@@ -30,7 +30,10 @@ struct InvLevelParams {
     int sw, sh;
     long long n;
     const float* ll[3];         // coarser reconstruction / lowpass (sw x sh)
-    const float* coef[3];       // bands LH, HH, HL
+    const float* coef[3];       // original bands LH, HH, HL of this level
+    const float* delta[3];      // band-passed deltas of the same bands
+    const float* thr;           // per-channel thresholds (device)
+    float alpha[3];             // per-channel level alpha (level 0 already halved)
     float* out_planes[3];       // reconstructed planes (kOutPlanes), optional for kOutRgb
     uint8_t* out_u8;            // kOutRgb: RGB24 output (optional)
     float* out_f32;             // kOutRgb: float RGB output (optional)
@@ -54,14 +57,17 @@ struct ThrScratch {             // device scratch, sized by thr_scratch_bytes
     double* part;               // [n_sub][8] exact-ish lane partial sums
     double* prefix;             // [n_sub][8] exclusive prefixes
     int4* cand;                 // [n_sub][8][2] binade top and monoids of 3 candidates
-    int2* cand1;                // unused
+    int* hist;                  // [n_sub][8] binade of the running sum at each sub-chunk
+                                // start, recorded by the last walk (the next frame's prediction)
 };
 size_t thr_scratch_bytes(long long n6);
 void thr_scratch_bind(ThrScratch& s, void* base, long long n6);
 // Writes thr[chan] = threshold of each of `nch` channels (single-frame form
 // (sum/N)*0.2, or batch form (0.2/N)*sum); optionally the raw sums.
+// use_hist: predict binades from scratch.hist (written by the previous call on
+// the same geometry) instead of the FP64 partial sums - skips two kernels.
 cudaError_t launch_threshold(const PyrView* views, int nch, ThrScratch* scratch, float* thr,
-                             float* sums, int batch_form, cudaStream_t st);
+                             float* sums, int batch_form, int use_hist, cudaStream_t st);
 
 // ---- IIR + amplification (iir.cu) ------------------------------------------
 struct IirParams {
@@ -75,15 +81,14 @@ struct IirParams {
 // preseed: run `warmup` iterations with the current coefficients as input
 cudaError_t launch_iir_preseed(const IirParams& p, const float* coef, float4* state, int warmup,
                                cudaStream_t st);
-// one frame: delta = cascade(coef), amplified = |coef| > thr ? fma(delta, a_l, coef) : coef
-// alpha: the channel's amplification (fade-in applied); thr: device scalar
-cudaError_t launch_iir_amp(const IirParams& p, const float* coef, float4* state, float* amplified,
-                           float* delta_out, const float* thr, float alpha, cudaStream_t st);
-// frames [0, F) of one stream: coefficients [F][Pu] frame-major, state kept
-// in registers across the frames (batch route)
-cudaError_t launch_iir_amp_frames(const IirParams& p, const float* coef, long long frame_stride,
-                                  int frames, float4* state, float* amplified, float* delta_out,
-                                  const float* thr, const float* amp, cudaStream_t st);
+// one frame: delta = cascade(coef); the amplification is applied where the
+// inverse DWT stages the coefficients (launch_dwt_inv) or by launch_amplify
+cudaError_t launch_iir(const IirParams& p, const float* coef, float4* state, float* delta,
+                       cudaStream_t st);
+// amplified = |coef| > thr ? fma(delta, alpha_l, coef) : coef over all unique
+// positions (inspection, and the batch route)
+cudaError_t launch_amplify(const IirParams& p, const float* coef, const float* delta,
+                           const float* thr, float alpha, float* amplified, cudaStream_t st);
 
 // ---- spatial filter + luma transfer (spatial.cu) ----------------------------
 struct TransferParams {
@@ -110,8 +115,7 @@ struct WindowParams {
     float time_w[256];
 };
 cudaError_t launch_ring_push(const float* coef, float* ring, long long pu, int slot, cudaStream_t st);
-cudaError_t launch_window_amp(const WindowParams& wp, const IirParams& geo, const float* ring,
-                              const float* coef, float* amplified, float* delta_out,
-                              const float* thr, float alpha, cudaStream_t st);
+cudaError_t launch_window(const WindowParams& wp, const float* ring, float* delta,
+                          cudaStream_t st);
 
 }  // namespace wema

@@ -160,6 +160,12 @@ Session::~Session() {
         cudaStreamSynchronize(stream);
         cudaStreamDestroy(stream);
     }
+    if (side) {
+        cudaStreamSynchronize(side);
+        cudaStreamDestroy(side);
+    }
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
     if (arena) cudaFree(arena);
     if (stage_u8) cudaFree(stage_u8);
     if (stage_f32) cudaFree(stage_f32);
@@ -171,10 +177,12 @@ Session::~Session() {
 bool Session::collect_timing() {
     if (!ev_pending) return true;
     ev_pending = false;
-    if (!cuda_ok(cudaEventSynchronize(ev[N_STAGE]), "event sync")) return false;
+    if (!cuda_ok(cudaEventSynchronize(ev[6]), "event sync")) return false;
+    const int from[N_STAGE] = {0, 1, 7, 2, 4, 5};
+    const int to[N_STAGE] = {1, 2, 8, 3, 5, 6};
     for (int k = 0; k < N_STAGE; k++) {
         float ms = 0.f;
-        if (cudaEventElapsedTime(&ms, ev[k], ev[k + 1]) == cudaSuccess) stage_ms[k] += ms;
+        if (cudaEventElapsedTime(&ms, ev[from[k]], ev[to[k]]) == cudaSuccess) stage_ms[k] += ms;
     }
     stage_frames++;
     return true;
@@ -208,7 +216,21 @@ bool Session::init(const wema_cuda_config& c) {
     layout(A, *this);
     if (!cuda_ok(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate"))
         return false;
+    if (!cuda_ok(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking), "cudaStreamCreate"))
+        return false;
+    if (!cuda_ok(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming), "cudaEventCreate"))
+        return false;
+    if (!cuda_ok(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming), "cudaEventCreate"))
+        return false;
     return true;
+}
+
+bool Session::materialize_amplified() {
+    for (int c = 0; c < nch; c++)
+        if (!cuda_ok(launch_amplify(ip, coef[c], delta[c], d_small + c, last_alpha[c], ampl[c], stream),
+                     "amplify"))
+            return false;
+    return cuda_ok(cudaStreamSynchronize(stream), "sync");
 }
 
 bool Session::ensure_staging() {
@@ -240,7 +262,7 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
             for (auto& e : ev)
                 if (!cuda_ok(cudaEventCreate(&e), "cudaEventCreate")) return false;
     }
-    mark(ST_FWD0, st);
+    mark(0, st);
 
     // forward DWT
     for (int l = 0; l < L; l++) {
@@ -267,18 +289,31 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
         }
         p.prev_n = l > 0 ? g.n[l - 1] : 0;
         if (!cuda_ok(launch_dwt_fwd(mode, nch, p, st), "forward DWT")) return false;
-        if (l == 0) mark(ST_FWD, st);
+        if (l == 0) mark(1, st);
     }
-    mark(ST_THR, st);
 
     PyrView views[3];
     for (int c = 0; c < nch; c++) views[c] = view(c);
+    const long long pu = g.uoff[L];
 
-    if (cfg.use_iir) {
-        if (!cuda_ok(launch_threshold(views, nch, thr_s, d_thr, d_sum, cfg.threshold_form, st),
+    // the threshold runs on the side stream while the temporal filter runs here
+    auto fork_threshold = [&]() -> bool {
+        if (!cuda_ok(cudaEventRecord(ev_fork, st), "event record")) return false;
+        if (!cuda_ok(cudaStreamWaitEvent(side, ev_fork, 0), "stream wait")) return false;
+        mark(7, side);
+        if (!cuda_ok(launch_threshold(views, nch, thr_s, d_thr, d_sum, cfg.threshold_form,
+                                      thr_hist ? 1 : 0, side),
                      "threshold"))
             return false;
-        mark(ST_TEMPORAL, st);
+        thr_hist = true;
+        mark(8, side);
+        return cuda_ok(cudaEventRecord(ev_join, side), "event record");
+    };
+
+    float alpha[3];
+    mark(2, st);
+    if (cfg.use_iir) {
+        if (!fork_threshold()) return false;
         if (frames_processed == 0) {   // iir_temporal_preseed on the first frame
             for (int c = 0; c < nch; c++)
                 if (!cuda_ok(launch_iir_preseed(ip, coef[c], state[c], warmup, st), "preseed"))
@@ -287,13 +322,11 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
         }
         const float amp = fade_amp(cfg.amp_factor, frames_processed, warmup);
         frames_processed++;
+        alpha[0] = amp;
+        alpha[1] = alpha[2] = amp * 0.5f;
         for (int c = 0; c < nch; c++)
-            if (!cuda_ok(launch_iir_amp(ip, coef[c], state[c], ampl[c], write_delta ? delta[c] : nullptr,
-                                        d_thr + c, c == 0 ? amp : amp * 0.5f, st),
-                         "IIR"))
-                return false;
+            if (!cuda_ok(launch_iir(ip, coef[c], state[c], delta[c], st), "IIR")) return false;
     } else {
-        const long long pu = g.uoff[L];
         for (int c = 0; c < nch; c++)
             if (!cuda_ok(launch_ring_push(coef[c], ring[c], pu, head, st), "ring push")) return false;
         head = (head + 1) % cfg.temporal_window;
@@ -309,10 +342,9 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
             last_passthrough = true;
             return cuda_ok(launch_passthrough(tp, st), "passthrough");
         }
-        if (!cuda_ok(launch_threshold(views, nch, thr_s, d_thr, d_sum, cfg.threshold_form, st),
-                     "threshold"))
-            return false;
-        mark(ST_TEMPORAL, st);
+        if (!fork_threshold()) return false;
+        alpha[0] = cfg.amp_factor;
+        alpha[1] = alpha[2] = cfg.amp_factor * 0.5f;
         WindowParams wp{};
         wp.pu = pu;
         wp.ws = cfg.temporal_window;
@@ -326,15 +358,14 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
             wp.time_w[t] = expf(-(d * d) * inv2);
         }
         for (int c = 0; c < nch; c++)
-            if (!cuda_ok(launch_window_amp(wp, ip, ring[c], coef[c], ampl[c],
-                                           write_delta ? delta[c] : nullptr, d_thr + c,
-                                           c == 0 ? cfg.amp_factor : cfg.amp_factor * 0.5f, st),
-                         "window filter"))
-                return false;
+            if (!cuda_ok(launch_window(wp, ring[c], delta[c], st), "window filter")) return false;
     }
+    for (int c = 0; c < nch; c++) last_alpha[c] = alpha[c];
+    mark(3, st);
+    if (!cuda_ok(cudaStreamWaitEvent(st, ev_join, 0), "stream wait")) return false;
+    mark(4, st);
 
-    mark(ST_INV, st);
-    // inverse DWT, coarse to fine
+    // inverse DWT, coarse to fine; amplification applied while staging
     for (int l = L - 1; l >= 0; l--) {
         InvLevelParams q{};
         q.ow = g.in_w[l];
@@ -342,9 +373,12 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
         q.sw = g.sw[l];
         q.sh = g.sh[l];
         q.n = g.n[l];
+        q.thr = d_thr;
         for (int c = 0; c < nch; c++) {
             q.ll[c] = (l == L - 1) ? ll[c][L - 1] : rec[c][l + 1];
-            q.coef[c] = ampl[c] + g.uoff[l];
+            q.coef[c] = coef[c] + g.uoff[l];
+            q.delta[c] = delta[c] + g.uoff[l];
+            q.alpha[c] = l == 0 ? alpha[c] * 0.5f : alpha[c];
             q.out_planes[c] = rec[c][l];
         }
         int mode = kOutPlanes;
@@ -355,7 +389,7 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
         }
         if (!cuda_ok(launch_dwt_inv(nch, mode, q, st), "inverse DWT")) return false;
     }
-    mark(ST_XFER, st);
+    mark(5, st);
     if (nch == 1) {
         TransferParams tp{};
         tp.w = g.w;
@@ -369,7 +403,7 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
         tp.edge_aware = cfg.edge_aware;
         if (!cuda_ok(launch_transfer(tp, st), "luma transfer")) return false;
     }
-    mark(N_STAGE, st);
+    mark(6, st);
     ev_pending = timing;
     return true;
 }
@@ -481,7 +515,8 @@ WEMA_API long wema_cuda_session_read(wema_cuda_session* s, int what, int channel
     Session& S = s->s;
     if (channel < 0 || channel >= S.nch) { set_error("bad channel"); return -1; }
     if (!cuda_ok(cudaSetDevice(S.cfg.device), "cudaSetDevice")) return -1;
-    if (!cuda_ok(cudaDeviceSynchronize(), "sync")) return -1;
+    if (!cuda_ok(cudaStreamSynchronize(S.stream), "sync")) return -1;
+    if (!cuda_ok(cudaStreamSynchronize(S.side), "sync")) return -1;
     const Geom& g = S.g;
     const long long pu = g.uoff[g.levels], n6 = g.off6[g.levels];
     auto rd = [&](const float* src, size_t n) -> long {
@@ -507,7 +542,9 @@ WEMA_API long wema_cuda_session_read(wema_cuda_session* s, int what, int channel
         case WEMA_CUDA_READ_GRAY_OUT: return rd(S.rec[channel][0], g.pixels);
         case WEMA_CUDA_READ_ORIG6: return rd6(S.coef[channel]);
         case WEMA_CUDA_READ_DELTA6: return rd6(S.delta[channel]);
-        case WEMA_CUDA_READ_AMP6: return rd6(S.ampl[channel]);
+        case WEMA_CUDA_READ_AMP6:
+            if (!S.materialize_amplified()) return -1;
+            return rd6(S.ampl[channel]);
         case WEMA_CUDA_READ_LOWPASS: return rd(S.ll[channel][g.levels - 1], g.low_n);
         case WEMA_CUDA_READ_THRESHOLD: return rd(S.d_small, S.nch);
         case WEMA_CUDA_READ_MAGSUM: return rd(S.d_small + 4, S.nch);
@@ -539,13 +576,6 @@ WEMA_API int wema_cuda_stage_times(wema_cuda_session* s, double* times_ms, long 
     return 0;
 }
 
-WEMA_API int wema_cuda_set_keep_deltas(wema_cuda_session* s, int keep) {
-    clear_error();
-    if (!s) { set_error("null session"); return -1; }
-    s->s.write_delta = keep != 0;
-    return 0;
-}
-
 WEMA_API int wema_cuda_threshold_flat(const float* d_x, size_t n, int threshold_form, float* d_thr,
                                       float* d_sum, void* cuda_stream) {
     clear_error();
@@ -560,7 +590,7 @@ WEMA_API int wema_cuda_threshold_flat(const float* d_x, size_t n, int threshold_
     v.coef = d_x;
     v.levels = 0;
     v.off6[0] = (long long)n;
-    bool ok = cuda_ok(launch_threshold(&v, 1, &ts, d_thr, d_sum, threshold_form, st), "threshold");
+    bool ok = cuda_ok(launch_threshold(&v, 1, &ts, d_thr, d_sum, threshold_form, 0, st), "threshold");
     cudaFreeAsync(scratch, st);
     return ok ? 0 : -1;
 }

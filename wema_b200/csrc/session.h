@@ -35,6 +35,10 @@ public:
     int head = 0, filled = 0;          // window ring
     bool last_passthrough = false;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;       // threshold branch, joined before the inverse
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    float last_alpha[3] = {};          // per-channel alpha of the last frame
+    bool thr_hist = false;             // threshold scratch holds the last frame's binades
 
     // device arena
     void* arena = nullptr;
@@ -49,15 +53,18 @@ public:
     float* ring[3] = {};
     ThrScratch thr_s[3] = {};
     float* d_small = nullptr;          // thr[3], sum[3]
-    bool write_delta = true;           // keep per-frame deltas (inspection)
     // per-stage timing (CUDA events), enabled on demand
     enum { ST_FWD0, ST_FWD, ST_THR, ST_TEMPORAL, ST_INV, ST_XFER, N_STAGE };
+    // events: 0 fwd0, 1 fwd levels, 2 temporal start, 3 temporal end, 4 inverse
+    // start (after the join), 5 transfer start, 6 end, 7/8 threshold begin/end
+    enum { N_EV = 9 };
     bool timing = false;
-    cudaEvent_t ev[N_STAGE + 1] = {};
+    cudaEvent_t ev[N_EV] = {};
     bool ev_pending = false;
     double stage_ms[N_STAGE] = {};
     long long stage_frames = 0;
     void mark(int k, cudaStream_t st) { if (timing) cudaEventRecord(ev[k], st); }
+    bool materialize_amplified();      // ampl[] = amplified coefficients of the last frame
     bool collect_timing();
     // host-API staging (allocated on first use)
     uint8_t* stage_u8 = nullptr;       // in [3P] + out [3P]

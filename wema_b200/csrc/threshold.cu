@@ -20,6 +20,9 @@
 //   thr_partials  - per (sub-chunk, lane) FP64 sum of |x| (exact enough to
 //                   predict the binade of s at each sub-chunk start);
 //   thr_prefix    - exclusive FP64 prefix per lane;
+//                   (both skipped when the previous frame's walk recorded the
+//                   binade at every sub-chunk start: a video's coefficient
+//                   statistics move slowly, and a wrong guess only costs time)
 //   thr_monoids   - per (sub-chunk, lane) monoids for the three binades
 //                   around the predicted one;
 //   thr_walk      - one warp per lane composes 32 sub-chunks at a time by a
@@ -70,19 +73,72 @@ __device__ __forceinline__ float from_m(int m, int eb) {
     return __uint_as_float(((uint32_t)eb << 23) | ((uint32_t)m & 0x7FFFFFu));
 }
 
-// |element| of the 6-slot flat array at index i (slots 3-5 mirror 2-0);
-// levels == 0 views coef as a plain flat array of off6[0] elements
-__device__ __forceinline__ uint32_t v6_bits(const PyrView& v, long long i) {
-    if (v.levels == 0) return __float_as_uint(v.coef[i]) & 0x7FFFFFFFu;   // plain flat array
+// Sequential reader of |element| of the 6-slot flat array (slots 3-5 mirror
+// 2-0).  seek() places it on the (level, slot) segment holding index i; get()
+// advances segment by segment, so a run of nearby indices costs one division.
+// levels == 0 views coef as a plain flat array of off6[0] elements.
+struct Cursor {
+    const float* base;           // element at seg0
+    long long seg0, seg1;        // current segment [seg0, seg1)
+    int l, slot;
+};
+
+__device__ __forceinline__ void cur_set(const PyrView& v, Cursor& c) {
+    const int band = c.slot < 3 ? c.slot : 5 - c.slot;
+    c.seg0 = v.off6[c.l] + c.slot * v.n[c.l];
+    c.seg1 = c.seg0 + v.n[c.l];
+    c.base = v.coef + v.uoff[c.l] + band * v.n[c.l];
+}
+
+__device__ __forceinline__ void cur_seek(const PyrView& v, Cursor& c, long long i) {
+    if (v.levels == 0) {
+        c.base = v.coef;
+        c.seg0 = 0;
+        c.seg1 = 0x7fffffffffffffffLL;
+        return;
+    }
     int l = 0;
 #pragma unroll
     for (int k = 1; k < 4; k++)
         if (k < v.levels && i >= v.off6[k]) l = k;
+    c.l = l;
     const long long r = i - v.off6[l];
-    const int slot = (int)(r / v.n[l]);
-    const long long k = r - (long long)slot * v.n[l];
-    const int band = slot < 3 ? slot : 5 - slot;
-    return __float_as_uint(v.coef[v.uoff[l] + band * v.n[l] + k]) & 0x7FFFFFFFu;
+    c.slot = (r < 0x7fffffffLL && v.n[l] < 0x7fffffffLL) ? (int)((int)r / (int)v.n[l])
+                                                           : (int)(r / v.n[l]);
+    if (c.slot > 5) c.slot = 5;
+    cur_set(v, c);
+}
+
+__device__ __forceinline__ const float* cur_addr(const PyrView& v, Cursor& c, long long i) {
+    while (i >= c.seg1) {
+        if (++c.slot == 6) { c.slot = 0; c.l++; }
+        cur_set(v, c);
+    }
+    return c.base + (i - c.seg0);
+}
+
+__device__ __forceinline__ uint32_t cur_get(const PyrView& v, Cursor& c, long long i) {
+    return __float_as_uint(*cur_addr(v, c, i)) & 0x7FFFFFFFu;
+}
+
+// |x| bits of the EPT lane-elements t0 .. t0+EPT-1 of lane j: all addresses
+// first, then all loads, so they are in flight together
+template <int EPT>
+__device__ __forceinline__ void load_run(const PyrView& v, long long nlane, long long t0, int j,
+                                         uint32_t (&out)[EPT]) {
+    const float* addr[EPT];
+    Cursor cu;
+    if (t0 < nlane) cur_seek(v, cu, 8 * t0 + j);
+#pragma unroll
+    for (int k = 0; k < EPT; k++) addr[k] = (t0 + k < nlane) ? cur_addr(v, cu, 8 * (t0 + k) + j) : nullptr;
+#pragma unroll
+    for (int k = 0; k < EPT; k++) out[k] = addr[k] ? (__float_as_uint(__ldg(addr[k])) & 0x7FFFFFFFu) : 0u;
+}
+
+__device__ __forceinline__ uint32_t v6_bits(const PyrView& v, long long i) {
+    Cursor c;
+    cur_seek(v, c, i);
+    return cur_get(v, c, i);
 }
 
 struct ThrGeom {
@@ -104,7 +160,7 @@ __host__ __device__ inline ThrGeom thr_geom(long long n6) {
 size_t thr_scratch_bytes(long long n6) {
     ThrGeom g = thr_geom(n6);
     size_t per = (size_t)g.nsub * LANES;
-    return per * (sizeof(double) * 2 + sizeof(int4) * 2) + 256;
+    return per * (sizeof(double) * 2 + sizeof(int4) * 2 + sizeof(int)) + 256;
 }
 
 void thr_scratch_bind(ThrScratch& s, void* base, long long n6) {
@@ -113,8 +169,8 @@ void thr_scratch_bind(ThrScratch& s, void* base, long long n6) {
     char* p = (char*)base;
     s.part = (double*)p;   p += per * sizeof(double);
     s.prefix = (double*)p; p += per * sizeof(double);
-    s.cand = (int4*)p;     // two int4 per (sub-chunk, lane)
-    s.cand1 = nullptr;
+    s.cand = (int4*)p;     p += per * 2 * sizeof(int4);   // two int4 per (sub-chunk, lane)
+    s.hist = (int*)p;
 }
 
 struct ThrArgs {
@@ -123,6 +179,7 @@ struct ThrArgs {
     float* thr;
     float* sums;
     int batch_form;
+    int use_hist;
 };
 
 // ---- partial sums: thread (lane j, block tb) covers G/32 lane-elements
@@ -134,12 +191,11 @@ __global__ void __launch_bounds__(THR_THREADS) k_thr_partials(ThrArgs a) {
     const int sub = blockIdx.x;
     const int j = threadIdx.x & 7, tb = threadIdx.x >> 3;
     const long long t0 = (long long)sub * g.G + (long long)tb * EPT;
+    uint32_t val[EPT];
+    load_run<EPT>(v, g.nlane, t0, j, val);
     double acc = 0.0;
 #pragma unroll
-    for (int k = 0; k < EPT; k++) {
-        const long long t = t0 + k;
-        if (t < g.nlane) acc += (double)__uint_as_float(v6_bits(v, 8 * t + j));
-    }
+    for (int k = 0; k < EPT; k++) acc += (double)__uint_as_float(val[k]);
     acc += __shfl_xor_sync(0xffffffffu, acc, 8);
     acc += __shfl_xor_sync(0xffffffffu, acc, 16);
     __shared__ double ws[8][8];
@@ -153,27 +209,48 @@ __global__ void __launch_bounds__(THR_THREADS) k_thr_partials(ThrArgs a) {
     }
 }
 
-// ---- exclusive prefix per lane (warp j scans lane j)
+// ---- exclusive prefix per lane: one CTA per (lane, channel), 8 entries per
+// thread per pass, block-wide scan in shared memory
 __global__ void __launch_bounds__(THR_THREADS) k_thr_prefix(ThrArgs a) {
-    const int ch = blockIdx.x;
+    const int j = blockIdx.x, ch = blockIdx.y;
     const PyrView& v = a.v[ch];
     const ThrGeom g = thr_geom(v.off6[v.levels]);
-    const int j = threadIdx.x >> 5, ln = threadIdx.x & 31;
-    const int per = (g.nsub + 31) / 32;
-    const int c0 = ln * per, c1 = min(c0 + per, g.nsub);
     const double* part = a.s[ch].part;
-    double local = 0.0;
-    for (int c = c0; c < c1; c++) local += part[(long long)c * LANES + j];
-    double incl = local;
-    for (int d = 1; d < 32; d <<= 1) {
-        double o = __shfl_up_sync(0xffffffffu, incl, d);
-        if (ln >= d) incl += o;
-    }
-    double run = incl - local;
     double* pre = a.s[ch].prefix;
-    for (int c = c0; c < c1; c++) {
-        pre[(long long)c * LANES + j] = run;
-        run += part[(long long)c * LANES + j];
+    __shared__ double wsum[THR_THREADS / 32];
+    __shared__ double carry_s;
+    double carry = 0.0;
+    const int ln = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int base = 0; base < g.nsub; base += THR_THREADS * 8) {
+        double x[8];
+        double local = 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const int c = base + threadIdx.x * 8 + k;
+            x[k] = c < g.nsub ? part[(long long)c * LANES + j] : 0.0;
+            local += x[k];
+        }
+        double incl = local;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const double o = __shfl_up_sync(0xffffffffu, incl, d);
+            if (ln >= d) incl += o;
+        }
+        if (ln == 31) wsum[warp] = incl;
+        __syncthreads();
+        double wpre = 0.0;
+        for (int w = 0; w < warp; w++) wpre += wsum[w];
+        double run = carry + wpre + incl - local;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const int c = base + threadIdx.x * 8 + k;
+            if (c < g.nsub) pre[(long long)c * LANES + j] = run;
+            run += x[k];
+        }
+        if (threadIdx.x == THR_THREADS - 1) carry_s = run;
+        __syncthreads();
+        carry = carry_s;
+        __syncthreads();
     }
 }
 
@@ -190,16 +267,19 @@ __global__ void __launch_bounds__(THR_THREADS) k_thr_monoids(ThrArgs a) {
     const ThrGeom g = thr_geom(v.off6[v.levels]);
     const int sub = blockIdx.x;
     const int j = threadIdx.x & 7, tb = threadIdx.x >> 3;
-    const int etop = predicted_top_binade(a.s[ch].prefix[(long long)sub * LANES + j]);
+    const int etop = a.use_hist ? a.s[ch].hist[(long long)sub * LANES + j] + 1
+                                : predicted_top_binade(a.s[ch].prefix[(long long)sub * LANES + j]);
     Mono m[NCAND];
 #pragma unroll
     for (int c = 0; c < NCAND; c++) m[c] = mono_id();
     const long long t0 = (long long)sub * g.G + (long long)tb * EPT;
+    uint32_t val[EPT];
+    load_run<EPT>(v, g.nlane, t0, j, val);
 #pragma unroll
     for (int k = 0; k < EPT; k++) {
         const long long t = t0 + k;
         if (t < g.nlane) {
-            const uint32_t ua = v6_bits(v, 8 * t + j);
+            const uint32_t ua = val[k];
 #pragma unroll
             for (int c = 0; c < NCAND; c++) m[c] = compose(m[c], elem_mono(ua, etop - c));
         }
@@ -251,12 +331,7 @@ __device__ __forceinline__ Mono warp_scan(Mono t, int ln) {
 template <int EPT>
 __device__ float resolve_sub(const PyrView& v, const ThrGeom& g, int j, int sub, float s, int ln) {
     uint32_t val[EPT];
-    const long long t0 = (long long)sub * g.G + (long long)ln * EPT;
-#pragma unroll
-    for (int k = 0; k < EPT; k++) {
-        const long long t = t0 + k;
-        val[k] = t < g.nlane ? v6_bits(v, 8 * t + j) : 0u;
-    }
+    load_run<EPT>(v, g.nlane, (long long)sub * g.G + (long long)ln * EPT, j, val);
     int pos = 0;
     while (pos < 32) {
         const uint32_t sb = __float_as_uint(s);
@@ -297,53 +372,103 @@ __device__ float resolve_sub(const PyrView& v, const ThrGeom& g, int j, int sub,
     return s;
 }
 
+// monoid of a sub-chunk for binade eb from its stored candidates, if present
+__device__ __forceinline__ bool cand_mono(const int4& k0, const int4& k1, int eb, Mono& m) {
+    const int dlt = k0.x - eb;
+    if (k0.x <= 0 || dlt < 0 || dlt >= NCAND) return false;
+    if (dlt == 0) m = {k0.y, k0.z};
+    else if (dlt == 1) m = {k0.w, k1.x};
+    else m = {k1.y, k1.z};
+    return true;
+}
+
+constexpr int SPT = 4;                // sub-chunks per lane-thread in a walk window
+constexpr int WIN = 32 * SPT;
+
 template <int EPT>
-__global__ void __launch_bounds__(THR_THREADS) k_thr_walk(ThrArgs a) {
+__global__ void __launch_bounds__(THR_THREADS, 1) k_thr_walk(ThrArgs a) {
     const int ch = blockIdx.x;
     const PyrView& v = a.v[ch];
     const ThrGeom g = thr_geom(v.off6[v.levels]);
     const int j = threadIdx.x >> 5, ln = threadIdx.x & 31;
     const int4* cand = a.s[ch].cand;
     float s = 0.0f;
-    for (int c0 = 0; c0 < g.nsub; c0 += 32) {
-        const int c = c0 + ln;
-        const int wend = min(32, g.nsub - c0);
-        int4 k0 = make_int4(0, 0, 0, 0), k1 = make_int4(0, 0, 0, 0);
-        if (c < g.nsub) {
-            k0 = cand[2 * ((long long)c * LANES + j)];
-            k1 = cand[2 * ((long long)c * LANES + j) + 1];
+    int4 k0[SPT], k1[SPT], n0[SPT], n1[SPT];
+    auto load = [&](int c0, int4* K0, int4* K1) {
+#pragma unroll
+        for (int q = 0; q < SPT; q++) {
+            const int c = c0 + ln * SPT + q;
+            if (c < g.nsub) {
+                K0[q] = cand[2 * ((long long)c * LANES + j)];
+                K1[q] = cand[2 * ((long long)c * LANES + j) + 1];
+            } else {
+                K0[q] = make_int4(0, 0, 0, 0);
+                K1[q] = make_int4(0, 0, 0, 0);
+            }
         }
+    };
+    if (g.nsub > 0) load(0, k0, k1);
+    for (int c0 = 0; c0 < g.nsub; c0 += WIN) {
+        if (c0 + WIN < g.nsub) load(c0 + WIN, n0, n1);   // prefetch the next window
+        const int wend = min(WIN, g.nsub - c0);
+        const int my0 = ln * SPT;
         int off = 0;
         while (off < wend) {
             const uint32_t sb = __float_as_uint(s);
             const int eb = sb >> 23;
-            if (eb == 0) {
+            if (eb == 0) {   // zero / subnormal running sum: exact element walk
+                if (ln == 0) a.s[ch].hist[(long long)(c0 + off) * LANES + j] = 0;
                 s = resolve_sub<EPT>(v, g, j, c0 + off, s, ln);
                 off++;
                 continue;
             }
             const int m = (sb & 0x7FFFFF) | 0x800000;
-            const int dlt = k0.x - eb;   // which candidate (0 = top) describes binade eb
-            bool has = ln >= off && ln < wend && k0.x > 0 && dlt >= 0 && dlt < NCAND;
+            int* hist = a.s[ch].hist + j;
+            // my sub-chunks' composition, up to my first missing candidate
             Mono t = mono_id();
-            if (has) {
-                if (dlt == 0) t = {k0.y, k0.z};
-                else if (dlt == 1) t = {k0.w, k1.x};
-                else t = {k1.y, k1.z};
+#pragma unroll
+            for (int q = 0; q < SPT; q++) {
+                const int r = my0 + q;
+                if (r >= off && r < wend) {
+                    Mono mq;
+                    if (!cand_mono(k0[q], k1[q], eb, mq)) break;
+                    t = compose(t, mq);
+                }
             }
-            const unsigned miss = __ballot_sync(0xffffffffu, ln >= off && ln < wend && !has);
-            const int lim = miss ? __ffs(miss) - 1 : wend;
-            t = warp_scan(t, ln);
-            const int mend = m + ((m & 1) ? t.d1 : t.d0);
-            const unsigned cross = __ballot_sync(0xffffffffu, ln >= off && ln < lim && mend >= (1 << 24));
-            const int stop = cross ? min(lim, __ffs(cross) - 1) : lim;
-            if (stop > off) s = from_m(__shfl_sync(0xffffffffu, mend, stop - 1), eb);
-            off = stop;
-            if (off < wend) {
-                s = resolve_sub<EPT>(v, g, j, c0 + off, s, ln);
-                off++;
+            const Mono incl = warp_scan(t, ln);
+            Mono ex;
+            ex.d0 = __shfl_up_sync(0xffffffffu, incl.d0, 1);
+            ex.d1 = __shfl_up_sync(0xffffffffu, incl.d1, 1);
+            if (ln == 0) ex = mono_id();
+            // exact m at my first sub-chunk, valid if nothing went wrong before it
+            int mm = m + ((m & 1) ? ex.d1 : ex.d0);
+            int stop = 0x7fffffff;
+#pragma unroll
+            for (int q = 0; q < SPT; q++) {
+                const int r = my0 + q;
+                if (r < off || r >= wend || stop != 0x7fffffff) continue;
+                Mono mq;
+                if (!cand_mono(k0[q], k1[q], eb, mq)) { stop = r; continue; }
+                const int mn = mm + ((mm & 1) ? mq.d1 : mq.d0);
+                if (mn >= (1 << 24)) { stop = r; continue; }
+                mm = mn;
+                hist[(long long)(c0 + r) * LANES] = eb;   // accepted: starts in binade eb
             }
+            int first = stop;
+#pragma unroll
+            for (int d = 16; d >= 1; d >>= 1) first = min(first, __shfl_xor_sync(0xffffffffu, first, d));
+            if (first == 0x7fffffff) {   // the rest of the window stays in this binade
+                s = from_m(__shfl_sync(0xffffffffu, mm, (wend - 1) / SPT), eb);
+                break;
+            }
+            const int mp = __shfl_sync(0xffffffffu, mm, first / SPT);
+            if (first > off) s = from_m(mp, eb);
+            if (ln == 0) hist[(long long)(c0 + first) * LANES] = eb;
+            s = resolve_sub<EPT>(v, g, j, c0 + first, s, ln);
+            off = first + 1;
         }
+#pragma unroll
+        for (int q = 0; q < SPT; q++) { k0[q] = n0[q]; k1[q] = n1[q]; }
     }
     __shared__ float lane_sum[LANES];
     if (ln == 0) lane_sum[j] = s;
@@ -375,8 +500,10 @@ __global__ void __launch_bounds__(THR_THREADS) k_thr_walk(ThrArgs a) {
 template <int EPT>
 static cudaError_t thr_launch(const ThrArgs& a, int nch, int nsub_max, cudaStream_t st) {
     if (nsub_max > 0) {
-        k_thr_partials<EPT><<<dim3(nsub_max, nch), THR_THREADS, 0, st>>>(a);
-        k_thr_prefix<<<nch, THR_THREADS, 0, st>>>(a);
+        if (!a.use_hist) {
+            k_thr_partials<EPT><<<dim3(nsub_max, nch), THR_THREADS, 0, st>>>(a);
+            k_thr_prefix<<<dim3(LANES, nch), THR_THREADS, 0, st>>>(a);
+        }
         k_thr_monoids<EPT><<<dim3(nsub_max, nch), THR_THREADS, 0, st>>>(a);
     }
     k_thr_walk<EPT><<<nch, THR_THREADS, 0, st>>>(a);
@@ -384,7 +511,7 @@ static cudaError_t thr_launch(const ThrArgs& a, int nch, int nsub_max, cudaStrea
 }
 
 cudaError_t launch_threshold(const PyrView* views, int nch, ThrScratch* scratch, float* thr,
-                             float* sums, int batch_form, cudaStream_t st) {
+                             float* sums, int batch_form, int use_hist, cudaStream_t st) {
     if (nch < 1 || nch > 3) return cudaErrorInvalidValue;
     ThrArgs a{};
     int G = 0;
@@ -398,6 +525,7 @@ cudaError_t launch_threshold(const PyrView* views, int nch, ThrScratch* scratch,
     a.thr = thr;
     a.sums = sums;
     a.batch_form = batch_form;
+    a.use_hist = use_hist;
     const int nsub = thr_geom(views[0].off6[views[0].levels]).nsub;
     switch (G) {
         case 256: return thr_launch<8>(a, nch, nsub, st);

@@ -1,5 +1,6 @@
-// window.cu - the window ("--haar") temporal filter (temporal_filter.c:139-319)
-// fused with the amplification (phase_amp.c:12-56).
+// window.cu - the window ("--haar") temporal filter (temporal_filter.c:139-319);
+// its deltas are amplified like the IIR's (phase_amp.c:12-56) where the
+// inverse DWT stages the coefficients.
 //
 // The ring holds the last ws frames of every unique coefficient, slot-major
 // ([ws][Pu]), so a push is one contiguous plane copy and each thread reads
@@ -27,29 +28,14 @@ __global__ void k_ring_push(const float* coef, float* ring, long long pu, int sl
 
 struct WinDev {
     WindowParams w;
-    IirParams g;
     const float* ring;
-    const float* coef;
-    float* amplified;
     float* delta_out;
-    const float* thr;
-    float alpha;
 };
 
-__device__ __forceinline__ int lvl(const IirParams& p, long long u) {
-    int l = 0;
-#pragma unroll
-    for (int k = 1; k < 4; k++)
-        if (k < p.levels && u >= p.uoff[k]) l = k;
-    return l;
-}
-
-__global__ void __launch_bounds__(WIN_THREADS) k_window_amp(WinDev a) {
+__global__ void __launch_bounds__(WIN_THREADS) k_window(WinDev a) {
     const long long pu = a.w.pu;
     const int ws = a.w.ws, head = a.w.head, center = ws / 2;
     const float inv_ws = __fdiv_rn(1.0f, (float)ws);
-    const float thr = *a.thr;
-    const float alpha = a.alpha;
     for (long long u = blockIdx.x * (long long)WIN_THREADS + threadIdx.x; u < pu;
          u += (long long)gridDim.x * WIN_THREADS) {
         float sum = 0.0f, cur = 0.0f;
@@ -83,11 +69,7 @@ __global__ void __launch_bounds__(WIN_THREADS) k_window_amp(WinDev a) {
             }
             if (wsum > 1e-8f) d = __fmul_rn(res, __fdiv_rn(1.0f, wsum));
         }
-        const float x = a.coef[u];
-        const int l = lvl(a.g, u);
-        const float al = l == 0 ? __fmul_rn(alpha, 0.5f) : alpha;
-        if (a.delta_out) a.delta_out[u] = d;
-        a.amplified[u] = fabsf(x) > thr ? __fmaf_rn(d, al, x) : x;
+        a.delta_out[u] = d;
     }
 }
 
@@ -98,12 +80,11 @@ cudaError_t launch_ring_push(const float* coef, float* ring, long long pu, int s
     return cudaGetLastError();
 }
 
-cudaError_t launch_window_amp(const WindowParams& wp, const IirParams& geo, const float* ring,
-                              const float* coef, float* amplified, float* delta_out,
-                              const float* thr, float alpha, cudaStream_t st) {
-    WinDev a{wp, geo, ring, coef, amplified, delta_out, thr, alpha};
+cudaError_t launch_window(const WindowParams& wp, const float* ring, float* delta,
+                          cudaStream_t st) {
+    WinDev a{wp, ring, delta};
     long long b = (wp.pu + WIN_THREADS - 1) / WIN_THREADS;
-    k_window_amp<<<(int)(b < 148 * 16 ? (b > 0 ? b : 1) : 148 * 16), WIN_THREADS, 0, st>>>(a);
+    k_window<<<(int)(b < 148 * 16 ? (b > 0 ? b : 1) : 148 * 16), WIN_THREADS, 0, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -53,7 +53,6 @@ def lib() -> C.CDLL:
         L.wema_cuda_threshold_flat.argtypes = [vp, sz, i, vp, vp, vp]
         L.wema_cuda_set_timing.argtypes = [vp, i]
         L.wema_cuda_stage_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
-        L.wema_cuda_set_keep_deltas.argtypes = [vp, i]
         _lib = L
     return _lib
 
@@ -148,9 +147,6 @@ class Session:
         n = C.c_longlong()
         _check(lib().wema_cuda_stage_times(self.h, t, C.byref(n)), "stage_times")
         return dict(zip(self.STAGES, list(t))), n.value
-
-    def keep_deltas(self, keep: bool):
-        _check(lib().wema_cuda_set_keep_deltas(self.h, int(bool(keep))), "keep_deltas")
 
     def close(self):
         if getattr(self, "h", None):
