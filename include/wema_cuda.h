@@ -104,6 +104,21 @@ int wema_cuda_stage_times(wema_cuda_session *s, double *times_ms, long long *fra
 int wema_cuda_threshold_flat(const float *d_x, size_t n, int threshold_form, float *d_thr,
                              float *d_sum, void *cuda_stream);
 
+/* The same exact threshold with no device allocation (no counterpart in the
+ * reference: it exists for callers that must not allocate device memory,
+ * e.g. a host that owns the GPU's memory through its own pool or a real-time
+ * loop that cannot absorb cudaMalloc's synchronisation).  Its scratch is a
+ * fixed 1 MiB array compiled into the library, held by every device that
+ * loads it; n is limited to 2^24 elements (more than a 3840x2160 frame's
+ * 6-slot coefficients) and larger n is rejected.  The first call on a device
+ * looks up that array's device address (with the device current); make it
+ * before any stream capture.  All calls on a device share the array, so calls
+ * whose work overlaps on the GPU race with each other: order them on one
+ * stream or synchronise between them.  Nothing in the array needs to start
+ * zeroed. */
+int wema_cuda_threshold_flat_noalloc(const float *d_x, size_t n, int threshold_form,
+                                     float *d_thr, float *d_sum, void *cuda_stream);
+
 /* Message of the last failure on this thread ("" if none). */
 const char *wema_cuda_last_error(void);
 

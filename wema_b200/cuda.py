@@ -51,6 +51,7 @@ def lib() -> C.CDLL:
         L.wema_cuda_session_read.argtypes = [vp, i, i, vp, sz]
         L.wema_cuda_session_read.restype = C.c_long
         L.wema_cuda_threshold_flat.argtypes = [vp, sz, i, vp, vp, vp]
+        L.wema_cuda_threshold_flat_noalloc.argtypes = [vp, sz, i, vp, vp, vp]
         L.wema_cuda_set_timing.argtypes = [vp, i]
         L.wema_cuda_stage_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
         _lib = L
@@ -167,6 +168,20 @@ def threshold_flat(d_x, threshold_form=THR_SINGLE, stream=None):
     s = stream.cuda_stream if stream is not None else None
     _check(lib().wema_cuda_threshold_flat(d_x.data_ptr(), d_x.numel(), threshold_form,
                                           out.data_ptr(), out.data_ptr() + 4, s), "threshold")
+    torch.cuda.synchronize()
+    v = out.cpu().numpy()
+    return np.float32(v[0]), np.float32(v[1])
+
+
+def threshold_flat_noalloc(d_x, threshold_form=THR_SINGLE, stream=None):
+    """As threshold_flat, through the entry point that allocates nothing
+    (scratch in a fixed device array inside the library) -> (thr, sum)."""
+    import torch
+    out = torch.empty(2, dtype=torch.float32, device=d_x.device)
+    s = stream.cuda_stream if stream is not None else None
+    _check(lib().wema_cuda_threshold_flat_noalloc(d_x.data_ptr(), d_x.numel(), threshold_form,
+                                                  out.data_ptr(), out.data_ptr() + 4, s),
+           "threshold (no-alloc)")
     torch.cuda.synchronize()
     v = out.cpu().numpy()
     return np.float32(v[0]), np.float32(v[1])
