@@ -257,14 +257,19 @@ def main():
     S.SynthVideo(spec).frames(0, nuniq, out=host.numpy())
     d_frames = host.to(dev)
     d_out = torch.empty((h, w, 3), dtype=torch.uint8, device=dev)
-    h_out = torch.empty((h, w, 3), dtype=torch.uint8).pin_memory()
 
-    sess = wc.Session(width=w, height=h, device=local, **kw)
-    stream = torch.cuda.ExternalStream  # noqa: F841  (the session has its own stream)
+    sess = wc.Session(width=w, height=h, device=local, inspect=False, **kw)
     t_stream = torch.cuda.Stream(device=dev)
 
     def frame(i):
         return d_frames[i % nuniq]
+
+    def ev():
+        # torch creates the CUDA event on its first record; the library then
+        # re-records it on its own streams
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(t_stream)
+        return e
 
     # warm-up (includes the first frame's IIR preseed)
     for i in range(a.warmup):
@@ -276,15 +281,18 @@ def main():
             dist.barrier()
         torch.cuda.synchronize(dev)
 
-    # ---- value: inputs resident in HBM
+    # ---- value: inputs resident in HBM; frames issued back to back (the
+    # session overlaps frame t+1's forward transform and filter with frame
+    # t's threshold and inverse); device time from an event the first frame
+    # waits on to the event the last frame records
     k0 = a.warmup
     barrier()
     with ClockSampler(local) as clk:
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0, ev1 = ev(), ev()
         ev0.record(t_stream)
         for i in range(a.steps):
-            sess.process_u8(frame(k0 + i), d_out, stream=t_stream)
-        ev1.record(t_stream)
+            sess.process_u8_async(frame(k0 + i), d_out, wait_event=ev0 if i == 0 else None,
+                                  done_event=ev1 if i == a.steps - 1 else None)
         ev1.synchronize()
         ms = ev0.elapsed_time(ev1)
     barrier()
@@ -299,18 +307,35 @@ def main():
     sess.set_timing(False)
     torch.cuda.synchronize(dev)
 
-    # ---- e2e through the C ABI from pinned host buffers
+    # ---- e2e through the C ABI from pinned host frames: a ring of R device
+    # buffers; H2D on one copy stream, D2H on another, each gated by the
+    # library's per-frame done event
     k2 = k1 + a.steps
-    d_in = torch.empty((h, w, 3), dtype=torch.uint8, device=dev)
+    R = 3
+    d_in = [torch.empty((h, w, 3), dtype=torch.uint8, device=dev) for _ in range(R)]
+    d_o = [torch.empty((h, w, 3), dtype=torch.uint8, device=dev) for _ in range(R)]
+    h_out = torch.empty((R, h, w, 3), dtype=torch.uint8).pin_memory()
+    s_h2d, s_d2h = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
+    ready = [ev() for _ in range(R)]
+    done = [ev() for _ in range(R)]
+    d2h_done = [ev() for _ in range(R)]
     barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with torch.cuda.stream(t_stream):
-        e0.record(t_stream)
-        for i in range(a.steps):
-            d_in.copy_(host[(k2 + i) % nuniq], non_blocking=True)
-            sess.process_u8(d_in, d_out, stream=t_stream)
-            h_out.copy_(d_out, non_blocking=True)
-        e1.record(t_stream)
+    e0, e1 = ev(), ev()
+    e0.record(s_h2d)
+    for i in range(a.steps):
+        r = i % R
+        with torch.cuda.stream(s_h2d):
+            if i >= R:
+                s_h2d.wait_event(done[r])        # input consumed
+                s_h2d.wait_event(d2h_done[r])    # output read back
+            d_in[r].copy_(host[(k2 + i) % nuniq], non_blocking=True)
+            ready[r].record(s_h2d)
+        sess.process_u8_async(d_in[r], d_o[r], wait_event=ready[r], done_event=done[r])
+        with torch.cuda.stream(s_d2h):
+            s_d2h.wait_event(done[r])
+            h_out[r].copy_(d_o[r], non_blocking=True)
+            d2h_done[r].record(s_d2h)
+    e1.record(s_d2h)
     e1.synchronize()
     e2e_ms = e0.elapsed_time(e1)
     barrier()

@@ -57,11 +57,20 @@ void wema_cuda_session_destroy(wema_cuda_session *s);
  * window ring, threshold scratch, staging): the admission footprint. */
 size_t wema_cuda_session_bytes(const wema_cuda_config *cfg);
 
-/* One frame, device pointers, asynchronous on `cuda_stream` (a
- * cudaStream_t; NULL = the session's own stream).  in/out are RGB24
- * [height][width][3]; out may not alias in. */
+/* One frame, device pointers.  in/out are RGB24 [height][width][3]; out may
+ * not alias in.  With a `cuda_stream` (a cudaStream_t) the frame is ordered
+ * after the work already queued on it and the stream waits for the output.
+ * With NULL the frame is queued behind the session's earlier frames only;
+ * wema_cuda_session_sync() waits for it.  Either way consecutive frames
+ * overlap inside the session: frame t+1's forward transform and temporal
+ * filter run while frame t's threshold and inverse finish. */
 int wema_cuda_process_u8(wema_cuda_session *s, const uint8_t *d_in, uint8_t *d_out,
                          void *cuda_stream);
+/* The same with explicit events (cudaEvent_t, either may be NULL): the
+ * session waits for `wait_event` before reading d_in or writing d_out, and
+ * records `done_event` once d_out is complete and d_in no longer read. */
+int wema_cuda_process_u8_async(wema_cuda_session *s, const uint8_t *d_in, uint8_t *d_out,
+                               void *wait_event, void *done_event);
 /* Same with float RGB in [0,1] (the reference's Frame layout); either output
  * pointer may be NULL. */
 int wema_cuda_process_f32(wema_cuda_session *s, const float *d_in, float *d_out_f32,
@@ -72,12 +81,17 @@ int wema_cuda_process_host_u8(wema_cuda_session *s, const uint8_t *h_in, uint8_t
 /* Waits for the session's queued work. */
 int wema_cuda_session_sync(wema_cuda_session *s);
 
+/* Keep each frame's converted input planes and (colour) reconstructed planes
+ * so WEMA_CUDA_READ_GRAY_IN / _GRAY_OUT can return them (off by default: they
+ * cost two extra plane writes per channel and frame). */
+int wema_cuda_set_inspect(wema_cuda_session *s, int enable);
+
 /* Frames seen by the temporal filter (the reference's frames_processed,
  * which jumps to the warm-up count at the first frame's preseed). */
 int wema_cuda_session_frames_processed(const wema_cuda_session *s);
 
-/* Copies a stage of the last processed frame to host memory, in the
- * reference's layouts (synchronises first).  Returns the element count, or
+/* Copies a stage of the last queued frame to host memory, in the
+ * reference's layouts (waits for the session first).  Returns the element count, or
  * -1.  `what`: */
 enum {
     WEMA_CUDA_READ_GRAY_IN = 0,   /* Y plane [P] (colour: Y) */

@@ -216,3 +216,27 @@ def test_4k_threshold(oracle, torch_cuda):
     for form in (0, 1):
         thr, s = wc.threshold_flat(d, form)
         assert u32([thr])[0] == u32([oracle.threshold(orig, form)])[0]
+
+
+@pytest.mark.parametrize("color", [False, True])
+def test_pipelined_frames(oracle, torch_cuda, color):
+    """Frames issued back to back without waiting (several in flight inside the
+    session: forward/filter of frame t+1 overlap threshold/inverse of frame t)
+    give the same outputs as the oracle run frame by frame."""
+    torch = torch_cuda
+    w, h, F = 256, 160, 12
+    u8 = frames_for(w, h, F, seed=21)
+    rgb = oracle.u8_to_float(u8)
+    so = oracle.stream(width=w, height=h, fps=30.0, amp=90.0, f_low=0.5, f_high=3.0, color=color)
+    ref = [oracle.float_to_u8(so.process(rgb[t])) for t in range(F)]
+    sg = wc.Session(width=w, height=h, fps=30.0, amp=90.0, f_low=0.5, f_high=3.0, color=color,
+                    inspect=False)
+    d_in = torch.from_numpy(u8).cuda()
+    outs = [torch.empty((h, w, 3), dtype=torch.uint8, device="cuda") for _ in range(F)]
+    torch.cuda.synchronize()
+    for t in range(F):
+        sg.process_u8_async(d_in[t], outs[t])
+    sg.sync()
+    for t in range(F):
+        d = np.abs(outs[t].cpu().numpy().astype(int) - ref[t].astype(int))
+        assert d.max() <= (0 if color else 1), f"frame {t}"

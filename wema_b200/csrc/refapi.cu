@@ -227,14 +227,15 @@ bool session_frame(Session* s, const float* in, float* out) {
     const size_t P3 = 3 * (size_t)s->g.pixels;
     float* d_in = s->stage_f32;
     float* d_out = s->stage_f32 + P3;
-    if (!cuda_ok(cudaMemcpyAsync(d_in, in, P3 * sizeof(float), cudaMemcpyHostToDevice, s->stream),
+    if (!s->sync_all()) return false;   // staging reuse: the previous frame is complete
+    if (!cuda_ok(cudaMemcpyAsync(d_in, in, P3 * sizeof(float), cudaMemcpyHostToDevice, s->s_fwd),
                  "H2D"))
         return false;
-    if (!s->run(nullptr, d_in, nullptr, d_out, s->stream)) return false;
-    if (!cuda_ok(cudaMemcpyAsync(out, d_out, P3 * sizeof(float), cudaMemcpyDeviceToHost, s->stream),
+    if (!s->run(nullptr, d_in, nullptr, d_out, nullptr, nullptr)) return false;
+    if (!cuda_ok(cudaMemcpyAsync(out, d_out, P3 * sizeof(float), cudaMemcpyDeviceToHost, s->s_inv),
                  "D2H"))
         return false;
-    return sync(s->stream);
+    return sync(s->s_inv);
 }
 
 }  // namespace

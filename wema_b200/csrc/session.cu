@@ -117,20 +117,25 @@ static void layout(Arena& A, Session& s) {
     const Geom& g = s.g;
     const long long pu = g.uoff[g.levels];
     const long long n6 = g.off6[g.levels];
+    for (int b = 0; b < kSlots; b++) {
+        Slot& q = s.slot[b];
+        for (int c = 0; c < s.nch; c++) {
+            q.coef[c] = A.take<float>(pu);
+            q.delta[c] = A.take<float>(pu);
+            for (int l = 0; l < g.levels; l++) q.ll[c][l] = A.take<float>(g.n[l]);
+            for (int l = 0; l < g.levels; l++)
+                q.rec[c][l] = A.take<float>((size_t)g.in_w[l] * g.in_h[l]);
+            q.gray_in[c] = A.take<float>(g.pixels);
+        }
+        q.thr = A.take<float>(8);
+    }
     for (int c = 0; c < s.nch; c++) {
-        s.coef[c] = A.take<float>(pu);
-        s.ampl[c] = A.take<float>(pu);
-        s.delta[c] = A.take<float>(pu);
         if (s.cfg.use_iir) s.state[c] = A.take<float4>(pu);
         else s.ring[c] = A.take<float>((size_t)pu * s.cfg.temporal_window);
-        for (int l = 0; l < g.levels; l++) s.ll[c][l] = A.take<float>(g.n[l]);
-        for (int l = 0; l < g.levels; l++)
-            s.rec[c][l] = A.take<float>((size_t)g.in_w[l] * g.in_h[l]);
-        s.gray_in[c] = A.take<float>(g.pixels);
+        s.ampl[c] = A.take<float>(pu);
         void* t = A.take<char>(thr_scratch_bytes(n6));
         if (A.base) thr_scratch_bind(s.thr_s[c], t, n6);
     }
-    s.d_small = A.take<float>(16);
 }
 
 static bool valid_config(const wema_cuda_config& c) {
@@ -152,37 +157,35 @@ size_t Session::bytes_for(const wema_cuda_config& c) {
     s.nch = c.color_mode ? 3 : 1;
     Arena A;
     layout(A, s);
-    return A.off + 6 * (size_t)s.g.pixels * (1 + sizeof(float));   // + host-API staging
+    return A.off;
 }
 
 Session::~Session() {
-    if (stream) {
-        cudaStreamSynchronize(stream);
-        cudaStreamDestroy(stream);
-    }
-    if (side) {
-        cudaStreamSynchronize(side);
-        cudaStreamDestroy(side);
-    }
-    if (ev_fork) cudaEventDestroy(ev_fork);
-    if (ev_join) cudaEventDestroy(ev_join);
+    for (cudaStream_t st : {s_fwd, s_tmp, s_thr, s_inv})
+        if (st) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
+    for (Slot& q : slot)
+        for (cudaEvent_t e : {q.ev_fwd, q.ev_tmp, q.ev_thr, q.ev_done})
+            if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : {ev_call, ev_last})
+        if (e) cudaEventDestroy(e);
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
     if (arena) cudaFree(arena);
     if (stage_u8) cudaFree(stage_u8);
     if (stage_f32) cudaFree(stage_f32);
-    for (auto& e : ev)
-        if (e) cudaEventDestroy(e);
 }
 
 // adds the last timed frame's per-stage durations (waits for it)
 bool Session::collect_timing() {
     if (!ev_pending) return true;
     ev_pending = false;
-    if (!cuda_ok(cudaEventSynchronize(ev[6]), "event sync")) return false;
-    const int from[N_STAGE] = {0, 1, 7, 2, 4, 5};
-    const int to[N_STAGE] = {1, 2, 8, 3, 5, 6};
     for (int k = 0; k < N_STAGE; k++) {
+        if (!cuda_ok(cudaEventSynchronize(ev[2 * k + 1]), "event sync")) return false;
         float ms = 0.f;
-        if (cudaEventElapsedTime(&ms, ev[from[k]], ev[to[k]]) == cudaSuccess) stage_ms[k] += ms;
+        if (cudaEventElapsedTime(&ms, ev[2 * k], ev[2 * k + 1]) == cudaSuccess) stage_ms[k] += ms;
     }
     stage_frames++;
     return true;
@@ -214,23 +217,34 @@ bool Session::init(const wema_cuda_config& c) {
     A = Arena();
     A.base = (char*)arena;
     layout(A, *this);
-    if (!cuda_ok(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate"))
-        return false;
-    if (!cuda_ok(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking), "cudaStreamCreate"))
-        return false;
-    if (!cuda_ok(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming), "cudaEventCreate"))
-        return false;
-    if (!cuda_ok(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming), "cudaEventCreate"))
-        return false;
+    for (cudaStream_t* st : {&s_fwd, &s_tmp, &s_thr, &s_inv})
+        if (!cuda_ok(cudaStreamCreateWithFlags(st, cudaStreamNonBlocking), "cudaStreamCreate"))
+            return false;
+    for (Slot& q : slot)
+        for (cudaEvent_t* e : {&q.ev_fwd, &q.ev_tmp, &q.ev_thr, &q.ev_done})
+            if (!cuda_ok(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate"))
+                return false;
+    for (cudaEvent_t* e : {&ev_call, &ev_last})
+        if (!cuda_ok(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate"))
+            return false;
+    return true;
+}
+
+bool Session::sync_all() {
+    for (cudaStream_t st : {s_fwd, s_tmp, s_thr, s_inv})
+        if (!cuda_ok(cudaStreamSynchronize(st), "sync")) return false;
     return true;
 }
 
 bool Session::materialize_amplified() {
+    if (last_slot < 0) { set_error("no frame processed yet"); return false; }
+    const Slot& q = slot[last_slot];
+    if (!sync_all()) return false;
     for (int c = 0; c < nch; c++)
-        if (!cuda_ok(launch_amplify(ip, coef[c], delta[c], d_small + c, last_alpha[c], ampl[c], stream),
+        if (!cuda_ok(launch_amplify(ip, q.coef[c], q.delta[c], q.thr + c, q.alpha[c], ampl[c], s_inv),
                      "amplify"))
             return false;
-    return cuda_ok(cudaStreamSynchronize(stream), "sync");
+    return cuda_ok(cudaStreamSynchronize(s_inv), "sync");
 }
 
 bool Session::ensure_staging() {
@@ -241,30 +255,38 @@ bool Session::ensure_staging() {
     return true;
 }
 
-PyrView Session::view(int c) const {
+PyrView Session::view(int b, int c) const {
     PyrView v{};
-    v.coef = coef[c];
+    v.coef = slot[b].coef[c];
     v.levels = g.levels;
     for (int l = 0; l < g.levels; l++) { v.n[l] = g.n[l]; v.uoff[l] = g.uoff[l]; }
     for (int l = 0; l <= g.levels; l++) v.off6[l] = g.off6[l];
     return v;
 }
 
+// Frame pipeline.  Each frame uses one of kSlots buffer sets and four
+// streams: forward DWT -> {temporal filter, threshold} -> inverse + output,
+// chained by the slot's events.  The temporal filter and the threshold run in
+// frame order on their own streams (IIR state, window ring and binade history
+// carry from frame to frame), and frame t+1's forward DWT and filter overlap
+// frame t's threshold and inverse.
 bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, float* out_f32,
-                  cudaStream_t st) {
+                  cudaEvent_t wait, cudaEvent_t done) {
     const int L = g.levels;
-    float* d_thr = d_small;
-    float* d_sum = d_small + 4;
-    last_passthrough = false;
+    const int b = (int)(frames_run % kSlots);
+    Slot& q = slot[b];
     if (timing) {
         if (!collect_timing()) return false;
         if (!ev[0])
             for (auto& e : ev)
                 if (!cuda_ok(cudaEventCreate(&e), "cudaEventCreate")) return false;
     }
-    mark(0, st);
+    // the slot's previous frame must have finished with its buffers
+    if (wait && !cuda_ok(cudaStreamWaitEvent(s_fwd, wait, 0), "stream wait")) return false;
+    if (q.valid && !cuda_ok(cudaStreamWaitEvent(s_fwd, q.ev_done, 0), "stream wait")) return false;
 
-    // forward DWT
+    // ---- forward DWT
+    mark(2 * ST_FWD0, s_fwd);
     for (int l = 0; l < L; l++) {
         FwdLevelParams p{};
         p.iw = g.in_w[l];
@@ -278,134 +300,160 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
             mode = in_u8 ? kSrcRgbU8 : kSrcRgbF32;
             p.src_u8 = in_u8;
             p.src_f32 = in_f32;
-            for (int c = 0; c < nch; c++) p.plane_out[c] = gray_in[c];
+            if (inspect)
+                for (int c = 0; c < nch; c++) p.plane_out[c] = q.gray_in[c];
         } else {
-            for (int c = 0; c < nch; c++) p.src_planes[c] = ll[c][l - 1];
+            for (int c = 0; c < nch; c++) p.src_planes[c] = q.ll[c][l - 1];
         }
         for (int c = 0; c < nch; c++) {
-            p.coef[c] = coef[c] + g.uoff[l];
-            p.prev[c] = l > 0 ? coef[c] + g.uoff[l - 1] : nullptr;
-            p.ll_out[c] = ll[c][l];
+            p.coef[c] = q.coef[c] + g.uoff[l];
+            p.prev[c] = l > 0 ? q.coef[c] + g.uoff[l - 1] : nullptr;
+            p.ll_out[c] = q.ll[c][l];
         }
         p.prev_n = l > 0 ? g.n[l - 1] : 0;
-        if (!cuda_ok(launch_dwt_fwd(mode, nch, p, st), "forward DWT")) return false;
-        if (l == 0) mark(1, st);
+        if (!cuda_ok(launch_dwt_fwd(mode, nch, p, s_fwd), "forward DWT")) return false;
+        if (l == 0) {
+            mark(2 * ST_FWD0 + 1, s_fwd);
+            mark(2 * ST_FWD, s_fwd);
+        }
     }
+    mark(2 * ST_FWD + 1, s_fwd);
+    if (!cuda_ok(cudaEventRecord(q.ev_fwd, s_fwd), "event record")) return false;
 
-    PyrView views[3];
-    for (int c = 0; c < nch; c++) views[c] = view(c);
+    // ---- temporal filter (frame order on s_tmp)
+    if (!cuda_ok(cudaStreamWaitEvent(s_tmp, q.ev_fwd, 0), "stream wait")) return false;
     const long long pu = g.uoff[L];
-
-    // the threshold runs on the side stream while the temporal filter runs here
-    auto fork_threshold = [&]() -> bool {
-        if (!cuda_ok(cudaEventRecord(ev_fork, st), "event record")) return false;
-        if (!cuda_ok(cudaStreamWaitEvent(side, ev_fork, 0), "stream wait")) return false;
-        mark(7, side);
-        if (!cuda_ok(launch_threshold(views, nch, thr_s, d_thr, d_sum, cfg.threshold_form,
-                                      thr_hist ? 1 : 0, side),
-                     "threshold"))
-            return false;
-        thr_hist = true;
-        mark(8, side);
-        return cuda_ok(cudaEventRecord(ev_join, side), "event record");
-    };
-
-    float alpha[3];
-    mark(2, st);
+    q.passthrough = false;
+    mark(2 * ST_TEMPORAL, s_tmp);
     if (cfg.use_iir) {
-        if (!fork_threshold()) return false;
         if (frames_processed == 0) {   // iir_temporal_preseed on the first frame
             for (int c = 0; c < nch; c++)
-                if (!cuda_ok(launch_iir_preseed(ip, coef[c], state[c], warmup, st), "preseed"))
+                if (!cuda_ok(launch_iir_preseed(ip, q.coef[c], state[c], warmup, s_tmp), "preseed"))
                     return false;
             frames_processed = warmup;
         }
         const float amp = fade_amp(cfg.amp_factor, frames_processed, warmup);
         frames_processed++;
-        alpha[0] = amp;
-        alpha[1] = alpha[2] = amp * 0.5f;
+        q.alpha[0] = amp;
+        q.alpha[1] = q.alpha[2] = amp * 0.5f;
         for (int c = 0; c < nch; c++)
-            if (!cuda_ok(launch_iir(ip, coef[c], state[c], delta[c], st), "IIR")) return false;
+            if (!cuda_ok(launch_iir(ip, q.coef[c], state[c], q.delta[c], s_tmp), "IIR")) return false;
     } else {
         for (int c = 0; c < nch; c++)
-            if (!cuda_ok(launch_ring_push(coef[c], ring[c], pu, head, st), "ring push")) return false;
+            if (!cuda_ok(launch_ring_push(q.coef[c], ring[c], pu, head, s_tmp), "ring push"))
+                return false;
         head = (head + 1) % cfg.temporal_window;
         if (filled < cfg.temporal_window) filled++;
-        if (filled < cfg.temporal_window) {   // wema.c:924-929: pass the input through
-            TransferParams tp{};
-            tp.w = g.w;
-            tp.h = g.h;
-            tp.src_u8 = in_u8;
-            tp.src_f32 = in_f32;
-            tp.out_u8 = out_u8;
-            tp.out_f32 = out_f32;
-            last_passthrough = true;
-            return cuda_ok(launch_passthrough(tp, st), "passthrough");
+        q.passthrough = filled < cfg.temporal_window;   // wema.c:924-929
+        q.alpha[0] = cfg.amp_factor;
+        q.alpha[1] = q.alpha[2] = cfg.amp_factor * 0.5f;
+        if (!q.passthrough) {
+            WindowParams wp{};
+            wp.pu = pu;
+            wp.ws = cfg.temporal_window;
+            wp.head = head;   // oldest sample (temporal_filter.c:221)
+            wp.bilateral = cfg.bilateral_temp;
+            const int ws = cfg.temporal_window, center = ws / 2;
+            const float ts = (float)ws * 0.15f;
+            const float inv2 = 0.5f / (ts * ts);
+            for (int t = 0; t < ws; t++) {
+                const float d = (float)(t - center);
+                wp.time_w[t] = expf(-(d * d) * inv2);
+            }
+            for (int c = 0; c < nch; c++)
+                if (!cuda_ok(launch_window(wp, ring[c], q.delta[c], s_tmp), "window filter"))
+                    return false;
         }
-        if (!fork_threshold()) return false;
-        alpha[0] = cfg.amp_factor;
-        alpha[1] = alpha[2] = cfg.amp_factor * 0.5f;
-        WindowParams wp{};
-        wp.pu = pu;
-        wp.ws = cfg.temporal_window;
-        wp.head = head;   // oldest sample (temporal_filter.c:221)
-        wp.bilateral = cfg.bilateral_temp;
-        const int ws = cfg.temporal_window, center = ws / 2;
-        const float ts = (float)ws * 0.15f;
-        const float inv2 = 0.5f / (ts * ts);
-        for (int t = 0; t < ws; t++) {
-            const float d = (float)(t - center);
-            wp.time_w[t] = expf(-(d * d) * inv2);
-        }
-        for (int c = 0; c < nch; c++)
-            if (!cuda_ok(launch_window(wp, ring[c], delta[c], st), "window filter")) return false;
     }
-    for (int c = 0; c < nch; c++) last_alpha[c] = alpha[c];
-    mark(3, st);
-    if (!cuda_ok(cudaStreamWaitEvent(st, ev_join, 0), "stream wait")) return false;
-    mark(4, st);
+    mark(2 * ST_TEMPORAL + 1, s_tmp);
+    if (!cuda_ok(cudaEventRecord(q.ev_tmp, s_tmp), "event record")) return false;
 
-    // inverse DWT, coarse to fine; amplification applied while staging
-    for (int l = L - 1; l >= 0; l--) {
-        InvLevelParams q{};
-        q.ow = g.in_w[l];
-        q.oh = g.in_h[l];
-        q.sw = g.sw[l];
-        q.sh = g.sh[l];
-        q.n = g.n[l];
-        q.thr = d_thr;
-        for (int c = 0; c < nch; c++) {
-            q.ll[c] = (l == L - 1) ? ll[c][L - 1] : rec[c][l + 1];
-            q.coef[c] = coef[c] + g.uoff[l];
-            q.delta[c] = delta[c] + g.uoff[l];
-            q.alpha[c] = l == 0 ? alpha[c] * 0.5f : alpha[c];
-            q.out_planes[c] = rec[c][l];
-        }
-        int mode = kOutPlanes;
-        if (l == 0 && nch == 3) {
-            mode = kOutRgb;
-            q.out_u8 = out_u8;
-            q.out_f32 = out_f32;
-        }
-        if (!cuda_ok(launch_dwt_inv(nch, mode, q, st), "inverse DWT")) return false;
+    // ---- threshold (frame order on s_thr: the binade history carries over)
+    if (!q.passthrough) {
+        if (!cuda_ok(cudaStreamWaitEvent(s_thr, q.ev_fwd, 0), "stream wait")) return false;
+        PyrView views[3];
+        for (int c = 0; c < nch; c++) views[c] = view(b, c);
+        ThrScratch ts[3];
+        for (int c = 0; c < nch; c++) ts[c] = thr_s[c];
+        mark(2 * ST_THR, s_thr);
+        if (!cuda_ok(launch_threshold(views, nch, ts, q.thr, q.thr + 4, cfg.threshold_form,
+                                      thr_hist ? 1 : 0, s_thr),
+                     "threshold"))
+            return false;
+        thr_hist = true;
+        mark(2 * ST_THR + 1, s_thr);
+        if (!cuda_ok(cudaEventRecord(q.ev_thr, s_thr), "event record")) return false;
     }
-    mark(5, st);
-    if (nch == 1) {
+
+    // ---- inverse DWT (amplification applied while staging) and output
+    if (!cuda_ok(cudaStreamWaitEvent(s_inv, q.ev_tmp, 0), "stream wait")) return false;
+    if (!q.passthrough && !cuda_ok(cudaStreamWaitEvent(s_inv, q.ev_thr, 0), "stream wait"))
+        return false;
+    if (q.passthrough) {
         TransferParams tp{};
         tp.w = g.w;
         tp.h = g.h;
-        tp.vec_end = vec_cover(g.pixels);
         tp.src_u8 = in_u8;
         tp.src_f32 = in_f32;
-        tp.gray_out = rec[0][0];
         tp.out_u8 = out_u8;
         tp.out_f32 = out_f32;
-        tp.edge_aware = cfg.edge_aware;
-        if (!cuda_ok(launch_transfer(tp, st), "luma transfer")) return false;
+        if (!cuda_ok(launch_passthrough(tp, s_inv), "passthrough")) return false;
+    } else {
+        mark(2 * ST_INV, s_inv);
+        for (int l = L - 1; l >= 0; l--) {
+            InvLevelParams iq{};
+            iq.ow = g.in_w[l];
+            iq.oh = g.in_h[l];
+            iq.sw = g.sw[l];
+            iq.sh = g.sh[l];
+            iq.n = g.n[l];
+            iq.thr = q.thr;
+            for (int c = 0; c < nch; c++) {
+                iq.ll[c] = (l == L - 1) ? q.ll[c][L - 1] : q.rec[c][l + 1];
+                iq.coef[c] = q.coef[c] + g.uoff[l];
+                iq.delta[c] = q.delta[c] + g.uoff[l];
+                iq.alpha[c] = l == 0 ? q.alpha[c] * 0.5f : q.alpha[c];
+                iq.out_planes[c] = (l > 0 || nch == 1 || inspect) ? q.rec[c][l] : nullptr;
+            }
+            int mode = kOutPlanes;
+            if (l == 0 && nch == 3) {
+                mode = kOutRgb;
+                iq.out_u8 = out_u8;
+                iq.out_f32 = out_f32;
+            }
+            if (!cuda_ok(launch_dwt_inv(nch, mode, iq, s_inv), "inverse DWT")) return false;
+        }
+        mark(2 * ST_INV + 1, s_inv);
+        mark(2 * ST_XFER, s_inv);
+        if (nch == 1) {
+            TransferParams tp{};
+            tp.w = g.w;
+            tp.h = g.h;
+            tp.vec_end = vec_cover(g.pixels);
+            tp.src_u8 = in_u8;
+            tp.src_f32 = in_f32;
+            tp.gray_out = q.rec[0][0];
+            tp.out_u8 = out_u8;
+            tp.out_f32 = out_f32;
+            tp.edge_aware = cfg.edge_aware;
+            if (!cuda_ok(launch_transfer(tp, s_inv), "luma transfer")) return false;
+        }
+        mark(2 * ST_XFER + 1, s_inv);
+        ev_pending = timing;
     }
-    mark(6, st);
-    ev_pending = timing;
+    if (!cuda_ok(cudaEventRecord(q.ev_done, s_inv), "event record")) return false;
+    if (done && !cuda_ok(cudaEventRecord(done, s_inv), "event record")) return false;
+    q.valid = true;
+    last_slot = b;
+    frames_run++;
     return true;
+}
+
+bool Session::run_on(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, float* out_f32,
+                     cudaStream_t st) {
+    if (!cuda_ok(cudaEventRecord(ev_call, st), "event record")) return false;
+    if (!run(in_u8, in_f32, out_u8, out_f32, ev_call, ev_last)) return false;
+    return cuda_ok(cudaStreamWaitEvent(st, ev_last, 0), "stream wait");
 }
 
 }  // namespace wema
@@ -469,8 +517,17 @@ WEMA_API int wema_cuda_process_u8(wema_cuda_session* s, const uint8_t* d_in, uin
     clear_error();
     if (!s || !d_in || !d_out) { set_error("null argument"); return -1; }
     if (!cuda_ok(cudaSetDevice(s->s.cfg.device), "cudaSetDevice")) return -1;
-    cudaStream_t st = cuda_stream ? (cudaStream_t)cuda_stream : s->s.stream;
-    return s->s.run(d_in, nullptr, d_out, nullptr, st) ? 0 : -1;
+    if (!cuda_stream) return s->s.run(d_in, nullptr, d_out, nullptr, nullptr, nullptr) ? 0 : -1;
+    return s->s.run_on(d_in, nullptr, d_out, nullptr, (cudaStream_t)cuda_stream) ? 0 : -1;
+}
+
+WEMA_API int wema_cuda_process_u8_async(wema_cuda_session* s, const uint8_t* d_in, uint8_t* d_out,
+                                        void* wait_event, void* done_event) {
+    clear_error();
+    if (!s || !d_in || !d_out) { set_error("null argument"); return -1; }
+    if (!cuda_ok(cudaSetDevice(s->s.cfg.device), "cudaSetDevice")) return -1;
+    return s->s.run(d_in, nullptr, d_out, nullptr, (cudaEvent_t)wait_event, (cudaEvent_t)done_event)
+               ? 0 : -1;
 }
 
 WEMA_API int wema_cuda_process_f32(wema_cuda_session* s, const float* d_in, float* d_out_f32,
@@ -478,8 +535,8 @@ WEMA_API int wema_cuda_process_f32(wema_cuda_session* s, const float* d_in, floa
     clear_error();
     if (!s || !d_in || (!d_out_f32 && !d_out_u8)) { set_error("null argument"); return -1; }
     if (!cuda_ok(cudaSetDevice(s->s.cfg.device), "cudaSetDevice")) return -1;
-    cudaStream_t st = cuda_stream ? (cudaStream_t)cuda_stream : s->s.stream;
-    return s->s.run(nullptr, d_in, d_out_u8, d_out_f32, st) ? 0 : -1;
+    if (!cuda_stream) return s->s.run(nullptr, d_in, d_out_u8, d_out_f32, nullptr, nullptr) ? 0 : -1;
+    return s->s.run_on(nullptr, d_in, d_out_u8, d_out_f32, (cudaStream_t)cuda_stream) ? 0 : -1;
 }
 
 WEMA_API int wema_cuda_process_host_u8(wema_cuda_session* s, const uint8_t* h_in, uint8_t* h_out) {
@@ -489,19 +546,28 @@ WEMA_API int wema_cuda_process_host_u8(wema_cuda_session* s, const uint8_t* h_in
     if (!cuda_ok(cudaSetDevice(S.cfg.device), "cudaSetDevice")) return -1;
     if (!S.ensure_staging()) return -1;
     const size_t P3 = 3 * (size_t)S.g.pixels;
-    if (!cuda_ok(cudaMemcpyAsync(S.stage_u8, h_in, P3, cudaMemcpyHostToDevice, S.stream), "H2D"))
+    // the staging buffers are reused: everything earlier on this session has finished
+    if (!S.sync_all()) return -1;
+    if (!cuda_ok(cudaMemcpyAsync(S.stage_u8, h_in, P3, cudaMemcpyHostToDevice, S.s_fwd), "H2D"))
         return -1;
-    if (!S.run(S.stage_u8, nullptr, S.stage_u8 + P3, nullptr, S.stream)) return -1;
-    if (!cuda_ok(cudaMemcpyAsync(h_out, S.stage_u8 + P3, P3, cudaMemcpyDeviceToHost, S.stream), "D2H"))
+    if (!S.run(S.stage_u8, nullptr, S.stage_u8 + P3, nullptr, nullptr, nullptr)) return -1;
+    if (!cuda_ok(cudaMemcpyAsync(h_out, S.stage_u8 + P3, P3, cudaMemcpyDeviceToHost, S.s_inv), "D2H"))
         return -1;
-    return cuda_ok(cudaStreamSynchronize(S.stream), "sync") ? 0 : -1;
+    return cuda_ok(cudaStreamSynchronize(S.s_inv), "sync") ? 0 : -1;
 }
 
 WEMA_API int wema_cuda_session_sync(wema_cuda_session* s) {
     clear_error();
     if (!s) { set_error("null session"); return -1; }
     if (!cuda_ok(cudaSetDevice(s->s.cfg.device), "cudaSetDevice")) return -1;
-    return cuda_ok(cudaStreamSynchronize(s->s.stream), "sync") ? 0 : -1;
+    return s->s.sync_all() ? 0 : -1;
+}
+
+WEMA_API int wema_cuda_set_inspect(wema_cuda_session* s, int enable) {
+    clear_error();
+    if (!s) { set_error("null session"); return -1; }
+    s->s.inspect = enable != 0;
+    return 0;
 }
 
 WEMA_API int wema_cuda_session_frames_processed(const wema_cuda_session* s) {
@@ -514,10 +580,11 @@ WEMA_API long wema_cuda_session_read(wema_cuda_session* s, int what, int channel
     if (!s || !h_dst) { set_error("null argument"); return -1; }
     Session& S = s->s;
     if (channel < 0 || channel >= S.nch) { set_error("bad channel"); return -1; }
+    if (S.last_slot < 0) { set_error("no frame processed yet"); return -1; }
     if (!cuda_ok(cudaSetDevice(S.cfg.device), "cudaSetDevice")) return -1;
-    if (!cuda_ok(cudaStreamSynchronize(S.stream), "sync")) return -1;
-    if (!cuda_ok(cudaStreamSynchronize(S.side), "sync")) return -1;
+    if (!S.sync_all()) return -1;
     const Geom& g = S.g;
+    const Slot& q = S.slot[S.last_slot];
     const long long pu = g.uoff[g.levels], n6 = g.off6[g.levels];
     auto rd = [&](const float* src, size_t n) -> long {
         if (n > cap) { set_error("buffer too small (%zu needed)", n); return -1; }
@@ -537,17 +604,20 @@ WEMA_API long wema_cuda_session_read(wema_cuda_session* s, int what, int channel
             }
         return (long)n6;
     };
+    const bool planes = S.inspect || (what == WEMA_CUDA_READ_GRAY_OUT && S.nch == 1);
     switch (what) {
-        case WEMA_CUDA_READ_GRAY_IN: return rd(S.gray_in[channel], g.pixels);
-        case WEMA_CUDA_READ_GRAY_OUT: return rd(S.rec[channel][0], g.pixels);
-        case WEMA_CUDA_READ_ORIG6: return rd6(S.coef[channel]);
-        case WEMA_CUDA_READ_DELTA6: return rd6(S.delta[channel]);
+        case WEMA_CUDA_READ_GRAY_IN:
+        case WEMA_CUDA_READ_GRAY_OUT:
+            if (!planes) { set_error("enable wema_cuda_set_inspect before processing"); return -1; }
+            return rd(what == WEMA_CUDA_READ_GRAY_IN ? q.gray_in[channel] : q.rec[channel][0], g.pixels);
+        case WEMA_CUDA_READ_ORIG6: return rd6(q.coef[channel]);
+        case WEMA_CUDA_READ_DELTA6: return rd6(q.delta[channel]);
         case WEMA_CUDA_READ_AMP6:
             if (!S.materialize_amplified()) return -1;
             return rd6(S.ampl[channel]);
-        case WEMA_CUDA_READ_LOWPASS: return rd(S.ll[channel][g.levels - 1], g.low_n);
-        case WEMA_CUDA_READ_THRESHOLD: return rd(S.d_small, S.nch);
-        case WEMA_CUDA_READ_MAGSUM: return rd(S.d_small + 4, S.nch);
+        case WEMA_CUDA_READ_LOWPASS: return rd(q.ll[channel][g.levels - 1], g.low_n);
+        case WEMA_CUDA_READ_THRESHOLD: return rd(q.thr, S.nch);
+        case WEMA_CUDA_READ_MAGSUM: return rd(q.thr + 4, S.nch);
     }
     set_error("unknown stage %d", what);
     return -1;

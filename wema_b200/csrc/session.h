@@ -23,6 +23,22 @@ bool ensure_device(int dev);
 int design_bandpass(float f_low, float f_high, float fs, float c[10], int* warmup);
 float fade_amp(float amp_factor, int frames_before, int warmup);
 
+constexpr int kSlots = 2;   // frames in flight per session (pyramid buffer sets)
+
+// Buffers of one frame in flight
+struct Slot {
+    float* coef[3] = {};
+    float* delta[3] = {};
+    float* ll[3][WEMA_MAX_LEV] = {};
+    float* rec[3][WEMA_MAX_LEV] = {};  // rec[c][0]: level-0 reconstruction (luma: gray_out)
+    float* gray_in[3] = {};            // inspection only
+    float* thr = nullptr;              // [0..2] thresholds, [4..6] sums
+    float alpha[3] = {};
+    bool valid = false;                // holds a processed frame
+    bool passthrough = false;
+    cudaEvent_t ev_fwd = nullptr, ev_tmp = nullptr, ev_thr = nullptr, ev_done = nullptr;
+};
+
 class Session {
 public:
     wema_cuda_config cfg{};
@@ -33,51 +49,52 @@ public:
     int warmup = 0;
     int frames_processed = 0;
     int head = 0, filled = 0;          // window ring
-    bool last_passthrough = false;
-    cudaStream_t stream = nullptr;
-    cudaStream_t side = nullptr;       // threshold branch, joined before the inverse
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-    float last_alpha[3] = {};          // per-channel alpha of the last frame
-    bool thr_hist = false;             // threshold scratch holds the last frame's binades
+    bool inspect = false;              // keep input / reconstructed planes for reading back
+    long long frames_run = 0;          // frames issued (slot = frames_run % kSlots)
+    int last_slot = -1;
 
-    // device arena
+    // streams: forward DWT, temporal filter, threshold, inverse + output
+    cudaStream_t s_fwd = nullptr, s_tmp = nullptr, s_thr = nullptr, s_inv = nullptr;
+    cudaEvent_t ev_call = nullptr, ev_last = nullptr;
+
     void* arena = nullptr;
     size_t arena_bytes = 0;
-    float* coef[3] = {};
-    float* ampl[3] = {};
-    float* delta[3] = {};
-    float4* state[3] = {};
-    float* ll[3][WEMA_MAX_LEV] = {};
-    float* rec[3][WEMA_MAX_LEV] = {};  // rec[c][0]: level-0 reconstruction
-    float* gray_in[3] = {};
-    float* ring[3] = {};
-    ThrScratch thr_s[3] = {};
-    float* d_small = nullptr;          // thr[3], sum[3]
-    // per-stage timing (CUDA events), enabled on demand
+    Slot slot[kSlots];
+    float4* state[3] = {};             // IIR state (shared by the slots, updated in frame order)
+    float* ring[3] = {};               // window ring
+    float* ampl[3] = {};               // materialised amplified coefficients (inspection)
+    ThrScratch thr_s[3] = {};          // threshold scratch + binade history (frame order)
+    bool thr_hist = false;
+    // host-API staging (allocated on first use)
+    uint8_t* stage_u8 = nullptr;       // in [3P] + out [3P]
+    float* stage_f32 = nullptr;        // in [3P] + out [3P]
+
+    // per-stage timing (CUDA events on each stage's stream), enabled on demand
     enum { ST_FWD0, ST_FWD, ST_THR, ST_TEMPORAL, ST_INV, ST_XFER, N_STAGE };
-    // events: 0 fwd0, 1 fwd levels, 2 temporal start, 3 temporal end, 4 inverse
-    // start (after the join), 5 transfer start, 6 end, 7/8 threshold begin/end
-    enum { N_EV = 9 };
+    enum { N_EV = 2 * N_STAGE };
     bool timing = false;
     cudaEvent_t ev[N_EV] = {};
     bool ev_pending = false;
     double stage_ms[N_STAGE] = {};
     long long stage_frames = 0;
     void mark(int k, cudaStream_t st) { if (timing) cudaEventRecord(ev[k], st); }
-    bool materialize_amplified();      // ampl[] = amplified coefficients of the last frame
     bool collect_timing();
-    // host-API staging (allocated on first use)
-    uint8_t* stage_u8 = nullptr;       // in [3P] + out [3P]
-    float* stage_f32 = nullptr;        // in [3P] + out [3P]
 
     ~Session();
     static size_t bytes_for(const wema_cuda_config& c);
     bool init(const wema_cuda_config& c);
-    // one frame; exactly one of in_u8 / in_f32 is set; outputs optional
+    // One frame, asynchronous: waits for `wait` (may be null) before touching
+    // in/out, records `done` (may be null) once out is written and in is no
+    // longer read.  Exactly one of in_u8 / in_f32 is set; outputs optional.
     bool run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, float* out_f32,
-             cudaStream_t st);
-    PyrView view(int c) const;
+             cudaEvent_t wait, cudaEvent_t done);
+    // synchronous-on-a-stream form: ordered after earlier work on st; st waits for the frame
+    bool run_on(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, float* out_f32,
+                cudaStream_t st);
+    bool sync_all();
+    PyrView view(int b, int c) const;
     bool ensure_staging();
+    bool materialize_amplified();      // ampl[] = amplified coefficients of the last frame
 };
 
 }  // namespace wema

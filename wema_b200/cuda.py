@@ -44,6 +44,8 @@ def lib() -> C.CDLL:
         L.wema_cuda_session_create.argtypes = [C.POINTER(Config), C.POINTER(vp)]
         L.wema_cuda_session_destroy.argtypes = [vp]
         L.wema_cuda_process_u8.argtypes = [vp, vp, vp, vp]
+        L.wema_cuda_process_u8_async.argtypes = [vp, vp, vp, vp, vp]
+        L.wema_cuda_set_inspect.argtypes = [vp, i]
         L.wema_cuda_process_f32.argtypes = [vp, vp, vp, vp, vp]
         L.wema_cuda_process_host_u8.argtypes = [vp, vp, vp]
         L.wema_cuda_session_sync.argtypes = [vp]
@@ -95,17 +97,25 @@ def _ptr(t) -> int:
 class Session:
     """One video stream with device-resident state."""
 
-    def __init__(self, **kw):
+    def __init__(self, inspect: bool = True, **kw):
         self.cfg = make_config(**kw)
         h = C.c_void_p()
         _check(lib().wema_cuda_session_create(C.byref(self.cfg), C.byref(h)), "session create")
         self.h = h
+        _check(lib().wema_cuda_set_inspect(self.h, int(bool(inspect))), "set_inspect")
         self.w, self.hgt = self.cfg.width, self.cfg.height
         self.channels = 3 if self.cfg.color_mode else 1
 
     def process_u8(self, d_in, d_out, stream=None):
         s = stream.cuda_stream if stream is not None else None
         _check(lib().wema_cuda_process_u8(self.h, _ptr(d_in), _ptr(d_out), s), "process_u8")
+
+    def process_u8_async(self, d_in, d_out, wait_event=None, done_event=None):
+        """wait_event / done_event: torch.cuda.Event (or None)."""
+        we = wait_event.cuda_event if wait_event is not None else None
+        de = done_event.cuda_event if done_event is not None else None
+        _check(lib().wema_cuda_process_u8_async(self.h, _ptr(d_in), _ptr(d_out), we, de),
+               "process_u8_async")
 
     def process_f32(self, d_in, d_out_f32=None, d_out_u8=None, stream=None):
         s = stream.cuda_stream if stream is not None else None
