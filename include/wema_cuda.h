@@ -122,7 +122,7 @@ int wema_cuda_threshold_flat(const float *d_x, size_t n, int threshold_form, flo
  * reference: it exists for callers that must not allocate device memory,
  * e.g. a host that owns the GPU's memory through its own pool or a real-time
  * loop that cannot absorb cudaMalloc's synchronisation).  Its scratch is a
- * fixed 1 MiB array compiled into the library, held by every device that
+ * fixed 4 MiB array compiled into the library, held by every device that
  * loads it; n is limited to 2^24 elements (more than a 3840x2160 frame's
  * 6-slot coefficients) and larger n is rejected.  The first call on a device
  * looks up that array's device address (with the device current); make it

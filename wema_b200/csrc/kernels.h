@@ -53,13 +53,17 @@ struct PyrView {
     long long n[4], uoff[4], off6[5];   // off6[levels] = N6
 };
 
-struct ThrScratch {             // device scratch, sized by thr_scratch_bytes
-    double* part;               // [n_sub][8] exact-ish lane partial sums
-    double* prefix;             // [n_sub][8] exclusive prefixes
-    int4* cand;                 // [n_sub][8][2] binade top and monoids of 3 candidates
-    int* hist;                  // [n_sub][8] binade of the running sum at each sub-chunk
-                                // start, recorded by the last walk (the next frame's prediction)
+struct ThrScratch {             // device scratch, sized by thr_scratch_bytes; lane-major [8][n_sub]
+    double* part;               // sub-chunk sums of |x| (binade prediction)
+    double* prefix;             // exclusive FP64 prefixes (first call only)
+    int4* candp;                // {primary binade, d0, d1, secondary binade or 0}
+    int2* candq;                // secondary {d0, d1}
+    int* hist;                  // binade of the running sum at each sub-chunk start, recorded
+                                // by the last walk (the next frame's candidates)
+    float* lanes;               // [8] final lane sums
+    unsigned* counter;          // lanes finished (the last one runs the epilogue)
 };
+cudaError_t thr_prepare_device();
 size_t thr_scratch_bytes(long long n6);
 void thr_scratch_bind(ThrScratch& s, void* base, long long n6);
 // Writes thr[chan] = threshold of each of `nch` channels (single-frame form

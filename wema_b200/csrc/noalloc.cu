@@ -22,9 +22,9 @@
 namespace wema {
 
 // Largest input: 2^24 floats, more than a 3840x2160 frame's 6-slot
-// coefficient array (16,524,000).  Its threshold scratch needs 852,224 bytes.
+// coefficient array (16,524,000).  Its threshold scratch needs 2,883,840 bytes.
 constexpr size_t kNoAllocMaxElems = (size_t)1 << 24;
-constexpr size_t kNoAllocScratchBytes = (size_t)1 << 20;
+constexpr size_t kNoAllocScratchBytes = (size_t)1 << 22;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -79,8 +79,9 @@ extern "C" __attribute__((visibility("default"))) int wema_cuda_threshold_flat_n
     void* scratch = noalloc_scratch(dev);
     if (!scratch) return -1;
     // Nothing in the scratch has to start at zero: the kernels write every
-    // partial sum, prefix and candidate entry before reading it, and the
-    // binade history (which a previous call may have left) is not consulted.
+    // partial sum, prefix and candidate entry before reading it, the first
+    // kernel clears the lane counter, and the binade history (which a
+    // previous call may have left) is not consulted.
     ThrScratch ts{};
     thr_scratch_bind(ts, scratch, (long long)n);
     PyrView v{};

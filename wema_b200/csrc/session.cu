@@ -52,6 +52,7 @@ bool ensure_device(int dev) {
     if (ready[dev]) return true;
     if (!cuda_ok(dwt_prepare_device(), "DWT kernel setup")) return false;
     if (!cuda_ok(spatial_prepare_device(), "spatial kernel setup")) return false;
+    if (!cuda_ok(thr_prepare_device(), "threshold kernel setup")) return false;
     ready[dev] = 1;
     return true;
 }
