@@ -52,6 +52,16 @@ WORKLOADS = {
 }
 METRIC = "Mpix-frames/s"
 
+# DRAM bytes (read + write) per frame of a stage's kernels from one ncu
+# capture each, keyed by (workload, stage); stages not captured report null.
+# profiles/k_thr_monoids_plain_fullhd_color.txt, k_thr_walk_..., k_dwt_inv_level0_...
+# and k_dwt_fwd_level0_... hold the captures and the commands that made them.
+TRAFFIC_NCU = {
+    ("plain_fullhd_color", "threshold"): 25081088 + 2323456,
+    ("plain_fullhd_color", "inv_dwt_level0"): 43630080 + 278784,
+    ("plain_fullhd_color", "fwd_dwt_level0"): 6266624 + 7168,
+}
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -129,8 +139,9 @@ class ClockSampler:
 
 
 def stage_bytes(w, h, channels, levels_dims, pu):
-    """Algorithmic HBM bytes per frame of each stage (each plane read or
-    written once by its stage)."""
+    """Algorithmic HBM bytes per frame of each stage: every plane its stage
+    reads or writes, once (the 6-slot mirror of the threshold is the same
+    memory as the unique planes, so it is counted once)."""
     P = w * h
     C = channels
     n0 = levels_dims[0][0] * levels_dims[0][1]
@@ -140,18 +151,33 @@ def stage_bytes(w, h, channels, levels_dims, pu):
         pw, ph = levels_dims[l - 1]
         sw, sh = levels_dims[l]
         rest += C * 4 * (pw * ph + 4 * sw * sh)
-    thr = C * 2 * 4 * pu                               # two passes over |x|
+    thr = C * 4 * pu                                   # |x| of every unique coefficient
     temporal = C * (4 + 32 + 4) * pu                   # coef in, state in/out, delta out
-    inv = 0
+    inv = {}
     for l in range(len(levels_dims)):
         sw, sh = levels_dims[l]
         iw = (w if l == 0 else levels_dims[l - 1][0])
         ih = (h if l == 0 else levels_dims[l - 1][1])
-        inv += C * 4 * sw * sh + C * 8 * 3 * sw * sh   # LL in; 3 bands: coef + delta in
-        inv += (3 * P if (l == 0 and C == 3) else C * 4 * iw * ih)
+        b = C * 4 * sw * sh + C * 8 * 3 * sw * sh      # LL in; 3 bands: coef + delta in
+        b += 3 * P if (l == 0 and C == 3) else C * 4 * iw * ih
+        inv[l] = b
     xfer = 0 if C == 3 else 3 * P + 4 * P + 3 * P      # RGB in, Y in, RGB out
     return {"fwd_dwt_level0": fwd0, "fwd_dwt_levels": rest, "threshold": thr,
-            "temporal_amplify": temporal, "inv_dwt": inv, "luma_transfer": xfer}
+            "temporal_amplify": temporal,
+            "inv_dwt_levels": sum(v for l, v in inv.items() if l > 0),
+            "inv_dwt_level0": inv[0], "luma_transfer": xfer}
+
+
+# kernels behind each stage (one launch per frame unless noted)
+STAGE_KERNELS = {
+    "fwd_dwt_level0": "k_dwt_fwd<1|2> (level 0, RGB in)",
+    "fwd_dwt_levels": "k_dwt_fwd<0> x (levels - 1)",
+    "threshold": "k_thr_monoids + k_thr_walk",
+    "temporal_amplify": "k_iir x channels",
+    "inv_dwt_levels": "k_dwt_inv<1,0> x (levels - 1)",
+    "inv_dwt_level0": "k_dwt_inv<3,1> (colour, RGB out) / k_dwt_inv<1,0> (luma)",
+    "luma_transfer": "k_guided_transfer / k_gauss_transfer",
+}
 
 
 def dims_of(w, h):
@@ -286,6 +312,7 @@ def main():
     # t's threshold and inverse); device time from an event the first frame
     # waits on to the event the last frame records
     k0 = a.warmup
+    launches0 = sess.launches()
     barrier()
     with ClockSampler(local) as clk:
         ev0, ev1 = ev(), ev()
@@ -295,14 +322,18 @@ def main():
                                   done_event=ev1 if i == a.steps - 1 else None)
         ev1.synchronize()
         ms = ev0.elapsed_time(ev1)
+    launches = sess.launches() - launches0
     barrier()
     clocks = clk.summary()
 
-    # ---- per-stage timing pass (same workload, continuing the stream)
+    # ---- per-stage timing pass: frames one at a time (each completes before
+    # the next is issued), CUDA events around every stage on its own stream;
+    # the threshold and the temporal filter of a frame still run side by side
     sess.set_timing(True)
     k1 = k0 + a.steps
     for i in range(a.steps):
         sess.process_u8(frame(k1 + i), d_out, stream=t_stream)
+        torch.cuda.synchronize(dev)
     stages, nst = sess.stage_times()
     sess.set_timing(False)
     torch.cuda.synchronize(dev)
@@ -354,12 +385,13 @@ def main():
     C = 3 if kw.get("color") else 1
     sb = stage_bytes(w, h, C, dims, pu)
     per_frame = {k: v / max(nst, 1) for k, v in stages.items()}
-    dom = max(per_frame, key=per_frame.get)
     peak, peak_kind = peaks()
+    dom = max(per_frame, key=per_frame.get)
     achieved = sb[dom] / (per_frame[dom] * 1e-3) / 1e9
     total_bytes = sum(sb.values())
-    total_ms = sum(per_frame.values())
-    launches_per_frame = (len(dims) + 4 + C + len(dims) + (0 if C == 3 else 1))
+    stage_frac = {k: round(sb[k] / (per_frame[k] * 1e-3) / 1e9 / peak, 4)
+                  for k in per_frame if per_frame[k] > 0 and sb[k] > 0}
+    traffic = TRAFFIC_NCU.get((a.workload, dom))
 
     line = {
         "metric": METRIC, "value": round(value, 2), "unit": METRIC, "n_gpus": world,
@@ -373,13 +405,14 @@ def main():
                          if total_bytes > 126e6 else "working set fits L2 (no flush)"},
         "e2e": {"value": round(e2e, 2), "unit": METRIC, "h2d_bytes_per_step": 3 * pix,
                 "d2h_bytes_per_step": 3 * pix},
-        "gpu_launches": launches_per_frame * a.steps,
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
-                     "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                     "peak_source": peak_kind, "traffic": None,
-                     "algorithmic_bytes_per_launch": sb[dom]},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": dom, "kernels": STAGE_KERNELS[dom],
+                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": sb[dom]},
         "pipeline": {"algorithmic_bytes_per_frame": total_bytes,
                      "stage_ms_per_frame": {k: round(v, 5) for k, v in per_frame.items()},
+                     "stage_frac_of_hbm": stage_frac,
                      "frac_of_hbm_roofline": round(total_bytes / (ms / a.steps * 1e-3) / 1e9 / peak, 4)},
         "clocks": clocks,
     }

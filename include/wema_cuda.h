@@ -105,13 +105,18 @@ enum {
 };
 long wema_cuda_session_read(wema_cuda_session *s, int what, int channel, float *h_dst, size_t cap);
 
-/* Per-stage device timing with CUDA events on the session's stream:
- * stages are forward DWT level 0, forward DWT levels >= 1, threshold,
- * temporal filter + amplification, inverse DWT, luma transfer.  times_ms[6]
- * receives the accumulated milliseconds, *frames the frames timed. */
-enum { WEMA_CUDA_STAGES = 6 };
+/* Per-stage device timing with CUDA events on each stage's stream: stages are
+ * forward DWT level 0, forward DWT levels >= 1, threshold, temporal filter,
+ * inverse DWT levels >= 1, inverse DWT level 0 (with the colour output),
+ * luma transfer.  times_ms[7] receives the accumulated milliseconds, *frames
+ * the frames timed.  No counterpart in the reference (instrumentation). */
+enum { WEMA_CUDA_STAGES = 7 };
 int wema_cuda_set_timing(wema_cuda_session *s, int enable);
 int wema_cuda_stage_times(wema_cuda_session *s, double *times_ms, long long *frames);
+
+/* Kernel launches this session has issued so far (all frames).  No
+ * counterpart in the reference (instrumentation). */
+int wema_cuda_session_launches(wema_cuda_session *s, long long *launches);
 
 /* Exact reference threshold of a device array of n floats (plain flat
  * order), written to *d_thr; d_sum optional.  Allocates its scratch. */

@@ -6,7 +6,7 @@
 // planes of each level, the threshold scratch and a few scalars.  A frame is
 // a fixed sequence of launches on one stream:
 //   forward DWT (L launches, level 0 reads RGB and converts on the fly)
-//   exact threshold (4 launches, all channels together)
+//   exact threshold (2 launches for all channels; 4 on the first frame)
 //   [first frame: preseed]  IIR + amplify  |  ring push + window amplify
 //   inverse DWT (L launches; colour writes RGB at level 0)
 //   luma: guided filter / Gaussian + RGB transfer + u8 quantisation
@@ -313,6 +313,7 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
         }
         p.prev_n = l > 0 ? g.n[l - 1] : 0;
         if (!cuda_ok(launch_dwt_fwd(mode, nch, p, s_fwd), "forward DWT")) return false;
+        launches++;
         if (l == 0) {
             mark(2 * ST_FWD0 + 1, s_fwd);
             mark(2 * ST_FWD, s_fwd);
@@ -331,6 +332,7 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
             for (int c = 0; c < nch; c++)
                 if (!cuda_ok(launch_iir_preseed(ip, q.coef[c], state[c], warmup, s_tmp), "preseed"))
                     return false;
+            launches += nch;
             frames_processed = warmup;
         }
         const float amp = fade_amp(cfg.amp_factor, frames_processed, warmup);
@@ -339,10 +341,12 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
         q.alpha[1] = q.alpha[2] = amp * 0.5f;
         for (int c = 0; c < nch; c++)
             if (!cuda_ok(launch_iir(ip, q.coef[c], state[c], q.delta[c], s_tmp), "IIR")) return false;
+        launches += nch;
     } else {
         for (int c = 0; c < nch; c++)
             if (!cuda_ok(launch_ring_push(q.coef[c], ring[c], pu, head, s_tmp), "ring push"))
                 return false;
+        launches += nch;
         head = (head + 1) % cfg.temporal_window;
         if (filled < cfg.temporal_window) filled++;
         q.passthrough = filled < cfg.temporal_window;   // wema.c:924-929
@@ -364,6 +368,7 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
             for (int c = 0; c < nch; c++)
                 if (!cuda_ok(launch_window(wp, ring[c], q.delta[c], s_tmp), "window filter"))
                     return false;
+            launches += nch;
         }
     }
     mark(2 * ST_TEMPORAL + 1, s_tmp);
@@ -381,6 +386,7 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
                                       thr_hist ? 1 : 0, s_thr),
                      "threshold"))
             return false;
+        launches += thr_hist ? 2 : 4;   // monoids + walk; partial sums + prefix without history
         thr_hist = true;
         mark(2 * ST_THR + 1, s_thr);
         if (!cuda_ok(cudaEventRecord(q.ev_thr, s_thr), "event record")) return false;
@@ -399,6 +405,7 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
         tp.out_u8 = out_u8;
         tp.out_f32 = out_f32;
         if (!cuda_ok(launch_passthrough(tp, s_inv), "passthrough")) return false;
+        launches++;
     } else {
         mark(2 * ST_INV, s_inv);
         for (int l = L - 1; l >= 0; l--) {
@@ -416,6 +423,10 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
                 iq.alpha[c] = l == 0 ? q.alpha[c] * 0.5f : q.alpha[c];
                 iq.out_planes[c] = (l > 0 || nch == 1 || inspect) ? q.rec[c][l] : nullptr;
             }
+            if (l == 0) {
+                mark(2 * ST_INV + 1, s_inv);
+                mark(2 * ST_INV0, s_inv);
+            }
             int mode = kOutPlanes;
             if (l == 0 && nch == 3) {
                 mode = kOutRgb;
@@ -423,8 +434,9 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
                 iq.out_f32 = out_f32;
             }
             if (!cuda_ok(launch_dwt_inv(nch, mode, iq, s_inv), "inverse DWT")) return false;
+            launches++;
         }
-        mark(2 * ST_INV + 1, s_inv);
+        mark(2 * ST_INV0 + 1, s_inv);
         mark(2 * ST_XFER, s_inv);
         if (nch == 1) {
             TransferParams tp{};
@@ -438,6 +450,7 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
             tp.out_f32 = out_f32;
             tp.edge_aware = cfg.edge_aware;
             if (!cuda_ok(launch_transfer(tp, s_inv), "luma transfer")) return false;
+            launches++;
         }
         mark(2 * ST_XFER + 1, s_inv);
         ev_pending = timing;
@@ -644,6 +657,13 @@ WEMA_API int wema_cuda_stage_times(wema_cuda_session* s, double* times_ms, long 
     if (!S.collect_timing()) return -1;
     for (int k = 0; k < Session::N_STAGE; k++) times_ms[k] = S.stage_ms[k];
     if (frames) *frames = S.stage_frames;
+    return 0;
+}
+
+WEMA_API int wema_cuda_session_launches(wema_cuda_session* s, long long* launches) {
+    clear_error();
+    if (!s || !launches) { set_error("null argument"); return -1; }
+    *launches = s->s.launches;
     return 0;
 }
 

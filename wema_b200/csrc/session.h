@@ -51,6 +51,7 @@ public:
     int head = 0, filled = 0;          // window ring
     bool inspect = false;              // keep input / reconstructed planes for reading back
     long long frames_run = 0;          // frames issued (slot = frames_run % kSlots)
+    long long launches = 0;            // kernels launched by run()
     int last_slot = -1;
 
     // streams: forward DWT, temporal filter, threshold, inverse + output
@@ -70,7 +71,7 @@ public:
     float* stage_f32 = nullptr;        // in [3P] + out [3P]
 
     // per-stage timing (CUDA events on each stage's stream), enabled on demand
-    enum { ST_FWD0, ST_FWD, ST_THR, ST_TEMPORAL, ST_INV, ST_XFER, N_STAGE };
+    enum { ST_FWD0, ST_FWD, ST_THR, ST_TEMPORAL, ST_INV, ST_INV0, ST_XFER, N_STAGE };
     enum { N_EV = 2 * N_STAGE };
     bool timing = false;
     cudaEvent_t ev[N_EV] = {};

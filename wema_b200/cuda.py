@@ -56,6 +56,7 @@ def lib() -> C.CDLL:
         L.wema_cuda_threshold_flat_noalloc.argtypes = [vp, sz, i, vp, vp, vp]
         L.wema_cuda_set_timing.argtypes = [vp, i]
         L.wema_cuda_stage_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
+        L.wema_cuda_session_launches.argtypes = [vp, C.POINTER(C.c_longlong)]
         _lib = L
     return _lib
 
@@ -147,17 +148,23 @@ class Session:
         return buf[:n].copy()
 
     STAGES = ("fwd_dwt_level0", "fwd_dwt_levels", "threshold", "temporal_amplify",
-              "inv_dwt", "luma_transfer")
+              "inv_dwt_levels", "inv_dwt_level0", "luma_transfer")
 
     def set_timing(self, enable: bool):
         _check(lib().wema_cuda_set_timing(self.h, int(bool(enable))), "set_timing")
 
     def stage_times(self):
         """-> (dict stage -> total ms, frames timed)"""
-        t = (C.c_double * 6)()
+        t = (C.c_double * len(self.STAGES))()
         n = C.c_longlong()
         _check(lib().wema_cuda_stage_times(self.h, t, C.byref(n)), "stage_times")
         return dict(zip(self.STAGES, list(t))), n.value
+
+    def launches(self) -> int:
+        """kernel launches issued by this session so far"""
+        n = C.c_longlong()
+        _check(lib().wema_cuda_session_launches(self.h, C.byref(n)), "session_launches")
+        return n.value
 
     def close(self):
         if getattr(self, "h", None):
