@@ -1,14 +1,23 @@
 // dwt.cu - 2D CDF 9/7 lifting DWT, forward and inverse, one fused kernel per
 // pyramid level.
 //
-// A CTA owns a tile of TP x TP subband pairs (TP = 27) of one channel and
-// stages a 64 x 64 sample region - the tile's 54 samples plus a 4-sample
-// halo before and a 6-sample halo after, clipped at the image - in shared
-// memory.  Lifting runs in registers: a warp takes one line of the region,
-// lane k holding the sample pair (2k, 2k+1), and each of the four lifting
-// steps is one warp shuffle for the neighbour plus one FMA.  Rows first, then
-// the tile's columns (forward); columns over the whole region, then the
-// tile's rows (inverse).  Three block barriers per tile.
+// A CTA owns a tile of TP x TP subband pairs (TP = 27) and stages a 64 x 64
+// sample region - the tile's 54 samples plus a 4-sample halo before and a
+// 6-sample halo after, clipped at the image - in shared memory, one plane per
+// channel it handles (level 0 of a colour frame: all three, so each RGB
+// pixel is converted once; otherwise one channel per CTA).  Lifting runs in
+// registers: a warp takes one line of the region, lane k holding the sample
+// pair (2k, 2k+1), and each of the four lifting steps is one warp shuffle for
+// the neighbour plus one FMA.  Rows first, then the tile's columns (forward);
+// columns over the whole region, then the tile's rows (inverse).
+//
+// Sample and pair indices are 32-bit: the runtime caps frames at 2^28 pixels.
+//
+// Shared layout: even and odd samples are stored apart in both directions -
+// sample (y, x) at row (y & 1) * 32 + (y >> 1), column (x & 1) * 48 + (x >> 1)
+// of a plane with an odd row stride - so a warp's row or column access, its
+// staging of 32 consecutive pixels and its quadrant reads and writes all hit
+// 32 distinct banks, and the four subband quadrants are contiguous blocks.
 //
 // Every output depends only on samples within 4 of it, so with the halo each
 // tile is independent: at the image border the reference's whole-sample
@@ -25,13 +34,18 @@ namespace wema {
 constexpr int TP = 27;                 // subband pairs per tile side
 constexpr int SEG = 64;                // staged samples per line (32 lanes x 2)
 constexpr int HALO_L = 4;
-constexpr int RS = SEG + 1;            // shared-memory row stride (odd: column reads spread banks)
+constexpr int ODD_COL = 48;            // first column of the odd samples
+constexpr int RS = 81;                 // plane row stride (odd, >= ODD_COL + 32)
+constexpr int PLANE = SEG * RS;        // floats per staged plane
 constexpr int DWT_THREADS = 256;
 constexpr int NWARP = DWT_THREADS / 32;
+constexpr int RAW_WORDS = 52;          // per-warp RGB24 row buffer (64 pixels + alignment)
 constexpr unsigned FULL = 0xffffffffu;
 
 // first staged sample of the tile starting at pair p0 (even)
 __device__ __forceinline__ int seg_start(int p0) { return p0 == 0 ? 0 : 2 * p0 - HALO_L; }
+__device__ __forceinline__ int prow(int y) { return (y & 1) * 32 + (y >> 1); }
+__device__ __forceinline__ int pcol(int x) { return (x & 1) * ODD_COL + (x >> 1); }
 
 // Forward lifting of one line: lane holds samples s = g0 + 2*lane (even) and
 // s + 1 of a line of n samples.
@@ -71,102 +85,178 @@ __device__ __forceinline__ void lift_inv(float& e, float& o, int s, int n) {
 #undef WEMA_UPDATE
 }
 
-__device__ __forceinline__ float src_value(const FwdLevelParams& p, const float* lut, int mode,
-                                           int c, int chans, long long pi) {
-    if (mode == kSrcPlanes) return p.src_planes[c][pi];
-    float r, g, b;
-    if (mode == kSrcRgbU8) {
-        const uint8_t* q = p.src_u8 + 3 * pi;
-        r = lut[q[0]]; g = lut[q[1]]; b = lut[q[2]];
-    } else {
-        const float* q = p.src_f32 + 3 * pi;
-        r = q[0]; g = q[1]; b = q[2];
-    }
-    const bool vec = pi < p.vec_end;
-    if (chans == 1) return vec ? luma_vec(r, g, b) : luma_tail(r, g, b);
-    float y, cb, cr;
-    if (vec) ycbcr_vec(r, g, b, y, cb, cr);
-    else ycbcr_tail(r, g, b, y, cb, cr);
-    return c == 0 ? y : (c == 1 ? cb : cr);
-}
-
 // ----------------------------------------------------------------- forward
-// grid: (tiles_x, tiles_y, channels); one channel per CTA
-template <int MODE>
-__global__ void __launch_bounds__(DWT_THREADS) k_dwt_fwd(FwdLevelParams p, int chans) {
-    __shared__ float sm[SEG * RS];
-    __shared__ float lut[256];
-    const int c = blockIdx.z;
-    if (MODE == kSrcRgbU8)
-        for (int i = threadIdx.x; i < 256; i += DWT_THREADS) lut[i] = __fdiv_rn((float)i, 255.0f);
+// C == 3: level 0 of a colour frame, all channels in one CTA, grid (tx, ty, 1).
+// C == 1: channel blockIdx.z (planes in), or the luma of an RGB frame.
+template <int C, int MODE>
+__global__ void __launch_bounds__(DWT_THREADS) k_dwt_fwd(FwdLevelParams p) {
+    extern __shared__ __align__(16) float dyn[];
+    float* planes = dyn;                                   // [C][PLANE]
+    float* lut = dyn + C * PLANE;                          // [256]
+    uint32_t* raw = reinterpret_cast<uint32_t*>(lut + 256);   // [NWARP][RAW_WORDS]
+    const int ch0 = (C == 1 && MODE == kSrcPlanes) ? blockIdx.z : 0;
     const int iw = p.iw, ih = p.ih, sw = p.sw, sh = p.sh;
     const int px0 = blockIdx.x * TP, py0 = blockIdx.y * TP;
     const int rx0 = seg_start(px0), ry0 = seg_start(py0);
     const int RW = min(SEG, iw - rx0), RH = min(SEG, ih - ry0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (MODE == kSrcRgbU8) __syncthreads();
 
-    // staging: all PER loads of a thread are issued before any is used
-    constexpr int PER = SEG * SEG / DWT_THREADS;
-    float v[PER];
-#pragma unroll
-    for (int q = 0; q < PER; q++) {
-        const int k = threadIdx.x + q * DWT_THREADS;
-        const int ly = k >> 6, lx = k & 63;
-        v[q] = (ly < RH && lx < RW)
-                   ? src_value(p, lut, MODE, c, chans, (long long)(ry0 + ly) * iw + (rx0 + lx))
-                   : 0.0f;
+    // ---- staging: one warp per region row
+    if (MODE == kSrcRgbU8) {
+        for (int i = threadIdx.x; i < 256; i += DWT_THREADS) lut[i] = __fdiv_rn((float)i, 255.0f);
+        __syncthreads();
     }
+    // every load of the warp's rows is issued before any is used
+    constexpr int RPW = SEG / NWARP;   // region rows per warp
+    if (MODE == kSrcPlanes) {
+        float v[RPW][2];
 #pragma unroll
-    for (int q = 0; q < PER; q++) {
-        const int k = threadIdx.x + q * DWT_THREADS;
-        const int ly = k >> 6, lx = k & 63;
-        if (ly < RH && lx < RW) {
-            sm[ly * RS + lx] = v[q];
-            if (MODE != kSrcPlanes && p.plane_out[c])
-                p.plane_out[c][(long long)(ry0 + ly) * iw + (rx0 + lx)] = v[q];
+        for (int r = 0; r < RPW; r++) {
+            const int ly = warp + r * NWARP;
+            const float* src = p.src_planes[ch0] + (ry0 + ly) * iw + rx0;
+            v[r][0] = (ly < RH && lane < RW) ? src[lane] : 0.0f;
+            v[r][1] = (ly < RH && lane + 32 < RW) ? src[lane + 32] : 0.0f;
+        }
+#pragma unroll
+        for (int r = 0; r < RPW; r++) {
+            const int ly = warp + r * NWARP;
+            if (ly >= RH) continue;
+            float* dst = planes + prow(ly) * RS;
+            if (lane < RW) dst[pcol(lane)] = v[r][0];
+            if (lane + 32 < RW) dst[pcol(lane + 32)] = v[r][1];
+        }
+    } else {
+        float rgb[RPW][2][3];
+        if (MODE == kSrcRgbU8) {
+            // a row's bytes through aligned 32-bit words (an aligned word
+            // that holds a byte of the frame is mapped memory)
+            uint32_t wv[RPW][2];
+            int offs[RPW];
+#pragma unroll
+            for (int r = 0; r < RPW; r++) {
+                const int ly = warp + r * NWARP;
+                const uintptr_t a0 = reinterpret_cast<uintptr_t>(
+                    p.src_u8 + 3 * ((ry0 + min(ly, RH - 1)) * iw + rx0));
+                const uint32_t* w0 = reinterpret_cast<const uint32_t*>(a0 & ~(uintptr_t)3);
+                offs[r] = (int)(a0 & 3);
+                const int nw = (offs[r] + 3 * RW + 3) >> 2;
+                wv[r][0] = (ly < RH && lane < nw) ? __ldg(w0 + lane) : 0u;
+                wv[r][1] = (ly < RH && lane + 32 < nw) ? __ldg(w0 + lane + 32) : 0u;
+            }
+            uint32_t* rb = raw + warp * RAW_WORDS;
+#pragma unroll
+            for (int r = 0; r < RPW; r++) {
+                rb[lane] = wv[r][0];
+                if (lane < RAW_WORDS - 32) rb[lane + 32] = wv[r][1];
+                __syncwarp();
+                const uint8_t* by = reinterpret_cast<const uint8_t*>(rb) + offs[r];
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int lx = lane + 32 * h;
+                    const int k = lx < RW ? 3 * lx : 0;
+                    rgb[r][h][0] = lut[by[k]];
+                    rgb[r][h][1] = lut[by[k + 1]];
+                    rgb[r][h][2] = lut[by[k + 2]];
+                }
+                __syncwarp();   // the buffer takes the next row
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < RPW; r++) {
+                const int ly = warp + r * NWARP;
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int lx = lane + 32 * h;
+                    const bool ok = ly < RH && lx < RW;
+                    const float* q = p.src_f32 + 3 * ((ry0 + (ok ? ly : 0)) * iw + rx0 + (ok ? lx : 0));
+                    rgb[r][h][0] = q[0];
+                    rgb[r][h][1] = q[1];
+                    rgb[r][h][2] = q[2];
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < RPW; r++) {
+            const int ly = warp + r * NWARP;
+            if (ly >= RH) continue;
+            const int rowpix = (ry0 + ly) * iw + rx0;
+            float* dst = planes + prow(ly) * RS;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int lx = lane + 32 * h;
+                if (lx >= RW) continue;
+                const int pi = rowpix + lx;
+                const bool vec = pi < p.vec_end;
+                const float rr = rgb[r][h][0], gg = rgb[r][h][1], bb = rgb[r][h][2];
+                float out[3];
+                if (C == 1) {
+                    out[0] = vec ? luma_vec(rr, gg, bb) : luma_tail(rr, gg, bb);
+                } else if (vec) {
+                    ycbcr_vec(rr, gg, bb, out[0], out[1], out[2]);
+                } else {
+                    ycbcr_tail(rr, gg, bb, out[0], out[1], out[2]);
+                }
+#pragma unroll
+                for (int cc = 0; cc < C; cc++) {
+                    dst[cc * PLANE + pcol(lx)] = out[cc];
+                    if (p.plane_out[cc]) p.plane_out[cc][pi] = out[cc];
+                }
+            }
         }
     }
     __syncthreads();
 
-    if (iw >= 2) {   // rows: every staged row
-        for (int ly = warp; ly < RH; ly += NWARP) {
-            float* row = sm + ly * RS;
-            float e = row[2 * lane], o = row[2 * lane + 1];
-            lift_fwd(e, o, rx0 + 2 * lane, iw);
-            if (2 * lane < RW) row[2 * lane] = e;
-            if (2 * lane + 1 < RW) row[2 * lane + 1] = o;
-        }
+    if (iw >= 2) {   // rows: every staged row of every plane
+#pragma unroll
+        for (int cc = 0; cc < C; cc++)
+            for (int ly = warp; ly < RH; ly += NWARP) {
+                float* row = planes + cc * PLANE + prow(ly) * RS;
+                float e = row[lane], o = row[ODD_COL + lane];
+                lift_fwd(e, o, rx0 + 2 * lane, iw);
+                if (2 * lane < RW) row[lane] = e;
+                if (2 * lane + 1 < RW) row[ODD_COL + lane] = o;
+            }
         __syncthreads();
     }
     const int cx0 = 2 * px0 - rx0, cx1 = min(2 * (px0 + TP), iw) - rx0;
     if (ih >= 2) {   // columns: the tile's own
-        for (int lx = cx0 + warp; lx < cx1; lx += NWARP) {
-            float* col = sm + lx;
-            float e = col[(2 * lane) * RS], o = col[(2 * lane + 1) * RS];
-            lift_fwd(e, o, ry0 + 2 * lane, ih);
-            if (2 * lane < RH) col[(2 * lane) * RS] = e;
-            if (2 * lane + 1 < RH) col[(2 * lane + 1) * RS] = o;
-        }
+#pragma unroll
+        for (int cc = 0; cc < C; cc++)
+            for (int lx = cx0 + warp; lx < cx1; lx += NWARP) {
+                float* col = planes + cc * PLANE + pcol(lx);
+                float e = col[lane * RS], o = col[(32 + lane) * RS];
+                lift_fwd(e, o, ry0 + 2 * lane, ih);
+                if (2 * lane < RH) col[lane * RS] = e;
+                if (2 * lane + 1 < RH) col[(32 + lane) * RS] = o;
+            }
         __syncthreads();
     }
 
     // quadrants: LL (even,even), HL (odd x), LH (odd y), HH; stale entries of
     // odd-sized levels take the previous level's value at the same index
     const int ni = min(TP, sw - px0), nj = min(TP, sh - py0);
-    float* bands = p.coef[c];
-    const float* prev = p.prev[c];
-    for (int k = threadIdx.x; k < ni * nj; k += DWT_THREADS) {
-        const int jj = k / ni, ii = k - jj * ni;
-        const int i = px0 + ii, j = py0 + jj;
-        const int lx = 2 * i - rx0, ly = 2 * j - ry0;
-        const long long o = (long long)j * sw + i;
-        const bool hx = 2 * i + 1 < iw, hy = 2 * j + 1 < ih;
-        p.ll_out[c][o] = sm[ly * RS + lx];
-        bands[o] = hy ? sm[(ly + 1) * RS + lx] : (prev ? prev[o] : 0.0f);                    // LH
-        bands[p.n + o] = (hx && hy) ? sm[(ly + 1) * RS + lx + 1]
-                                    : (prev ? prev[p.prev_n + o] : 0.0f);                 // HH
-        bands[2 * p.n + o] = hx ? sm[ly * RS + lx + 1] : (prev ? prev[2 * p.prev_n + o] : 0.0f); // HL
+    const int qx0 = px0 - (rx0 >> 1), qy0 = py0 - (ry0 >> 1);   // tile's first pair in the region
+    const int i = px0 + lane;
+    const bool hx = 2 * i + 1 < iw;
+    const int n = (int)p.n, pn = (int)p.prev_n;
+#pragma unroll
+    for (int cc = 0; cc < C; cc++) {
+        const int ch = ch0 + cc;
+        const float* pl = planes + cc * PLANE + qx0 + lane;
+        float* ll = p.ll_out[ch];
+        float* bands = p.coef[ch];
+        const float* prev = p.prev[ch];
+        for (int jj = warp; jj < nj; jj += NWARP) {
+            if (lane >= ni) continue;
+            const int j = py0 + jj, ry = qy0 + jj;
+            const int o = j * sw + i;
+            const bool hy = 2 * j + 1 < ih;
+            ll[o] = pl[ry * RS];
+            bands[o] = hy ? pl[(32 + ry) * RS] : (prev ? prev[o] : 0.0f);                        // LH
+            bands[n + o] = (hx && hy) ? pl[(32 + ry) * RS + ODD_COL]
+                                      : (prev ? prev[pn + o] : 0.0f);                          // HH
+            bands[2 * n + o] = hx ? pl[ry * RS + ODD_COL] : (prev ? prev[2 * pn + o] : 0.0f);  // HL
+        }
     }
 }
 
@@ -175,69 +265,64 @@ __global__ void __launch_bounds__(DWT_THREADS) k_dwt_fwd(FwdLevelParams p, int c
 // C == 3: one CTA per tile does all three channels (YCbCr -> RGB at level 0).
 template <int C, int OUT>
 __global__ void __launch_bounds__(DWT_THREADS) k_dwt_inv(InvLevelParams p) {
-    extern __shared__ float dyn[];
-    float(*smem)[SEG * RS] = reinterpret_cast<float(*)[SEG * RS]>(dyn);
-    const int ow = p.ow, oh = p.oh, sw = p.sw;
+    extern __shared__ __align__(16) float dyn[];
+    float* planes = dyn;   // [C][PLANE]
+    const int ow = p.ow, oh = p.oh, sw = p.sw, sh = p.sh;
     const int px0 = blockIdx.x * TP, py0 = blockIdx.y * TP;
     const int rx0 = seg_start(px0), ry0 = seg_start(py0);
     const int RW = min(SEG, ow - rx0), RH = min(SEG, oh - ry0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int c0 = (C == 1) ? blockIdx.z : 0;
+    const int gx0 = rx0 >> 1, gy0 = ry0 >> 1;   // region's first pair
 
-    // interleave LL / HL / LH / HH into the sample grid; bands are amplified
-    // on the way in.  Coefficient and delta loads of all PER samples of a
-    // thread are issued before any is used.
-    constexpr int PER = SEG * SEG / DWT_THREADS;
+    // ---- staging: quadrant q (0 LL, 1 HL, 2 LH, 3 HH) of a plane is a 32 x 32
+    // block of one subband, its rows 32 consecutive pairs; bands are amplified
+    // on the way in.  Each warp takes rows warp, warp + 8, ... of every block,
+    // loads first.
+    const int n = (int)p.n;
+    const int o0 = gy0 * sw + gx0 + lane;
 #pragma unroll
     for (int cc = 0; cc < C; cc++) {
         const int ch = c0 + cc;
-        const float thr = p.thr[ch];
-        const float al = p.alpha[ch];
-        float a[PER], d[PER];
-        bool band[PER];
+        const float thr = p.thr[ch], al = p.alpha[ch];
+        float* pl = planes + cc * PLANE + lane;
 #pragma unroll
-        for (int q = 0; q < PER; q++) {
-            const int k = threadIdx.x + q * DWT_THREADS;
-            const int ly = k >> 6, lx = k & 63;
-            a[q] = 0.0f;
-            d[q] = 0.0f;
-            band[q] = false;
-            if (ly < RH && lx < RW) {
-                const int gy = ry0 + ly, gx = rx0 + lx;
-                const long long o = (long long)(gy >> 1) * sw + (gx >> 1);
-                const int qd = (gx & 1) | ((gy & 1) << 1);
-                if (qd == 0) {
-                    a[q] = p.ll[ch][o];
-                } else {
-                    // LH (qd 2), HH (qd 3), HL (qd 1)
-                    const long long bo = (qd == 1 ? 2 * p.n : (qd == 2 ? 0 : p.n)) + o;
-                    a[q] = p.coef[ch][bo];
-                    d[q] = p.delta[ch][bo];
-                    band[q] = true;
-                }
+        for (int q = 0; q < 4; q++) {
+            const int xo = q & 1, yo = q >> 1;
+            const int boff = q == 1 ? 2 * n : (q == 2 ? 0 : n);   // HL 2, LH 0, HH 1
+            const float* src = q == 0 ? p.ll[ch] : p.coef[ch] + boff;
+            const float* dsrc = p.delta[ch] + boff;
+            const bool okx = 2 * lane + xo < RW;
+            float xv[4], dv[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int qy = warp + NWARP * u;
+                const bool ok = okx && 2 * qy + yo < RH;
+                const int o = o0 + qy * sw;
+                xv[u] = ok ? src[o] : 0.0f;
+                dv[u] = (ok && q != 0) ? dsrc[o] : 0.0f;
             }
-        }
 #pragma unroll
-        for (int q = 0; q < PER; q++) {
-            const int k = threadIdx.x + q * DWT_THREADS;
-            const int ly = k >> 6, lx = k & 63;
-            if (ly < RH && lx < RW) {
-                float x = a[q];
-                if (band[q] && fabsf(x) > thr) x = __fmaf_rn(d[q], al, x);
-                smem[cc][ly * RS + lx] = x;
+            for (int u = 0; u < 4; u++) {
+                const int qy = warp + NWARP * u;
+                if (!(okx && 2 * qy + yo < RH)) continue;
+                float x = xv[u];
+                if (q != 0 && fabsf(x) > thr) x = __fmaf_rn(dv[u], al, x);
+                pl[(yo * 32 + qy) * RS + xo * ODD_COL] = x;
             }
         }
     }
+    (void)sh;
     __syncthreads();
     if (oh >= 2) {   // columns over the whole staged region
 #pragma unroll
         for (int cc = 0; cc < C; cc++)
             for (int lx = warp; lx < RW; lx += NWARP) {
-                float* col = smem[cc] + lx;
-                float e = col[(2 * lane) * RS], o = col[(2 * lane + 1) * RS];
+                float* col = planes + cc * PLANE + pcol(lx);
+                float e = col[lane * RS], o = col[(32 + lane) * RS];
                 lift_inv(e, o, ry0 + 2 * lane, oh);
-                if (2 * lane < RH) col[(2 * lane) * RS] = e;
-                if (2 * lane + 1 < RH) col[(2 * lane + 1) * RS] = o;
+                if (2 * lane < RH) col[lane * RS] = e;
+                if (2 * lane + 1 < RH) col[(32 + lane) * RS] = o;
             }
         __syncthreads();
     }
@@ -247,40 +332,50 @@ __global__ void __launch_bounds__(DWT_THREADS) k_dwt_inv(InvLevelParams p) {
 #pragma unroll
         for (int cc = 0; cc < C; cc++)
             for (int ly = ty0 + warp; ly < ty1; ly += NWARP) {
-                float* row = smem[cc] + ly * RS;
-                float e = row[2 * lane], o = row[2 * lane + 1];
+                float* row = planes + cc * PLANE + prow(ly) * RS;
+                float e = row[lane], o = row[ODD_COL + lane];
                 lift_inv(e, o, rx0 + 2 * lane, ow);
-                if (2 * lane < RW) row[2 * lane] = e;
-                if (2 * lane + 1 < RW) row[2 * lane + 1] = o;
+                if (2 * lane < RW) row[lane] = e;
+                if (2 * lane + 1 < RW) row[ODD_COL + lane] = o;
             }
         __syncthreads();
     }
-    const int nx = tx1 - tx0, ny = ty1 - ty0;
-    for (int k = threadIdx.x; k < nx * ny; k += DWT_THREADS) {
-        const int yy = k / nx, xx = k - yy * nx;
-        const int ly = ty0 + yy, lx = tx0 + xx;
-        const long long pi = (long long)(ry0 + ly) * ow + (rx0 + lx);
-        if (OUT == kOutPlanes) {
+    // ---- output: one warp per tile row, lanes along x
+    for (int ly = ty0 + warp; ly < ty1; ly += NWARP) {
+        const int rowpix = (ry0 + ly) * ow + rx0;
+        const int pr = prow(ly) * RS;
 #pragma unroll
-            for (int cc = 0; cc < C; cc++) p.out_planes[c0 + cc][pi] = smem[cc][ly * RS + lx];
-        } else {
-            const float y = smem[0][ly * RS + lx];
-            const float cb = smem[C > 1 ? 1 : 0][ly * RS + lx];
-            const float cr = smem[C > 2 ? 2 : 0][ly * RS + lx];
-            if (p.out_planes[0]) {
-                p.out_planes[0][pi] = y;
-                p.out_planes[1][pi] = cb;
-                p.out_planes[2][pi] = cr;
-            }
-            float r, g, b;
-            ycbcr_to_rgb(y, cb, cr, r, g, b);
-            if (p.out_u8) {
-                uint8_t* d = p.out_u8 + 3 * pi;
-                d[0] = quant_u8(r); d[1] = quant_u8(g); d[2] = quant_u8(b);
-            }
-            if (p.out_f32) {
-                float* d = p.out_f32 + 3 * pi;
-                d[0] = r; d[1] = g; d[2] = b;
+        for (int h = 0; h < 2; h++) {
+            const int lx = tx0 + lane + 32 * h;
+            if (lx >= tx1) continue;
+            const int pi = rowpix + lx;
+            const int idx = pr + pcol(lx);
+            if (OUT == kOutPlanes) {
+#pragma unroll
+                for (int cc = 0; cc < C; cc++) p.out_planes[c0 + cc][pi] = planes[cc * PLANE + idx];
+            } else {
+                const float y = planes[idx];
+                const float cb = planes[(C > 1 ? PLANE : 0) + idx];
+                const float cr = planes[(C > 2 ? 2 * PLANE : 0) + idx];
+                if (p.out_planes[0]) {
+                    p.out_planes[0][pi] = y;
+                    p.out_planes[1][pi] = cb;
+                    p.out_planes[2][pi] = cr;
+                }
+                float r, g, b;
+                ycbcr_to_rgb(y, cb, cr, r, g, b);
+                if (p.out_u8) {
+                    uint8_t* d = p.out_u8 + 3 * pi;
+                    d[0] = quant_u8(r);
+                    d[1] = quant_u8(g);
+                    d[2] = quant_u8(b);
+                }
+                if (p.out_f32) {
+                    float* d = p.out_f32 + 3 * pi;
+                    d[0] = r;
+                    d[1] = g;
+                    d[2] = b;
+                }
             }
         }
     }
@@ -288,24 +383,41 @@ __global__ void __launch_bounds__(DWT_THREADS) k_dwt_inv(InvLevelParams p) {
 
 // ----------------------------------------------------------------- launch
 
-size_t dwt_smem_bytes(int C) { return (size_t)C * SEG * RS * sizeof(float); }
+static size_t fwd_smem(int C) {
+    return (size_t)C * PLANE * sizeof(float) + 256 * sizeof(float) +
+           (size_t)NWARP * RAW_WORDS * sizeof(uint32_t);
+}
+static size_t inv_smem(int C) { return (size_t)C * PLANE * sizeof(float); }
+size_t dwt_smem_bytes(int C) { return fwd_smem(C); }
 
 static unsigned tiles_of(int pairs) { return (unsigned)((pairs + TP - 1) / TP); }
 
-// the three-channel inverse needs more than the 48 KB default; call once per device
+template <class K>
+static cudaError_t allow_smem(K k, size_t bytes) {
+    return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+// kernels above the 48 KB default; call once per device
 cudaError_t dwt_prepare_device() {
-    return cudaFuncSetAttribute(k_dwt_inv<3, kOutRgb>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)dwt_smem_bytes(3));
+    cudaError_t e = allow_smem(k_dwt_inv<3, kOutRgb>, inv_smem(3));
+    if (e == cudaSuccess) e = allow_smem(k_dwt_fwd<3, kSrcRgbU8>, fwd_smem(3));
+    if (e == cudaSuccess) e = allow_smem(k_dwt_fwd<3, kSrcRgbF32>, fwd_smem(3));
+    return e;
 }
 
 cudaError_t launch_dwt_fwd(int mode, int channels, const FwdLevelParams& p, cudaStream_t st) {
     if (channels != 1 && channels != 3) return cudaErrorInvalidValue;
-    dim3 grid(tiles_of(p.sw), tiles_of(p.sh), channels);
-    switch (mode) {
-        case kSrcPlanes: k_dwt_fwd<kSrcPlanes><<<grid, DWT_THREADS, 0, st>>>(p, channels); break;
-        case kSrcRgbU8: k_dwt_fwd<kSrcRgbU8><<<grid, DWT_THREADS, 0, st>>>(p, channels); break;
-        case kSrcRgbF32: k_dwt_fwd<kSrcRgbF32><<<grid, DWT_THREADS, 0, st>>>(p, channels); break;
-        default: return cudaErrorInvalidValue;
+    const unsigned tx = tiles_of(p.sw), ty = tiles_of(p.sh);
+    if (mode == kSrcPlanes) {
+        k_dwt_fwd<1, kSrcPlanes><<<dim3(tx, ty, channels), DWT_THREADS, fwd_smem(1), st>>>(p);
+    } else if (mode == kSrcRgbU8) {
+        if (channels == 3) k_dwt_fwd<3, kSrcRgbU8><<<dim3(tx, ty, 1), DWT_THREADS, fwd_smem(3), st>>>(p);
+        else k_dwt_fwd<1, kSrcRgbU8><<<dim3(tx, ty, 1), DWT_THREADS, fwd_smem(1), st>>>(p);
+    } else if (mode == kSrcRgbF32) {
+        if (channels == 3) k_dwt_fwd<3, kSrcRgbF32><<<dim3(tx, ty, 1), DWT_THREADS, fwd_smem(3), st>>>(p);
+        else k_dwt_fwd<1, kSrcRgbF32><<<dim3(tx, ty, 1), DWT_THREADS, fwd_smem(1), st>>>(p);
+    } else {
+        return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }
@@ -313,9 +425,9 @@ cudaError_t launch_dwt_fwd(int mode, int channels, const FwdLevelParams& p, cuda
 cudaError_t launch_dwt_inv(int channels, int out_mode, const InvLevelParams& p, cudaStream_t st) {
     const unsigned tx = tiles_of((p.ow + 1) / 2), ty = tiles_of((p.oh + 1) / 2);
     if (out_mode == kOutPlanes && (channels == 1 || channels == 3))
-        k_dwt_inv<1, kOutPlanes><<<dim3(tx, ty, channels), DWT_THREADS, dwt_smem_bytes(1), st>>>(p);
+        k_dwt_inv<1, kOutPlanes><<<dim3(tx, ty, channels), DWT_THREADS, inv_smem(1), st>>>(p);
     else if (out_mode == kOutRgb && channels == 3)
-        k_dwt_inv<3, kOutRgb><<<dim3(tx, ty, 1), DWT_THREADS, dwt_smem_bytes(3), st>>>(p);
+        k_dwt_inv<3, kOutRgb><<<dim3(tx, ty, 1), DWT_THREADS, inv_smem(3), st>>>(p);
     else
         return cudaErrorInvalidValue;
     return cudaGetLastError();

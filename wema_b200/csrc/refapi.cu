@@ -253,6 +253,7 @@ WEMA_API int dwt_init(DWTCoeffs* coeffs, int width, int height, int num_levels) 
     coeffs->orig_height = height;
     coeffs->num_levels = num_levels;
     if (num_levels < 1 || num_levels > WEMA_MAX_LEVELS || width < 1 || height < 1) return -1;
+    if ((long long)width * height > (1LL << 28)) return -1;   // the kernels' 32-bit indexing
     int w = width, h = height;
     for (int l = 0; l < num_levels; l++) {
         w = (w + 1) / 2;
