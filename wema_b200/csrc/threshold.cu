@@ -403,12 +403,32 @@ __device__ __forceinline__ void lane_monoids(const PyrView& v, long long main, l
     }
 }
 
+// The 64 elements of thread ln in the warp's float4 layout when the
+// sub-chunk straddles a (level, slot) segment or is not 16-byte aligned.  Out
+// of line (and reading the view from shared memory) so that the common path
+// stays small in the instruction cache.
+__device__ __noinline__ void load_generic(const PyrView* sv, long long main, long long i0,
+                                          const float* p, bool one, int ln, float* out) {
+    Cursor cu;
+    if (!one && i0 < main) cur_seek(*sv, cu, i0);
+    for (int k = 0; k < 2 * G / 32; k++)
+        for (int i = 0; i < 4; i++) {
+            const long long e = 4 * (32 * k + ln) + i;
+            out[4 * k + i] = one ? __ldg(p + e) : (i0 + e < main ? *cur_addr(*sv, cu, i0 + e) : 0.0f);
+        }
+}
+
 __global__ void __launch_bounds__(32 * MON_WARPS, 2) k_thr_monoids(ThrArgs a) {
     const int ch = blockIdx.y;
     const PyrView& v = a.v[ch];
     const ThrGeom g = thr_geom(v.off6[v.levels]);
     const ThrScratch& sc = a.s[ch];
-    if (blockIdx.x == 0 && threadIdx.x == 0) *sc.counter = 0u;   // the walk's lane counter
+    __shared__ PyrView sv;
+    if (threadIdx.x == 0) {
+        sv = v;
+        if (blockIdx.x == 0) *sc.counter = 0u;   // the walk's lane counter
+    }
+    __syncthreads();
     const int warp = threadIdx.x >> 5, ln = threadIdx.x & 31;
     const int sub = blockIdx.x * MON_WARPS + warp;
     if (sub >= g.nsub) return;   // whole warps only; no block barrier follows
@@ -429,14 +449,12 @@ __global__ void __launch_bounds__(32 * MON_WARPS, 2) k_thr_monoids(ThrArgs a) {
             xv[k][0] = x.x; xv[k][1] = x.y; xv[k][2] = x.z; xv[k][3] = x.w;
         }
     } else {
+        float tmp[8 * G / 32];
+        load_generic(&sv, g.main, i0, p, one, ln, tmp);
 #pragma unroll
-        for (int k = 0; k < 2 * G / 32; k++) {
+        for (int k = 0; k < 2 * G / 32; k++)
 #pragma unroll
-            for (int i = 0; i < 4; i++) {
-                const long long e = 4 * (32 * k + ln) + i;
-                xv[k][i] = one ? __ldg(p + e) : (i0 + e < g.main ? *cur_addr(v, cu, i0 + e) : 0.0f);
-            }
-        }
+            for (int i = 0; i < 4; i++) xv[k][i] = tmp[4 * k + i];
     }
     int ep, eq;                  // candidates of lane ln & 7
     sub_candidates(a, sc, g, (long long)(ln & 7) * g.nsub, sub, ep, eq);
@@ -453,33 +471,28 @@ __global__ void __launch_bounds__(32 * MON_WARPS, 2) k_thr_monoids(ThrArgs a) {
     float dmax = 0.0f;
 #pragma unroll
     for (int i = 0; i < 4; i++) { sp[i] = 0.0f; sq[i] = 0.0f; ps[i] = 0.0f; }
-    const bool has_q = __any_sync(FULL, (EQ[0] | EQ[1] | EQ[2] | EQ[3]) != 0);
-    if (has_q) {   // both candidates in one pass
 #pragma unroll
-        for (int k = 0; k < 2 * G / 32; k++) {
+    for (int k = 0; k < 2 * G / 32; k++) {
 #pragma unroll
-            for (int i = 0; i < 4; i++) {
-                const float a = fabsf(xv[k][i]);
-                const float q = a * sc4[i], q2 = a * sq4[i];
-                const float r = __fsub_rn(__fadd_rn(q, RND), RND);
-                const float r2 = __fsub_rn(__fadd_rn(q2, RND), RND);
-                sp[i] += r;
-                sq[i] += r2;
-                dmax = fmaxf(dmax, fmaxf(fabsf(q - r), fabsf(q2 - r2)));
-                ps[i] += a;
-            }
+        for (int i = 0; i < 4; i++) {
+            const float a = fabsf(xv[k][i]);
+            const float q = a * sc4[i];
+            const float r = __fsub_rn(__fadd_rn(q, RND), RND);
+            sp[i] += r;
+            dmax = fmaxf(dmax, fabsf(q - r));
+            ps[i] += a;
         }
-    } else {
+    }
+    const bool has_q = __any_sync(FULL, (EQ[0] | EQ[1] | EQ[2] | EQ[3]) != 0);
+    if (has_q) {   // secondary candidates
 #pragma unroll
         for (int k = 0; k < 2 * G / 32; k++) {
 #pragma unroll
             for (int i = 0; i < 4; i++) {
-                const float a = fabsf(xv[k][i]);
-                const float q = a * sc4[i];
+                const float q = fabsf(xv[k][i]) * sq4[i];
                 const float r = __fsub_rn(__fadd_rn(q, RND), RND);
-                sp[i] += r;
+                sq[i] += r;
                 dmax = fmaxf(dmax, fabsf(q - r));
-                ps[i] += a;
             }
         }
     }
