@@ -85,6 +85,33 @@ __device__ __forceinline__ void lift_inv(float& e, float& o, int s, int n) {
 #undef WEMA_UPDATE
 }
 
+// Four lines of one plane at a time: their lifting chains are independent, so
+// the warp interleaves them.  b[u] is line u's base (a valid line even when
+// act[u] is false - then nothing is stored); ei / oi address this lane's even
+// and odd sample, s is its even sample's global index, n the line length, lim
+// the staged length.
+template <bool FWD>
+__device__ __forceinline__ void lift4(float* const (&b)[4], const bool (&act)[4], int ei, int oi,
+                                      int s, int n, int lim, int lane) {
+    float e[4], o[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+        e[u] = b[u][ei];
+        o[u] = b[u][oi];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+        if (FWD) lift_fwd(e[u], o[u], s, n);
+        else lift_inv(e[u], o[u], s, n);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+        if (!act[u]) continue;
+        if (2 * lane < lim) b[u][ei] = e[u];
+        if (2 * lane + 1 < lim) b[u][oi] = o[u];
+    }
+}
+
 // ----------------------------------------------------------------- forward
 // C == 3: level 0 of a colour frame, all channels in one CTA, grid (tx, ty, 1).
 // C == 1: channel blockIdx.z (planes in), or the luma of an RGB frame.
@@ -209,12 +236,16 @@ __global__ void __launch_bounds__(DWT_THREADS) k_dwt_fwd(FwdLevelParams p) {
     if (iw >= 2) {   // rows: every staged row of every plane
 #pragma unroll
         for (int cc = 0; cc < C; cc++)
-            for (int ly = warp; ly < RH; ly += NWARP) {
-                float* row = planes + cc * PLANE + prow(ly) * RS;
-                float e = row[lane], o = row[ODD_COL + lane];
-                lift_fwd(e, o, rx0 + 2 * lane, iw);
-                if (2 * lane < RW) row[lane] = e;
-                if (2 * lane + 1 < RW) row[ODD_COL + lane] = o;
+            for (int l0 = warp; l0 < RH; l0 += 4 * NWARP) {
+                float* b[4];
+                bool act[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int ly = l0 + u * NWARP;
+                    act[u] = ly < RH;
+                    b[u] = planes + cc * PLANE + prow(min(ly, RH - 1)) * RS;
+                }
+                lift4<true>(b, act, lane, ODD_COL + lane, rx0 + 2 * lane, iw, RW, lane);
             }
         __syncthreads();
     }
@@ -222,12 +253,16 @@ __global__ void __launch_bounds__(DWT_THREADS) k_dwt_fwd(FwdLevelParams p) {
     if (ih >= 2) {   // columns: the tile's own
 #pragma unroll
         for (int cc = 0; cc < C; cc++)
-            for (int lx = cx0 + warp; lx < cx1; lx += NWARP) {
-                float* col = planes + cc * PLANE + pcol(lx);
-                float e = col[lane * RS], o = col[(32 + lane) * RS];
-                lift_fwd(e, o, ry0 + 2 * lane, ih);
-                if (2 * lane < RH) col[lane * RS] = e;
-                if (2 * lane + 1 < RH) col[(32 + lane) * RS] = o;
+            for (int l0 = cx0 + warp; l0 < cx1; l0 += 4 * NWARP) {
+                float* b[4];
+                bool act[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int lx = l0 + u * NWARP;
+                    act[u] = lx < cx1;
+                    b[u] = planes + cc * PLANE + pcol(min(lx, cx1 - 1));
+                }
+                lift4<true>(b, act, lane * RS, (32 + lane) * RS, ry0 + 2 * lane, ih, RH, lane);
             }
         __syncthreads();
     }
@@ -278,9 +313,29 @@ __global__ void __launch_bounds__(DWT_THREADS) k_dwt_inv(InvLevelParams p) {
     // ---- staging: quadrant q (0 LL, 1 HL, 2 LH, 3 HH) of a plane is a 32 x 32
     // block of one subband, its rows 32 consecutive pairs; bands are amplified
     // on the way in.  Each warp takes rows warp, warp + 8, ... of every block,
-    // loads first.
+    // all of its loads before any store.
     const int n = (int)p.n;
     const int o0 = gy0 * sw + gx0 + lane;
+    float xv[C][4][4], dv[C][3][4];   // every load of the warp's rows first
+#pragma unroll
+    for (int cc = 0; cc < C; cc++) {
+        const int ch = c0 + cc;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int boff = q == 1 ? 2 * n : (q == 2 ? 0 : n);   // HL 2, LH 0, HH 1
+            const float* src = q == 0 ? p.ll[ch] : p.coef[ch] + boff;
+            const float* dsrc = p.delta[ch] + boff;
+            const bool okx = 2 * lane + (q & 1) < RW;
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int qy = warp + NWARP * u;
+                const bool ok = okx && 2 * qy + (q >> 1) < RH;
+                const int o = o0 + qy * sw;
+                xv[cc][q][u] = ok ? __ldg(src + o) : 0.0f;
+                if (q != 0) dv[cc][q - 1][u] = ok ? __ldg(dsrc + o) : 0.0f;
+            }
+        }
+    }
 #pragma unroll
     for (int cc = 0; cc < C; cc++) {
         const int ch = c0 + cc;
@@ -289,25 +344,13 @@ __global__ void __launch_bounds__(DWT_THREADS) k_dwt_inv(InvLevelParams p) {
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const int xo = q & 1, yo = q >> 1;
-            const int boff = q == 1 ? 2 * n : (q == 2 ? 0 : n);   // HL 2, LH 0, HH 1
-            const float* src = q == 0 ? p.ll[ch] : p.coef[ch] + boff;
-            const float* dsrc = p.delta[ch] + boff;
             const bool okx = 2 * lane + xo < RW;
-            float xv[4], dv[4];
-#pragma unroll
-            for (int u = 0; u < 4; u++) {
-                const int qy = warp + NWARP * u;
-                const bool ok = okx && 2 * qy + yo < RH;
-                const int o = o0 + qy * sw;
-                xv[u] = ok ? src[o] : 0.0f;
-                dv[u] = (ok && q != 0) ? dsrc[o] : 0.0f;
-            }
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 const int qy = warp + NWARP * u;
                 if (!(okx && 2 * qy + yo < RH)) continue;
-                float x = xv[u];
-                if (q != 0 && fabsf(x) > thr) x = __fmaf_rn(dv[u], al, x);
+                float x = xv[cc][q][u];
+                if (q != 0 && fabsf(x) > thr) x = __fmaf_rn(dv[cc][q - 1][u], al, x);
                 pl[(yo * 32 + qy) * RS + xo * ODD_COL] = x;
             }
         }
@@ -317,12 +360,16 @@ __global__ void __launch_bounds__(DWT_THREADS) k_dwt_inv(InvLevelParams p) {
     if (oh >= 2) {   // columns over the whole staged region
 #pragma unroll
         for (int cc = 0; cc < C; cc++)
-            for (int lx = warp; lx < RW; lx += NWARP) {
-                float* col = planes + cc * PLANE + pcol(lx);
-                float e = col[lane * RS], o = col[(32 + lane) * RS];
-                lift_inv(e, o, ry0 + 2 * lane, oh);
-                if (2 * lane < RH) col[lane * RS] = e;
-                if (2 * lane + 1 < RH) col[(32 + lane) * RS] = o;
+            for (int l0 = warp; l0 < RW; l0 += 4 * NWARP) {
+                float* b[4];
+                bool act[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int lx = l0 + u * NWARP;
+                    act[u] = lx < RW;
+                    b[u] = planes + cc * PLANE + pcol(min(lx, RW - 1));
+                }
+                lift4<false>(b, act, lane * RS, (32 + lane) * RS, ry0 + 2 * lane, oh, RH, lane);
             }
         __syncthreads();
     }
@@ -331,12 +378,16 @@ __global__ void __launch_bounds__(DWT_THREADS) k_dwt_inv(InvLevelParams p) {
     if (ow >= 2) {   // rows of the tile
 #pragma unroll
         for (int cc = 0; cc < C; cc++)
-            for (int ly = ty0 + warp; ly < ty1; ly += NWARP) {
-                float* row = planes + cc * PLANE + prow(ly) * RS;
-                float e = row[lane], o = row[ODD_COL + lane];
-                lift_inv(e, o, rx0 + 2 * lane, ow);
-                if (2 * lane < RW) row[lane] = e;
-                if (2 * lane + 1 < RW) row[ODD_COL + lane] = o;
+            for (int l0 = ty0 + warp; l0 < ty1; l0 += 4 * NWARP) {
+                float* b[4];
+                bool act[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int ly = l0 + u * NWARP;
+                    act[u] = ly < ty1;
+                    b[u] = planes + cc * PLANE + prow(min(ly, ty1 - 1)) * RS;
+                }
+                lift4<false>(b, act, lane, ODD_COL + lane, rx0 + 2 * lane, ow, RW, lane);
             }
         __syncthreads();
     }
