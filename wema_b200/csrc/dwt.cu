@@ -39,7 +39,6 @@ constexpr int RS = 81;                 // plane row stride (odd, >= ODD_COL + 32
 constexpr int PLANE = SEG * RS;        // floats per staged plane
 constexpr int DWT_THREADS = 256;
 constexpr int NWARP = DWT_THREADS / 32;
-constexpr int RAW_WORDS = 52;          // per-warp RGB24 row buffer (64 pixels + alignment)
 constexpr unsigned FULL = 0xffffffffu;
 
 // first staged sample of the tile starting at pair p0 (even)
@@ -116,11 +115,10 @@ __device__ __forceinline__ void lift4(float* const (&b)[4], const bool (&act)[4]
 // C == 3: level 0 of a colour frame, all channels in one CTA, grid (tx, ty, 1).
 // C == 1: channel blockIdx.z (planes in), or the luma of an RGB frame.
 template <int C, int MODE>
-__global__ void __launch_bounds__(DWT_THREADS) k_dwt_fwd(FwdLevelParams p) {
+__global__ void __launch_bounds__(DWT_THREADS, 3) k_dwt_fwd(FwdLevelParams p) {
     extern __shared__ __align__(16) float dyn[];
     float* planes = dyn;                                   // [C][PLANE]
     float* lut = dyn + C * PLANE;                          // [256]
-    uint32_t* raw = reinterpret_cast<uint32_t*>(lut + 256);   // [NWARP][RAW_WORDS]
     const int ch0 = (C == 1 && MODE == kSrcPlanes) ? blockIdx.z : 0;
     const int iw = p.iw, ih = p.ih, sw = p.sw, sh = p.sh;
     const int px0 = blockIdx.x * TP, py0 = blockIdx.y * TP;
@@ -170,22 +168,31 @@ __global__ void __launch_bounds__(DWT_THREADS) k_dwt_fwd(FwdLevelParams p) {
                 wv[r][0] = (ly < RH && lane < nw) ? __ldg(w0 + lane) : 0u;
                 wv[r][1] = (ly < RH && lane + 32 < nw) ? __ldg(w0 + lane + 32) : 0u;
             }
-            uint32_t* rb = raw + warp * RAW_WORDS;
+            // pixel lx's bytes start at byte off + 3 lx of the row's words:
+            // fetch that word and the next by shuffles, funnel-shift them out
 #pragma unroll
             for (int r = 0; r < RPW; r++) {
-                rb[lane] = wv[r][0];
-                if (lane < RAW_WORDS - 32) rb[lane + 32] = wv[r][1];
-                __syncwarp();
-                const uint8_t* by = reinterpret_cast<const uint8_t*>(rb) + offs[r];
 #pragma unroll
                 for (int h = 0; h < 2; h++) {
-                    const int lx = lane + 32 * h;
-                    const int k = lx < RW ? 3 * lx : 0;
-                    rgb[r][h][0] = lut[by[k]];
-                    rgb[r][h][1] = lut[by[k + 1]];
-                    rgb[r][h][2] = lut[by[k + 2]];
+                    const int b = offs[r] + 3 * (lane + 32 * h);
+                    const int w = b >> 2;           // 0 .. 48
+                    uint32_t lo, hi;
+                    if (h == 0) {                   // w <= 24: both words in the low half
+                        lo = __shfl_sync(FULL, wv[r][0], w);
+                        hi = __shfl_sync(FULL, wv[r][0], w + 1);
+                    } else {
+                        const uint32_t l0 = __shfl_sync(FULL, wv[r][0], w & 31);
+                        const uint32_t l1 = __shfl_sync(FULL, wv[r][1], w & 31);
+                        const uint32_t h0 = __shfl_sync(FULL, wv[r][0], (w + 1) & 31);
+                        const uint32_t h1 = __shfl_sync(FULL, wv[r][1], (w + 1) & 31);
+                        lo = w < 32 ? l0 : l1;
+                        hi = w + 1 < 32 ? h0 : h1;
+                    }
+                    const uint32_t x = __funnelshift_r(lo, hi, 8 * (b & 3));
+                    rgb[r][h][0] = lut[x & 0xFFu];
+                    rgb[r][h][1] = lut[(x >> 8) & 0xFFu];
+                    rgb[r][h][2] = lut[(x >> 16) & 0xFFu];
                 }
-                __syncwarp();   // the buffer takes the next row
             }
         } else {
 #pragma unroll
@@ -434,10 +441,7 @@ __global__ void __launch_bounds__(DWT_THREADS) k_dwt_inv(InvLevelParams p) {
 
 // ----------------------------------------------------------------- launch
 
-static size_t fwd_smem(int C) {
-    return (size_t)C * PLANE * sizeof(float) + 256 * sizeof(float) +
-           (size_t)NWARP * RAW_WORDS * sizeof(uint32_t);
-}
+static size_t fwd_smem(int C) { return (size_t)C * PLANE * sizeof(float) + 256 * sizeof(float); }
 static size_t inv_smem(int C) { return (size_t)C * PLANE * sizeof(float); }
 size_t dwt_smem_bytes(int C) { return fwd_smem(C); }
 
