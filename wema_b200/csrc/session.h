@@ -23,7 +23,7 @@ bool ensure_device(int dev);
 int design_bandpass(float f_low, float f_high, float fs, float c[10], int* warmup);
 float fade_amp(float amp_factor, int frames_before, int warmup);
 
-constexpr int kSlots = 2;   // frames in flight per session (pyramid buffer sets)
+constexpr int kSlots = 4;   // frames in flight per session (pyramid buffer sets)
 
 // Buffers of one frame in flight
 struct Slot {
