@@ -138,6 +138,36 @@ int wema_cuda_threshold_flat(const float *d_x, size_t n, int threshold_form, flo
 int wema_cuda_threshold_flat_noalloc(const float *d_x, size_t n, int threshold_form,
                                      float *d_thr, float *d_sum, void *cuda_stream);
 
+/* ---- Batched streams: one frame tick over many streams ------------------
+ * No counterpart in the reference (its CLI runs one stream per process).
+ * A batch owns the device state of every stream added to it (IIR band-pass
+ * streams, luma or colour, RGB24 frames in device memory) and advances a
+ * chosen set of them by one frame per tick with one launch per kernel type
+ * over all of them.  A stream's frames are bit-identical to what a
+ * wema_cuda_session with the same config produces. */
+typedef struct wema_cuda_batch wema_cuda_batch;
+
+/* Device bytes one batched stream of this config holds (its admission cost). */
+size_t wema_cuda_batch_stream_bytes(const wema_cuda_config *cfg);
+int wema_cuda_batch_create(int device, int max_streams, wema_cuda_batch **out);
+void wema_cuda_batch_destroy(wema_cuda_batch *b);
+/* Allocates the stream's state; *id names it in later calls. */
+int wema_cuda_batch_add(wema_cuda_batch *b, const wema_cuda_config *cfg, int *id);
+/* Waits for the batch's work, then frees the stream's state. */
+int wema_cuda_batch_remove(wema_cuda_batch *b, int id);
+/* One frame of each of the n streams ids[k]: d_in_u8[k] (H x W x 3 RGB24 on
+ * the device) -> d_out_u8[k].  Asynchronous: waits for wait_event (may be
+ * NULL) before reading the inputs, records done_event (may be NULL) once every
+ * output is written and no input is read any more.  A stream may appear once
+ * per tick. */
+int wema_cuda_batch_tick(wema_cuda_batch *b, const int *ids, const void *const *d_in_u8,
+                         void *const *d_out_u8, int n, void *wait_event, void *done_event);
+int wema_cuda_batch_sync(wema_cuda_batch *b);
+/* Ticks issued, kernels launched, streams held. */
+int wema_cuda_batch_stats(wema_cuda_batch *b, long long *ticks, long long *launches, int *live);
+/* WEMA_CUDA_READ_THRESHOLD of a stream's last frame (waits for the batch). */
+int wema_cuda_batch_read(wema_cuda_batch *b, int id, int what, int channel, void *host, size_t bytes);
+
 /* Message of the last failure on this thread ("" if none). */
 const char *wema_cuda_last_error(void);
 

@@ -1,0 +1,149 @@
+"""Batched streams (wema_cuda_batch_*): every stream's frames in a mixed batch
+are bit-identical to the same stream run alone through a wema_cuda_session,
+whatever the mix (sizes, luma / colour, edge-aware / Gaussian, streams that
+skip ticks, streams added and removed between ticks); one batched stream is
+also checked against the oracle (u8 within 1 LSB, colour bit-exact)."""
+import numpy as np
+import pytest
+
+from wema_b200 import cuda as wc
+from wema_b200.synth import SynthSpec, SynthVideo
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("GPU tests need a CUDA device")
+    return torch
+
+
+def frames(w, h, n, seed, fps=30.0):
+    spec = SynthSpec(w, h, fps, seed, [0.9 + 0.1 * seed], [0.4], max(2.0, min(w, h) / 5), 2.0)
+    return SynthVideo(spec).frames(0, n)
+
+
+# (width, height, config): uneven sizes, odd level inputs, both modes
+STREAMS = [
+    (160, 128, dict(amp=50.0)),
+    (200, 120, dict(amp=80.0, edge_aware=False)),
+    (96, 80, dict(amp=120.0, color=True)),
+    (320, 240, dict(amp=30.0, f_high=5.0)),
+    (137, 91, dict(amp=60.0, color=True, fps=60.0, f_high=8.0)),
+    (64, 48, dict(amp=40.0)),
+]
+
+
+def alone(torch, w, h, cfg, u8):
+    """The stream's outputs through a plain session, one frame at a time."""
+    s = wc.Session(width=w, height=h, **cfg)
+    d_in = torch.from_numpy(u8).cuda()
+    outs = []
+    for t in range(u8.shape[0]):
+        o = torch.empty((h, w, 3), dtype=torch.uint8, device="cuda")
+        s.process_u8(d_in[t], o)
+        torch.cuda.synchronize()
+        outs.append(o.cpu().numpy())
+    thr = s.read(wc.READ_THRESHOLD)[0]
+    s.close()
+    return outs, thr
+
+
+def test_batch_matches_streams_alone(torch_cuda):
+    torch = torch_cuda
+    F = 6
+    data = [frames(w, h, F, seed=k + 1, fps=cfg.get("fps", 30.0)) for k, (w, h, cfg) in enumerate(STREAMS)]
+    b = wc.Batch(device=0, max_streams=16)
+    ids = [b.add(w, h, **cfg) for (w, h, cfg) in STREAMS]
+    d_in = [torch.from_numpy(u).cuda() for u in data]
+    outs = [[None] * F for _ in STREAMS]
+    # stream k takes part in tick t when (t + k) % 3 != 2, so streams skip ticks
+    # and every tick mixes a different subset; each stream still sees its frames
+    # in order
+    nxt = [0] * len(STREAMS)
+    tick = 0
+    while min(nxt) < F:
+        sel = [k for k in range(len(STREAMS)) if nxt[k] < F and ((tick + k) % 3 != 2 or tick > 3 * F)]
+        tick += 1
+        if not sel:
+            continue
+        o_t = [torch.empty((STREAMS[k][1], STREAMS[k][0], 3), dtype=torch.uint8, device="cuda") for k in sel]
+        b.tick([ids[k] for k in sel], [d_in[k][nxt[k]] for k in sel], o_t)
+        b.sync()
+        for k, o in zip(sel, o_t):
+            outs[k][nxt[k]] = o.cpu().numpy()
+            nxt[k] += 1
+    st = b.stats()
+    assert st["live"] == len(STREAMS)
+    for k, (w, h, cfg) in enumerate(STREAMS):
+        ref, thr = alone(torch, w, h, cfg, data[k])
+        for t in range(F):
+            assert np.array_equal(outs[k][t], ref[t]), f"stream {k} frame {t}"
+        assert b.threshold(ids[k]) == thr, f"stream {k} threshold"
+    b.close()
+
+
+def test_batch_add_remove(torch_cuda):
+    torch = torch_cuda
+    F = 4
+    (w0, h0, c0), (w1, h1, c1) = STREAMS[0], STREAMS[2]
+    u0, u1 = frames(w0, h0, 2 * F, seed=11), frames(w1, h1, F, seed=12)
+    b = wc.Batch(device=0, max_streams=2)
+    a = b.add(w0, h0, **c0)
+    d0, d1 = torch.from_numpy(u0).cuda(), torch.from_numpy(u1).cuda()
+    got0 = []
+    for t in range(F):
+        o = torch.empty((h0, w0, 3), dtype=torch.uint8, device="cuda")
+        b.tick([a], [d0[t]], [o])
+        b.sync()
+        got0.append(o.cpu().numpy())
+    c = b.add(w1, h1, **c1)
+    with pytest.raises(RuntimeError):
+        b.add(w1, h1, **c1)                  # over max_streams
+    got1 = []
+    for t in range(F):
+        o0 = torch.empty((h0, w0, 3), dtype=torch.uint8, device="cuda")
+        o1 = torch.empty((h1, w1, 3), dtype=torch.uint8, device="cuda")
+        b.tick([c, a], [d1[t], d0[F + t]], [o1, o0])
+        b.sync()
+        got0.append(o0.cpu().numpy())
+        got1.append(o1.cpu().numpy())
+    b.remove(a)
+    with pytest.raises(RuntimeError):
+        b.tick([a], [d0[0]], [o0])           # removed
+    ref0, _ = alone(torch, w0, h0, c0, u0)
+    ref1, _ = alone(torch, w1, h1, c1, u1)
+    for t in range(2 * F):
+        assert np.array_equal(got0[t], ref0[t]), f"stream a frame {t}"
+    for t in range(F):
+        assert np.array_equal(got1[t], ref1[t]), f"stream c frame {t}"
+    b.close()
+
+
+@pytest.mark.parametrize("color", [False, True])
+def test_batch_against_oracle(oracle, torch_cuda, color):
+    torch = torch_cuda
+    w, h, F = 160, 128, 4
+    u8 = frames(w, h, F, seed=21)
+    rgb = oracle.u8_to_float(u8)
+    so = oracle.stream(width=w, height=h, fps=30.0, amp=50.0, f_low=0.5, f_high=3.0, window=32,
+                       edge_aware=True, bilateral=False, color=color, use_iir=True)
+    b = wc.Batch(device=0, max_streams=2)
+    other = b.add(200, 120, amp=80.0)        # a neighbour in every tick
+    sid = b.add(w, h, amp=50.0, f_low=0.5, f_high=3.0, color=color)
+    d = torch.from_numpy(u8).cuda()
+    dn = torch.from_numpy(frames(200, 120, F, seed=22)).cuda()
+    for t in range(F):
+        o = torch.empty((h, w, 3), dtype=torch.uint8, device="cuda")
+        on = torch.empty((120, 200, 3), dtype=torch.uint8, device="cuda")
+        b.tick([other, sid], [dn[t], d[t]], [on, o])
+        b.sync()
+        ref = oracle.float_to_u8(so.process(rgb[t]))
+        diff = np.abs(ref.astype(int) - o.cpu().numpy().astype(int))
+        if color:
+            assert diff.max() == 0, f"frame {t}: colour output"
+        else:
+            assert diff.max() <= 1, f"frame {t}: {diff.max()} LSB"
+    b.close()

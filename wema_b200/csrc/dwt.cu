@@ -28,6 +28,7 @@
 // (dwt.c:45-170 as GCC -Ofast evaluates it), so coefficients are bit-exact.
 #include "common.cuh"
 #include "kernels.h"
+#include "multi.cuh"
 
 namespace wema {
 
@@ -115,13 +116,13 @@ __device__ __forceinline__ void lift4(float* const (&b)[4], const bool (&act)[4]
 // C == 3: level 0 of a colour frame, all channels in one CTA, grid (tx, ty, 1).
 // C == 1: channel blockIdx.z (planes in), or the luma of an RGB frame.
 template <int C, int MODE>
-__global__ void __launch_bounds__(DWT_THREADS, 3) k_dwt_fwd(FwdLevelParams p) {
+__device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, int by, int bz) {
     extern __shared__ __align__(16) float dyn[];
     float* planes = dyn;                                   // [C][PLANE]
     float* lut = dyn + C * PLANE;                          // [256]
-    const int ch0 = (C == 1 && MODE == kSrcPlanes) ? blockIdx.z : 0;
+    const int ch0 = (C == 1 && MODE == kSrcPlanes) ? bz : 0;
     const int iw = p.iw, ih = p.ih, sw = p.sw, sh = p.sh;
-    const int px0 = blockIdx.x * TP, py0 = blockIdx.y * TP;
+    const int px0 = bx * TP, py0 = by * TP;
     const int rx0 = seg_start(px0), ry0 = seg_start(py0);
     const int RW = min(SEG, iw - rx0), RH = min(SEG, ih - ry0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -306,15 +307,15 @@ __global__ void __launch_bounds__(DWT_THREADS, 3) k_dwt_fwd(FwdLevelParams p) {
 // C == 1: grid (tiles_x, tiles_y, channels), planes out.
 // C == 3: one CTA per tile does all three channels (YCbCr -> RGB at level 0).
 template <int C, int OUT>
-__global__ void __launch_bounds__(DWT_THREADS) k_dwt_inv(InvLevelParams p) {
+__device__ __forceinline__ void dwt_inv_body(const InvLevelParams& p, int bx, int by, int bz) {
     extern __shared__ __align__(16) float dyn[];
     float* planes = dyn;   // [C][PLANE]
     const int ow = p.ow, oh = p.oh, sw = p.sw, sh = p.sh;
-    const int px0 = blockIdx.x * TP, py0 = blockIdx.y * TP;
+    const int px0 = bx * TP, py0 = by * TP;
     const int rx0 = seg_start(px0), ry0 = seg_start(py0);
     const int RW = min(SEG, ow - rx0), RH = min(SEG, oh - ry0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int c0 = (C == 1) ? blockIdx.z : 0;
+    const int c0 = (C == 1) ? bz : 0;
     const int gx0 = rx0 >> 1, gy0 = ry0 >> 1;   // region's first pair
 
     // ---- staging: quadrant q (0 LL, 1 HL, 2 LH, 3 HH) of a plane is a 32 x 32
@@ -439,6 +440,30 @@ __global__ void __launch_bounds__(DWT_THREADS) k_dwt_inv(InvLevelParams p) {
     }
 }
 
+// ------------------------------------------------------------- wrappers
+// one stream per launch, and the batched form (task = stream; params in device
+// memory, one entry per task)
+template <int C, int MODE>
+__global__ void __launch_bounds__(DWT_THREADS, 3) k_dwt_fwd(FwdLevelParams p) {
+    dwt_fwd_body<C, MODE>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <int C, int MODE>
+__global__ void __launch_bounds__(DWT_THREADS, 3)
+    k_dwt_fwd_multi(const FwdLevelParams* __restrict__ ps, const int* __restrict__ map) {
+    const TaskBlock t = task_block(map, blockIdx.x);
+    dwt_fwd_body<C, MODE>(ps[t.task], t.x, t.y, t.z);
+}
+template <int C, int OUT>
+__global__ void __launch_bounds__(DWT_THREADS) k_dwt_inv(InvLevelParams p) {
+    dwt_inv_body<C, OUT>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <int C, int OUT>
+__global__ void __launch_bounds__(DWT_THREADS)
+    k_dwt_inv_multi(const InvLevelParams* __restrict__ ps, const int* __restrict__ map) {
+    const TaskBlock t = task_block(map, blockIdx.x);
+    dwt_inv_body<C, OUT>(ps[t.task], t.x, t.y, t.z);
+}
+
 // ----------------------------------------------------------------- launch
 
 static size_t fwd_smem(int C) { return (size_t)C * PLANE * sizeof(float) + 256 * sizeof(float); }
@@ -457,7 +482,47 @@ cudaError_t dwt_prepare_device() {
     cudaError_t e = allow_smem(k_dwt_inv<3, kOutRgb>, inv_smem(3));
     if (e == cudaSuccess) e = allow_smem(k_dwt_fwd<3, kSrcRgbU8>, fwd_smem(3));
     if (e == cudaSuccess) e = allow_smem(k_dwt_fwd<3, kSrcRgbF32>, fwd_smem(3));
+    if (e == cudaSuccess) e = allow_smem(k_dwt_inv_multi<3, kOutRgb>, inv_smem(3));
+    if (e == cudaSuccess) e = allow_smem(k_dwt_fwd_multi<3, kSrcRgbU8>, fwd_smem(3));
     return e;
+}
+
+// ---- batched launches: grid = sum of the tasks' grids (map built by the host)
+unsigned dwt_fwd_grid(const FwdLevelParams& p, int channels_z, unsigned& gx, unsigned& gy) {
+    gx = tiles_of(p.sw);
+    gy = tiles_of(p.sh);
+    return gx * gy * (unsigned)channels_z;
+}
+unsigned dwt_inv_grid(const InvLevelParams& p, int channels_z, unsigned& gx, unsigned& gy) {
+    gx = tiles_of((p.ow + 1) / 2);
+    gy = tiles_of((p.oh + 1) / 2);
+    return gx * gy * (unsigned)channels_z;
+}
+
+cudaError_t launch_dwt_fwd_multi(int mode, int channels, const FwdLevelParams* d_params,
+                                 const int* d_map, unsigned blocks, cudaStream_t st) {
+    if (blocks == 0) return cudaSuccess;
+    if (mode == kSrcPlanes)
+        k_dwt_fwd_multi<1, kSrcPlanes><<<blocks, DWT_THREADS, fwd_smem(1), st>>>(d_params, d_map);
+    else if (mode == kSrcRgbU8 && channels == 3)
+        k_dwt_fwd_multi<3, kSrcRgbU8><<<blocks, DWT_THREADS, fwd_smem(3), st>>>(d_params, d_map);
+    else if (mode == kSrcRgbU8 && channels == 1)
+        k_dwt_fwd_multi<1, kSrcRgbU8><<<blocks, DWT_THREADS, fwd_smem(1), st>>>(d_params, d_map);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dwt_inv_multi(int channels, int out_mode, const InvLevelParams* d_params,
+                                 const int* d_map, unsigned blocks, cudaStream_t st) {
+    if (blocks == 0) return cudaSuccess;
+    if (out_mode == kOutPlanes)
+        k_dwt_inv_multi<1, kOutPlanes><<<blocks, DWT_THREADS, inv_smem(1), st>>>(d_params, d_map);
+    else if (out_mode == kOutRgb && channels == 3)
+        k_dwt_inv_multi<3, kOutRgb><<<blocks, DWT_THREADS, inv_smem(3), st>>>(d_params, d_map);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
 }
 
 cudaError_t launch_dwt_fwd(int mode, int channels, const FwdLevelParams& p, cudaStream_t st) {

@@ -15,6 +15,9 @@
 // the filter need not wait for the threshold.
 #include "common.cuh"
 #include "kernels.h"
+#include "multi.cuh"
+
+#include <string.h>
 
 namespace wema {
 
@@ -63,10 +66,10 @@ __device__ __forceinline__ int level_of(const IirParams& p, long long u, bool& t
     return l;
 }
 
-__global__ void __launch_bounds__(IIR_THREADS) k_iir_preseed(IirDev a) {
+__device__ __forceinline__ void iir_preseed_body(const IirDev& a, int block, int nblocks) {
     const long long pu = a.p.uoff[a.p.levels];
-    for (long long u = blockIdx.x * (long long)IIR_THREADS + threadIdx.x; u < pu;
-         u += (long long)gridDim.x * IIR_THREADS) {
+    for (long long u = block * (long long)IIR_THREADS + threadIdx.x; u < pu;
+         u += (long long)nblocks * IIR_THREADS) {
         bool tail;
         level_of(a.p, u, tail);
         const float x = a.coef[u];
@@ -76,16 +79,29 @@ __global__ void __launch_bounds__(IIR_THREADS) k_iir_preseed(IirDev a) {
     }
 }
 
-__global__ void __launch_bounds__(IIR_THREADS) k_iir(IirDev a) {
+__device__ __forceinline__ void iir_body(const IirDev& a, int block, int nblocks) {
     const long long pu = a.p.uoff[a.p.levels];
-    for (long long u = blockIdx.x * (long long)IIR_THREADS + threadIdx.x; u < pu;
-         u += (long long)gridDim.x * IIR_THREADS) {
+    for (long long u = block * (long long)IIR_THREADS + threadIdx.x; u < pu;
+         u += (long long)nblocks * IIR_THREADS) {
         bool tail;
         level_of(a.p, u, tail);
         float4 st = a.state[u];
         a.delta_out[u] = cascade(a.p.c, st, a.coef[u], tail);
         a.state[u] = st;
     }
+}
+
+__global__ void __launch_bounds__(IIR_THREADS) k_iir_preseed(IirDev a) {
+    iir_preseed_body(a, blockIdx.x, gridDim.x);
+}
+__global__ void __launch_bounds__(IIR_THREADS) k_iir(IirDev a) { iir_body(a, blockIdx.x, gridDim.x); }
+// batched: task = one (stream, channel); the task's grid x is its block count
+__global__ void __launch_bounds__(IIR_THREADS)
+    k_iir_multi(const IirDev* __restrict__ as, const int* __restrict__ map, int preseed) {
+    const TaskBlock t = task_block(map, blockIdx.x);
+    const int nb = map[map[0] + 2 + t.task];
+    if (preseed) iir_preseed_body(as[t.task], t.x, nb);
+    else iir_body(as[t.task], t.x, nb);
 }
 
 __global__ void __launch_bounds__(IIR_THREADS) k_amplify(IirDev a) {
@@ -138,6 +154,28 @@ cudaError_t launch_amplify(const IirParams& p, const float* coef, const float* d
     a.alpha = alpha;
     a.amplified = amplified;
     k_amplify<<<grid_for(p.uoff[p.levels]), IIR_THREADS, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+// ---- batched filter (the host fills one IirDev per stream and channel)
+size_t iir_args_bytes() { return sizeof(IirDev); }
+
+unsigned iir_args_fill(void* dst, const IirParams& p, const float* coef, float4* state, float* delta,
+                       int warmup) {
+    IirDev a{};
+    a.p = p;
+    a.coef = coef;
+    a.state = state;
+    a.delta_out = delta;
+    a.warmup = warmup;
+    memcpy(dst, &a, sizeof a);
+    return (unsigned)grid_for(p.uoff[p.levels]);
+}
+
+cudaError_t launch_iir_multi(const void* d_args, const int* d_map, unsigned blocks, int preseed,
+                             cudaStream_t st) {
+    if (blocks == 0) return cudaSuccess;
+    k_iir_multi<<<blocks, IIR_THREADS, 0, st>>>(static_cast<const IirDev*>(d_args), d_map, preseed);
     return cudaGetLastError();
 }
 

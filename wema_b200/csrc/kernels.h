@@ -122,4 +122,28 @@ cudaError_t launch_ring_push(const float* coef, float* ring, long long pu, int s
 cudaError_t launch_window(const WindowParams& wp, const float* ring, float* delta,
                           cudaStream_t st);
 
+// ---- batched launches: one launch of a kernel over many streams --------------
+// Every launch takes a device array of per-task parameters and a task map
+// (multi.cuh); `blocks` is the sum of the tasks' grids.
+unsigned dwt_fwd_grid(const FwdLevelParams& p, int channels_z, unsigned& gx, unsigned& gy);
+unsigned dwt_inv_grid(const InvLevelParams& p, int channels_z, unsigned& gx, unsigned& gy);
+cudaError_t launch_dwt_fwd_multi(int mode, int channels, const FwdLevelParams* d_params,
+                                 const int* d_map, unsigned blocks, cudaStream_t st);
+cudaError_t launch_dwt_inv_multi(int channels, int out_mode, const InvLevelParams* d_params,
+                                 const int* d_map, unsigned blocks, cudaStream_t st);
+size_t thr_args_bytes();
+// grids[stage] = {x, y} for stage 0 partials, 1 prefix, 2 monoids, 3 walk
+cudaError_t thr_args_fill(void* dst, const PyrView* views, int nch, const ThrScratch* scratch,
+                          float* thr, float* sums, int batch_form, int use_hist, unsigned grids[4][2]);
+cudaError_t launch_threshold_multi(int stage, const void* d_args, const int* d_map, unsigned blocks,
+                                   cudaStream_t st);
+size_t iir_args_bytes();
+unsigned iir_args_fill(void* dst, const IirParams& p, const float* coef, float4* state, float* delta,
+                       int warmup);   // returns the task's block count
+cudaError_t launch_iir_multi(const void* d_args, const int* d_map, unsigned blocks, int preseed,
+                             cudaStream_t st);
+unsigned transfer_grid(const TransferParams& p, unsigned& gx, unsigned& gy);
+cudaError_t launch_transfer_multi(int edge_aware, const TransferParams* d_params, const int* d_map,
+                                  unsigned blocks, cudaStream_t st);
+
 }  // namespace wema

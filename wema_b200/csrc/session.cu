@@ -118,7 +118,7 @@ static void layout(Arena& A, Session& s) {
     const Geom& g = s.g;
     const long long pu = g.uoff[g.levels];
     const long long n6 = g.off6[g.levels];
-    for (int b = 0; b < kSlots; b++) {
+    for (int b = 0; b < s.nslots; b++) {
         Slot& q = s.slot[b];
         for (int c = 0; c < s.nch; c++) {
             q.coef[c] = A.take<float>(pu);
@@ -150,9 +150,10 @@ static bool valid_config(const wema_cuda_config& c) {
     return true;
 }
 
-size_t Session::bytes_for(const wema_cuda_config& c) {
+size_t Session::bytes_for(const wema_cuda_config& c, int nslots) {
     if (!valid_config(c)) return 0;
     Session s;
+    s.nslots = nslots < 1 ? 1 : (nslots > kSlots ? kSlots : nslots);
     s.cfg = c;
     s.g = make_geom(c.width, c.height);
     s.nch = c.color_mode ? 3 : 1;
@@ -192,8 +193,9 @@ bool Session::collect_timing() {
     return true;
 }
 
-bool Session::init(const wema_cuda_config& c) {
+bool Session::init(const wema_cuda_config& c, int ns) {
     if (!valid_config(c)) return false;
+    nslots = ns < 1 ? 1 : (ns > kSlots ? kSlots : ns);
     cfg = c;
     if (!ensure_device(c.device)) return false;
     g = make_geom(c.width, c.height);
@@ -274,7 +276,7 @@ PyrView Session::view(int b, int c) const {
 bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, float* out_f32,
                   cudaEvent_t wait, cudaEvent_t done) {
     const int L = g.levels;
-    const int b = (int)(frames_run % kSlots);
+    const int b = (int)(frames_run % nslots);
     Slot& q = slot[b];
     if (timing) {
         if (!collect_timing()) return false;

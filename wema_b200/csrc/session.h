@@ -82,8 +82,9 @@ public:
     bool collect_timing();
 
     ~Session();
-    static size_t bytes_for(const wema_cuda_config& c);
-    bool init(const wema_cuda_config& c);
+    int nslots = kSlots;               // buffer sets in use (a batched stream keeps one)
+    static size_t bytes_for(const wema_cuda_config& c, int nslots = kSlots);
+    bool init(const wema_cuda_config& c, int nslots = kSlots);
     // One frame, asynchronous: waits for `wait` (may be null) before touching
     // in/out, records `done` (may be null) once out is written and in is no
     // longer read.  Exactly one of in_u8 / in_f32 is set; outputs optional.

@@ -15,6 +15,7 @@
 // differ in the last bits only, which the u8 output absorbs (<= 1 LSB).
 #include "common.cuh"
 #include "kernels.h"
+#include "multi.cuh"
 
 namespace wema {
 
@@ -62,14 +63,13 @@ struct GuidedSmem {
     float ha[2][R1][TS + 1];     // row means of a, b
 };
 
-__global__ void __launch_bounds__(SP_THREADS) k_guided_transfer(SpArgs args) {
+__device__ __forceinline__ void guided_body(const TransferParams& p, int bx, int by) {
     extern __shared__ unsigned char raw[];
     GuidedSmem& S = *reinterpret_cast<GuidedSmem*>(raw);
     __shared__ float lut[256];
-    const TransferParams& p = args.p;
     for (int i = threadIdx.x; i < 256; i += SP_THREADS) lut[i] = __fdiv_rn((float)i, 255.0f);
     const int W = p.w, H = p.h;
-    const int x0 = blockIdx.x * TS, y0 = blockIdx.y * TS;
+    const int x0 = bx * TS, y0 = by * TS;
     const int gx0 = x0 - H0, gy0 = y0 - H0;      // region origin (may be negative)
     __syncthreads();
 
@@ -175,14 +175,13 @@ __global__ void __launch_bounds__(SP_THREADS) k_guided_transfer(SpArgs args) {
 constexpr int GH = 2;
 constexpr int RG = TS + 2 * GH;
 
-__global__ void __launch_bounds__(SP_THREADS) k_gauss_transfer(SpArgs args) {
+__device__ __forceinline__ void gauss_body(const TransferParams& p, int bx, int by) {
     __shared__ float P[RG][RG + 1];
     __shared__ float T[RG][TS + 1];
     __shared__ float lut[256];
-    const TransferParams& p = args.p;
     for (int i = threadIdx.x; i < 256; i += SP_THREADS) lut[i] = __fdiv_rn((float)i, 255.0f);
     const int W = p.w, H = p.h;
-    const int x0 = blockIdx.x * TS, y0 = blockIdx.y * TS;
+    const int x0 = bx * TS, y0 = by * TS;
     const int gx0 = x0 - GH, gy0 = y0 - GH;
     const float kw[5] = {1.0f / 16.0f, 4.0f / 16.0f, 6.0f / 16.0f, 4.0f / 16.0f, 1.0f / 16.0f};
     __syncthreads();
@@ -237,6 +236,24 @@ __global__ void __launch_bounds__(SP_THREADS) k_gauss_transfer(SpArgs args) {
     }
 }
 
+__global__ void __launch_bounds__(SP_THREADS) k_guided_transfer(SpArgs args) {
+    guided_body(args.p, blockIdx.x, blockIdx.y);
+}
+__global__ void __launch_bounds__(SP_THREADS) k_gauss_transfer(SpArgs args) {
+    gauss_body(args.p, blockIdx.x, blockIdx.y);
+}
+// batched: task = one stream (edge-aware and Gaussian streams in separate launches)
+__global__ void __launch_bounds__(SP_THREADS)
+    k_guided_transfer_multi(const TransferParams* __restrict__ ps, const int* __restrict__ map) {
+    const TaskBlock t = task_block(map, blockIdx.x);
+    guided_body(ps[t.task], t.x, t.y);
+}
+__global__ void __launch_bounds__(SP_THREADS)
+    k_gauss_transfer_multi(const TransferParams* __restrict__ ps, const int* __restrict__ map) {
+    const TaskBlock t = task_block(map, blockIdx.x);
+    gauss_body(ps[t.task], t.x, t.y);
+}
+
 __global__ void k_passthrough(SpArgs args) {
     const TransferParams& p = args.p;
     const long long n = (long long)p.w * p.h * 3;
@@ -249,8 +266,28 @@ __global__ void k_passthrough(SpArgs args) {
 }
 
 cudaError_t spatial_prepare_device() {
-    return cudaFuncSetAttribute(k_guided_transfer, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sizeof(GuidedSmem));
+    cudaError_t e = cudaFuncSetAttribute(k_guided_transfer, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sizeof(GuidedSmem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_guided_transfer_multi, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(GuidedSmem));
+    return e;
+}
+
+unsigned transfer_grid(const TransferParams& p, unsigned& gx, unsigned& gy) {
+    gx = (unsigned)((p.w + TS - 1) / TS);
+    gy = (unsigned)((p.h + TS - 1) / TS);
+    return gx * gy;
+}
+
+cudaError_t launch_transfer_multi(int edge_aware, const TransferParams* d_params, const int* d_map,
+                                  unsigned blocks, cudaStream_t st) {
+    if (blocks == 0) return cudaSuccess;
+    if (edge_aware)
+        k_guided_transfer_multi<<<blocks, SP_THREADS, sizeof(GuidedSmem), st>>>(d_params, d_map);
+    else
+        k_gauss_transfer_multi<<<blocks, SP_THREADS, 0, st>>>(d_params, d_map);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_transfer(const TransferParams& p, cudaStream_t st) {

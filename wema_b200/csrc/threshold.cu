@@ -41,9 +41,11 @@
 //                   finishes last reduces the eight lane sums and divides.
 // Predictions only decide speed, never the result.
 #include <atomic>
+#include <string.h>
 
 #include "common.cuh"
 #include "kernels.h"
+#include "multi.cuh"
 
 namespace wema {
 
@@ -221,11 +223,11 @@ struct ThrArgs {
 };
 
 // ---- FP64 partial sums: thread (lane j, block tb) covers EPT lane-elements
-__global__ void __launch_bounds__(THR_THREADS) k_thr_partials(ThrArgs a) {
-    const int ch = blockIdx.y;
+__device__ __forceinline__ void thr_partials_body(const ThrArgs& a, int bx, int by) {
+    const int ch = by;
     const PyrView& v = a.v[ch];
     const ThrGeom g = thr_geom(v.off6[v.levels]);
-    const int sub = blockIdx.x;
+    const int sub = bx;
     if (sub >= g.nsub) return;
     const int j = threadIdx.x & 7, tb = threadIdx.x >> 3;
     const long long t0 = (long long)sub * G + (long long)tb * EPT;
@@ -248,8 +250,8 @@ __global__ void __launch_bounds__(THR_THREADS) k_thr_partials(ThrArgs a) {
 }
 
 // ---- exclusive FP64 prefix per lane: one CTA per (lane, channel)
-__global__ void __launch_bounds__(THR_THREADS) k_thr_prefix(ThrArgs a) {
-    const int j = blockIdx.x, ch = blockIdx.y;
+__device__ __forceinline__ void thr_prefix_body(const ThrArgs& a, int bx, int by) {
+    const int j = bx, ch = by;
     const PyrView& v = a.v[ch];
     const ThrGeom g = thr_geom(v.off6[v.levels]);
     const double* part = a.s[ch].part + (long long)j * g.nsub;
@@ -418,19 +420,19 @@ __device__ __noinline__ void load_generic(const PyrView* sv, long long main, lon
         }
 }
 
-__global__ void __launch_bounds__(32 * MON_WARPS, 2) k_thr_monoids(ThrArgs a) {
-    const int ch = blockIdx.y;
+__device__ __forceinline__ void thr_monoids_body(const ThrArgs& a, int bx, int by) {
+    const int ch = by;
     const PyrView& v = a.v[ch];
     const ThrGeom g = thr_geom(v.off6[v.levels]);
     const ThrScratch& sc = a.s[ch];
     __shared__ PyrView sv;
     if (threadIdx.x == 0) {
         sv = v;
-        if (blockIdx.x == 0) *sc.counter = 0u;   // the walk's lane counter
+        if (bx == 0) *sc.counter = 0u;   // the walk's lane counter
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5, ln = threadIdx.x & 31;
-    const int sub = blockIdx.x * MON_WARPS + warp;
+    const int sub = bx * MON_WARPS + warp;
     if (sub >= g.nsub) return;   // whole warps only; no block barrier follows
     const int half = ln & 1;     // this thread's lanes: 4 * half + i
     const long long i0 = (long long)sub * (8 * G);
@@ -694,10 +696,10 @@ __device__ __forceinline__ Mono warp_scan(Mono t, int ln) {
     return t;
 }
 
-__global__ void __launch_bounds__(THR_THREADS, 1) k_thr_walk(ThrArgs a) {
+__device__ __forceinline__ void thr_walk_body(const ThrArgs& a, int bx, int by) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WalkSmem& sm = *reinterpret_cast<WalkSmem*>(smem_raw);
-    const int j = blockIdx.x, ch = blockIdx.y;
+    const int j = bx, ch = by;
     const PyrView& v = a.v[ch];
     const ThrGeom g = thr_geom(v.off6[v.levels]);
     const ThrScratch& sc = a.s[ch];
@@ -1043,6 +1045,41 @@ __global__ void __launch_bounds__(THR_THREADS, 1) k_thr_walk(ThrArgs a) {
     }
 }
 
+// ------------------------------------------------------------- wrappers
+__global__ void __launch_bounds__(THR_THREADS) k_thr_partials(ThrArgs a) {
+    thr_partials_body(a, blockIdx.x, blockIdx.y);
+}
+__global__ void __launch_bounds__(THR_THREADS) k_thr_prefix(ThrArgs a) {
+    thr_prefix_body(a, blockIdx.x, blockIdx.y);
+}
+__global__ void __launch_bounds__(32 * MON_WARPS, 2) k_thr_monoids(ThrArgs a) {
+    thr_monoids_body(a, blockIdx.x, blockIdx.y);
+}
+__global__ void __launch_bounds__(THR_THREADS, 1) k_thr_walk(ThrArgs a) {
+    thr_walk_body(a, blockIdx.x, blockIdx.y);
+}
+// batched: task = one stream's ThrArgs
+__global__ void __launch_bounds__(THR_THREADS)
+    k_thr_partials_multi(const ThrArgs* __restrict__ as, const int* __restrict__ map) {
+    const TaskBlock t = task_block(map, blockIdx.x);
+    thr_partials_body(as[t.task], t.x, t.y);
+}
+__global__ void __launch_bounds__(THR_THREADS)
+    k_thr_prefix_multi(const ThrArgs* __restrict__ as, const int* __restrict__ map) {
+    const TaskBlock t = task_block(map, blockIdx.x);
+    thr_prefix_body(as[t.task], t.x, t.y);
+}
+__global__ void __launch_bounds__(32 * MON_WARPS, 2)
+    k_thr_monoids_multi(const ThrArgs* __restrict__ as, const int* __restrict__ map) {
+    const TaskBlock t = task_block(map, blockIdx.x);
+    thr_monoids_body(as[t.task], t.x, t.y);
+}
+__global__ void __launch_bounds__(THR_THREADS, 1)
+    k_thr_walk_multi(const ThrArgs* __restrict__ as, const int* __restrict__ map) {
+    const TaskBlock t = task_block(map, blockIdx.x);
+    thr_walk_body(as[t.task], t.x, t.y);
+}
+
 cudaError_t thr_prepare_device() {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -1051,6 +1088,9 @@ cudaError_t thr_prepare_device() {
     if (dev >= 0 && dev < 64 && done[dev].load(std::memory_order_acquire)) return cudaSuccess;
     e = cudaFuncSetAttribute(k_thr_walk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(WalkSmem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_thr_walk_multi, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(WalkSmem));
     if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev].store(1, std::memory_order_release);
     return e;
 }
@@ -1077,6 +1117,49 @@ cudaError_t launch_threshold(const PyrView* views, int nch, ThrScratch* scratch,
     }
     k_thr_monoids<<<dim3(max((nsub + MON_WARPS - 1) / MON_WARPS, 1), nch), 32 * MON_WARPS, 0, st>>>(a);
     k_thr_walk<<<dim3(LANES, nch), THR_THREADS, sizeof(WalkSmem), st>>>(a);
+    return cudaGetLastError();
+}
+
+// ---- batched threshold (the host fills one ThrArgs per stream)
+size_t thr_args_bytes() { return sizeof(ThrArgs); }
+
+cudaError_t thr_args_fill(void* dst, const PyrView* views, int nch, const ThrScratch* scratch,
+                          float* thr, float* sums, int batch_form, int use_hist, unsigned grids[4][2]) {
+    if (nch < 1 || nch > 3) return cudaErrorInvalidValue;
+    ThrArgs a{};
+    int nsub = 0;
+    for (int c = 0; c < nch; c++) {
+        a.v[c] = views[c];
+        a.s[c] = scratch[c];
+        nsub = max(nsub, thr_geom(views[c].off6[views[c].levels]).nsub);
+    }
+    a.thr = thr;
+    a.sums = sums;
+    a.batch_form = batch_form;
+    a.use_hist = use_hist;
+    memcpy(dst, &a, sizeof a);
+    grids[0][0] = (unsigned)nsub;                                         // partials
+    grids[1][0] = LANES;                                                  // prefix
+    grids[2][0] = (unsigned)max((nsub + MON_WARPS - 1) / MON_WARPS, 1);   // monoids
+    grids[3][0] = LANES;                                                  // walk
+    for (int k = 0; k < 4; k++) grids[k][1] = (unsigned)nch;
+    if (nsub == 0) grids[0][0] = 0;
+    return cudaSuccess;
+}
+
+cudaError_t launch_threshold_multi(int stage, const void* d_args, const int* d_map, unsigned blocks,
+                                   cudaStream_t st) {
+    if (blocks == 0) return cudaSuccess;
+    cudaError_t e = thr_prepare_device();
+    if (e != cudaSuccess) return e;
+    const ThrArgs* as = static_cast<const ThrArgs*>(d_args);
+    switch (stage) {
+        case 0: k_thr_partials_multi<<<blocks, THR_THREADS, 0, st>>>(as, d_map); break;
+        case 1: k_thr_prefix_multi<<<blocks, THR_THREADS, 0, st>>>(as, d_map); break;
+        case 2: k_thr_monoids_multi<<<blocks, 32 * MON_WARPS, 0, st>>>(as, d_map); break;
+        case 3: k_thr_walk_multi<<<blocks, THR_THREADS, sizeof(WalkSmem), st>>>(as, d_map); break;
+        default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 

@@ -57,6 +57,19 @@ def lib() -> C.CDLL:
         L.wema_cuda_set_timing.argtypes = [vp, i]
         L.wema_cuda_stage_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
         L.wema_cuda_session_launches.argtypes = [vp, C.POINTER(C.c_longlong)]
+        L.wema_cuda_batch_stream_bytes.argtypes = [C.POINTER(Config)]
+        L.wema_cuda_batch_stream_bytes.restype = sz
+        L.wema_cuda_batch_create.argtypes = [i, i, C.POINTER(vp)]
+        L.wema_cuda_batch_destroy.argtypes = [vp]
+        L.wema_cuda_batch_destroy.restype = None
+        L.wema_cuda_batch_add.argtypes = [vp, C.POINTER(Config), C.POINTER(i)]
+        L.wema_cuda_batch_remove.argtypes = [vp, i]
+        L.wema_cuda_batch_tick.argtypes = [vp, C.POINTER(i), C.POINTER(vp), C.POINTER(vp), i, vp, vp]
+        L.wema_cuda_batch_sync.argtypes = [vp]
+        L.wema_cuda_batch_stats.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
+                                            C.POINTER(i)]
+        L.wema_cuda_batch_read.argtypes = [vp, i, i, i, vp, sz]
+        L.wema_cuda_batch_read.restype = C.c_long
         _lib = L
     return _lib
 
@@ -202,3 +215,68 @@ def threshold_flat_noalloc(d_x, threshold_form=THR_SINGLE, stream=None):
     torch.cuda.synchronize()
     v = out.cpu().numpy()
     return np.float32(v[0]), np.float32(v[1])
+
+
+def batch_stream_bytes(**kw) -> int:
+    """Device bytes one batched stream of this config holds (its admission cost)."""
+    c = make_config(**kw)
+    return int(lib().wema_cuda_batch_stream_bytes(C.byref(c)))
+
+
+class Batch:
+    """Many streams advanced one frame per tick, one launch per kernel type
+    over all of them (wema_cuda_batch_*)."""
+
+    def __init__(self, device=0, max_streams=64):
+        self.h = C.c_void_p()
+        self.device = device
+        _check(lib().wema_cuda_batch_create(int(device), int(max_streams), C.byref(self.h)),
+               "batch_create")
+        self.streams = {}     # id -> (width, height, channels)
+
+    def add(self, width, height, **kw) -> int:
+        c = make_config(width, height, device=self.device, **kw)
+        sid = C.c_int()
+        _check(lib().wema_cuda_batch_add(self.h, C.byref(c), C.byref(sid)), "batch_add")
+        self.streams[sid.value] = (width, height, 3 if kw.get("color") else 1)
+        return sid.value
+
+    def remove(self, sid: int):
+        _check(lib().wema_cuda_batch_remove(self.h, int(sid)), "batch_remove")
+        self.streams.pop(sid, None)
+
+    def tick(self, ids, inputs, outputs, wait_event=None, done_event=None):
+        n = len(ids)
+        ia = (C.c_int * n)(*ids)
+        pin = (C.c_void_p * n)(*[_ptr(t) for t in inputs])
+        pout = (C.c_void_p * n)(*[_ptr(t) for t in outputs])
+        w = C.c_void_p(wait_event.cuda_event) if wait_event is not None else None
+        d = C.c_void_p(done_event.cuda_event) if done_event is not None else None
+        _check(lib().wema_cuda_batch_tick(self.h, ia, pin, pout, n, w, d), "batch_tick")
+
+    def sync(self):
+        _check(lib().wema_cuda_batch_sync(self.h), "batch_sync")
+
+    def stats(self):
+        t, l, n = C.c_longlong(), C.c_longlong(), C.c_int()
+        _check(lib().wema_cuda_batch_stats(self.h, C.byref(t), C.byref(l), C.byref(n)), "batch_stats")
+        return {"ticks": t.value, "launches": l.value, "live": n.value}
+
+    def threshold(self, sid: int, channel=0) -> float:
+        f = C.c_float()
+        rc = lib().wema_cuda_batch_read(self.h, int(sid), READ_THRESHOLD, int(channel),
+                                        C.byref(f), 4)
+        if rc < 0:
+            raise RuntimeError(f"batch_read failed: {last_error()}")
+        return f.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().wema_cuda_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
