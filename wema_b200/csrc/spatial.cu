@@ -28,7 +28,7 @@ constexpr int SP_THREADS = 256;
 
 struct SpArgs { TransferParams p; };
 
-__device__ __forceinline__ void load_rgb(const TransferParams& p, const float* lut, long long pi,
+__device__ __forceinline__ void load_rgb(const TransferParams& p, const float* lut, int pi,
                                          float& r, float& g, float& b) {
     if (p.src_u8) {
         const uint8_t* q = p.src_u8 + 3 * pi;
@@ -39,7 +39,7 @@ __device__ __forceinline__ void load_rgb(const TransferParams& p, const float* l
     }
 }
 
-__device__ __forceinline__ void store_rgb(const TransferParams& p, long long pi, float r, float g,
+__device__ __forceinline__ void store_rgb(const TransferParams& p, int pi, float r, float g,
                                           float b, float dy) {
     r = clamp01(__fadd_rn(r, dy));
     g = clamp01(__fadd_rn(g, dy));
@@ -55,119 +55,178 @@ __device__ __forceinline__ void store_rgb(const TransferParams& p, long long pi,
 }
 
 struct GuidedSmem {
-    float I[R0][R0 + 1];
+    float I[R0][R0 + 1];          // guide and p over the 48x48 region, 0 outside the image
     float P[R0][R0 + 1];
-    float hm[4][R0][R1 + 1];     // row means of I, p, I*I, I*p over the region rows
-    float A[R1][R1 + 1];
+    float hm[4][R0][R1 + 1];      // row means of I, p, I*I, I*p (rows outside the image: 0)
+    float A[R1][R1 + 1];          // a, b over the 40x40 first-round region (0 outside)
     float B[R1][R1 + 1];
-    float ha[2][R1][TS + 1];     // row means of a, b
+    float ha[2][R1][TS + 1];      // row means of a, b
+    float dy[TS][TS + 1];         // the smoothed luma delta of the tile
+    float rgb[TS][TS][3];         // the tile's input RGB (reused by the output pass)
+    float rcp[2 * GR + 2];        // 1/k for the clipped window counts k = 1 .. 2 GR + 1
 };
 
+// 1 / (clipped count of a radius-4 window at coordinate c of a line of n)
+__device__ __forceinline__ float inv_count(const float* rcp, int c, int n) {
+    return rcp[min(c + GR, n - 1) - max(c - GR, 0) + 1];
+}
+
+// Box means with the image's edges: every array holds 0 outside the image,
+// so a radius-4 window's sum is its clipped sum, and the mean is that sum
+// times 1/(clipped count).  Sums slide along segments of 8 outputs.
 __device__ __forceinline__ void guided_body(const TransferParams& p, int bx, int by) {
     extern __shared__ unsigned char raw[];
     GuidedSmem& S = *reinterpret_cast<GuidedSmem*>(raw);
     __shared__ float lut[256];
     for (int i = threadIdx.x; i < 256; i += SP_THREADS) lut[i] = __fdiv_rn((float)i, 255.0f);
+    if (threadIdx.x < 2 * GR + 2) S.rcp[threadIdx.x] = threadIdx.x ? __frcp_rn((float)threadIdx.x) : 0.f;
     const int W = p.w, H = p.h;
     const int x0 = bx * TS, y0 = by * TS;
     const int gx0 = x0 - H0, gy0 = y0 - H0;      // region origin (may be negative)
     __syncthreads();
 
-    // I and p over the 48x48 region (positions outside the image unused)
+    // I and p over the 48x48 region
     for (int k = threadIdx.x; k < R0 * R0; k += SP_THREADS) {
-        const int ly = k / R0, lx = k % R0;
+        const int ly = k / R0, lx = k - ly * R0;
         const int gx = gx0 + lx, gy = gy0 + ly;
         float I = 0.f, P = 0.f;
         if (gx >= 0 && gx < W && gy >= 0 && gy < H) {
-            const long long pi = (long long)gy * W + gx;
+            const int pi = gy * W + gx;
             float r, g, b;
             load_rgb(p, lut, pi, r, g, b);
             I = pi < p.vec_end ? luma_vec(r, g, b) : luma_tail(r, g, b);
             P = __fadd_rn(p.gray_out[pi], -I);
+            const int ty = ly - H0, tx = lx - H0;
+            if (ty >= 0 && ty < TS && tx >= 0 && tx < TS) {
+                S.rgb[ty][tx][0] = r;
+                S.rgb[ty][tx][1] = g;
+                S.rgb[ty][tx][2] = b;
+            }
         }
         S.I[ly][lx] = I;
         S.P[ly][lx] = P;
     }
     __syncthreads();
 
-    // row means for columns of the 40-wide first-round region
-    for (int k = threadIdx.x; k < R0 * R1; k += SP_THREADS) {
-        const int ly = k / R1, cx = k % R1;
-        const int gx = x0 - GR + cx;
+    // first round, rows: 48 rows x 5 segments of 8 of the 40 columns
+    if (threadIdx.x < R0 * (R1 / 8)) {
+        const int ly = threadIdx.x / (R1 / 8), c0 = (threadIdx.x % (R1 / 8)) * 8;
         const int gy = gy0 + ly;
-        if (gx < 0 || gx >= W || gy < 0 || gy >= H) continue;
-        const int a = max(gx - GR, 0), b = min(gx + GR + 1, W);
+        const float* Ir = S.I[ly];
+        const float* Pr = S.P[ly];
         float sI = 0.f, sP = 0.f, sII = 0.f, sIP = 0.f;
-        for (int x = a; x < b; x++) {
-            const float I = S.I[ly][x - gx0], P = S.P[ly][x - gx0];
+        // output column cx sits at region column cx + GR; its window is cx .. cx + 2 GR
+#pragma unroll
+        for (int x = c0; x < c0 + 2 * GR; x++) {
+            const float I = Ir[x], P = Pr[x];
             sI = __fadd_rn(sI, I);
             sP = __fadd_rn(sP, P);
-            sII = __fadd_rn(sII, __fmul_rn(I, I));
-            sIP = __fadd_rn(sIP, __fmul_rn(I, P));
+            sII = __fmaf_rn(I, I, sII);
+            sIP = __fmaf_rn(I, P, sIP);
         }
-        const float cnt = (float)(b - a);
-        S.hm[0][ly][cx] = __fdiv_rn(sI, cnt);
-        S.hm[1][ly][cx] = __fdiv_rn(sP, cnt);
-        S.hm[2][ly][cx] = __fdiv_rn(sII, cnt);
-        S.hm[3][ly][cx] = __fdiv_rn(sIP, cnt);
+#pragma unroll
+        for (int cx = c0; cx < c0 + 8; cx++) {
+            const float In = Ir[cx + 2 * GR], Pn = Pr[cx + 2 * GR];
+            sI = __fadd_rn(sI, In);
+            sP = __fadd_rn(sP, Pn);
+            sII = __fmaf_rn(In, In, sII);
+            sIP = __fmaf_rn(In, Pn, sIP);
+            const int gx = x0 - GR + cx;
+            const bool in = gx >= 0 && gx < W && gy >= 0 && gy < H;
+            const float inv = inv_count(S.rcp, gx, W);
+            S.hm[0][ly][cx] = in ? __fmul_rn(sI, inv) : 0.f;
+            S.hm[1][ly][cx] = in ? __fmul_rn(sP, inv) : 0.f;
+            S.hm[2][ly][cx] = in ? __fmul_rn(sII, inv) : 0.f;
+            S.hm[3][ly][cx] = in ? __fmul_rn(sIP, inv) : 0.f;
+            const float Io = Ir[cx], Po = Pr[cx];
+            sI = __fsub_rn(sI, Io);
+            sP = __fsub_rn(sP, Po);
+            sII = __fmaf_rn(-Io, Io, sII);
+            sIP = __fmaf_rn(-Io, Po, sIP);
+        }
     }
     __syncthreads();
 
-    // column means -> a, b over the 40x40 first-round region
-    for (int k = threadIdx.x; k < R1 * R1; k += SP_THREADS) {
-        const int cy = k / R1, cx = k % R1;
-        const int gx = x0 - GR + cx, gy = y0 - GR + cy;
-        if (gx < 0 || gx >= W || gy < 0 || gy >= H) continue;
-        const int a = max(gy - GR, 0), b = min(gy + GR + 1, H);
+    // first round, columns -> a, b: 40 columns x 5 segments of 8 of the 40 rows
+    if (threadIdx.x < R1 * (R1 / 8)) {
+        const int cx = threadIdx.x / (R1 / 8), r0 = (threadIdx.x % (R1 / 8)) * 8;
+        const int gx = x0 - GR + cx;
         float m[4] = {0.f, 0.f, 0.f, 0.f};
-        for (int y = a; y < b; y++)
 #pragma unroll
-            for (int q = 0; q < 4; q++) m[q] = __fadd_rn(m[q], S.hm[q][y - gy0][cx]);
-        const float cnt = (float)(b - a);
+        for (int y = r0; y < r0 + 2 * GR; y++)
 #pragma unroll
-        for (int q = 0; q < 4; q++) m[q] = __fdiv_rn(m[q], cnt);
-        const float mI = m[0], mP = m[1], cII = m[2], cIP = m[3];
-        const float av = __fdiv_rn(__fmaf_rn(-mI, mP, cIP), __fmaf_rn(-mI, mI, __fadd_rn(cII, 0.01f)));
-        S.A[cy][cx] = av;
-        S.B[cy][cx] = __fmaf_rn(-av, mI, mP);
+            for (int q = 0; q < 4; q++) m[q] = __fadd_rn(m[q], S.hm[q][y][cx]);
+#pragma unroll
+        for (int cy = r0; cy < r0 + 8; cy++) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) m[q] = __fadd_rn(m[q], S.hm[q][cy + 2 * GR][cx]);
+            const int gy = y0 - GR + cy;
+            float av = 0.f, bv = 0.f;
+            if (gx >= 0 && gx < W && gy >= 0 && gy < H) {
+                const float inv = inv_count(S.rcp, gy, H);
+                const float mI = __fmul_rn(m[0], inv), mP = __fmul_rn(m[1], inv);
+                const float cII = __fmul_rn(m[2], inv), cIP = __fmul_rn(m[3], inv);
+                av = __fdiv_rn(__fmaf_rn(-mI, mP, cIP), __fmaf_rn(-mI, mI, __fadd_rn(cII, 0.01f)));
+                bv = __fmaf_rn(-av, mI, mP);
+            }
+            S.A[cy][cx] = av;
+            S.B[cy][cx] = bv;
+#pragma unroll
+            for (int q = 0; q < 4; q++) m[q] = __fsub_rn(m[q], S.hm[q][cy][cx]);
+        }
     }
     __syncthreads();
 
-    // second round: row means of a, b for the tile's columns
-    for (int k = threadIdx.x; k < R1 * TS; k += SP_THREADS) {
-        const int cy = k / TS, tx = k % TS;
-        const int gx = x0 + tx, gy = y0 - GR + cy;
-        if (gx >= W || gy < 0 || gy >= H) continue;
-        const int a = max(gx - GR, 0), b = min(gx + GR + 1, W);
+    // second round, rows: 40 rows x 4 segments of 8 of the tile's 32 columns
+    if (threadIdx.x < R1 * (TS / 8)) {
+        const int cy = threadIdx.x / (TS / 8), t0 = (threadIdx.x % (TS / 8)) * 8;
         float sa = 0.f, sb = 0.f;
-        for (int x = a; x < b; x++) {
-            sa = __fadd_rn(sa, S.A[cy][x - (x0 - GR)]);
-            sb = __fadd_rn(sb, S.B[cy][x - (x0 - GR)]);
+        // tile column tx sits at first-round column tx + GR; window tx .. tx + 2 GR
+#pragma unroll
+        for (int x = t0; x < t0 + 2 * GR; x++) {
+            sa = __fadd_rn(sa, S.A[cy][x]);
+            sb = __fadd_rn(sb, S.B[cy][x]);
         }
-        const float cnt = (float)(b - a);
-        S.ha[0][cy][tx] = __fdiv_rn(sa, cnt);
-        S.ha[1][cy][tx] = __fdiv_rn(sb, cnt);
+#pragma unroll
+        for (int tx = t0; tx < t0 + 8; tx++) {
+            sa = __fadd_rn(sa, S.A[cy][tx + 2 * GR]);
+            sb = __fadd_rn(sb, S.B[cy][tx + 2 * GR]);
+            const float inv = inv_count(S.rcp, min(x0 + tx, W - 1), W);
+            S.ha[0][cy][tx] = __fmul_rn(sa, inv);
+            S.ha[1][cy][tx] = __fmul_rn(sb, inv);
+            sa = __fsub_rn(sa, S.A[cy][tx]);
+            sb = __fsub_rn(sb, S.B[cy][tx]);
+        }
+    }
+    __syncthreads();
+
+    // second round, columns: 32 columns x 4 segments of 8 rows -> dy
+    if (threadIdx.x < TS * (TS / 8)) {
+        const int tx = threadIdx.x / (TS / 8), t0 = (threadIdx.x % (TS / 8)) * 8;
+        float sa = 0.f, sb = 0.f;
+#pragma unroll
+        for (int y = t0; y < t0 + 2 * GR; y++) {
+            sa = __fadd_rn(sa, S.ha[0][y][tx]);
+            sb = __fadd_rn(sb, S.ha[1][y][tx]);
+        }
+#pragma unroll
+        for (int ty = t0; ty < t0 + 8; ty++) {
+            sa = __fadd_rn(sa, S.ha[0][ty + 2 * GR][tx]);
+            sb = __fadd_rn(sb, S.ha[1][ty + 2 * GR][tx]);
+            const float inv = inv_count(S.rcp, min(y0 + ty, H - 1), H);
+            const float ma = __fmul_rn(sa, inv), mb = __fmul_rn(sb, inv);
+            S.dy[ty][tx] = __fmaf_rn(ma, S.I[ty + H0][tx + H0], mb);
+            sa = __fsub_rn(sa, S.ha[0][ty][tx]);
+            sb = __fsub_rn(sb, S.ha[1][ty][tx]);
+        }
     }
     __syncthreads();
 
     for (int k = threadIdx.x; k < TS * TS; k += SP_THREADS) {
-        const int ty = k / TS, tx = k % TS;
+        const int ty = k / TS, tx = k - ty * TS;
         const int gx = x0 + tx, gy = y0 + ty;
         if (gx >= W || gy >= H) continue;
-        const int a = max(gy - GR, 0), b = min(gy + GR + 1, H);
-        float sa = 0.f, sb = 0.f;
-        for (int y = a; y < b; y++) {
-            sa = __fadd_rn(sa, S.ha[0][y - (y0 - GR)][tx]);
-            sb = __fadd_rn(sb, S.ha[1][y - (y0 - GR)][tx]);
-        }
-        const float cnt = (float)(b - a);
-        const float ma = __fdiv_rn(sa, cnt), mb = __fdiv_rn(sb, cnt);
-        const float I = S.I[gy - gy0][gx - gx0];
-        const float dy = __fmaf_rn(ma, I, mb);
-        const long long pi = (long long)gy * W + gx;
-        float r, g, bb;
-        load_rgb(p, lut, pi, r, g, bb);
-        store_rgb(p, pi, r, g, bb, dy);
+        store_rgb(p, gy * W + gx, S.rgb[ty][tx][0], S.rgb[ty][tx][1], S.rgb[ty][tx][2], S.dy[ty][tx]);
     }
 }
 

@@ -113,3 +113,27 @@ def plain_fullhd(seed: int = 2) -> SynthSpec:
 def precision_720p(seed: int = 3) -> SynthSpec:
     """1280x720 @240, one disc 0.4 Hz / 0.15 px, noise 3 LSB."""
     return SynthSpec(1280, 720, 240.0, seed, [0.4], [0.15], 30.0, 3.0)
+
+
+def mixed_streams(seed: int = 7):
+    """The 48-stream batched workload: (SynthSpec, stream settings) per stream.
+    16 x 640x480@30, 16 x 1280x720@30, 12 x 1920x1080@60, 4 x 3840x2160@30;
+    each stream its own seed, 1-3 discs at 0.5-4 Hz (0.2-0.5 px), amp 20-150,
+    window 16-64 (recorded; the IIR filter does not use it), band 0.5-5 Hz,
+    luma with the edge-aware guided filter, FP32."""
+    rng = np.random.default_rng(seed)
+    mix = [(640, 480, 30.0, 16), (1280, 720, 30.0, 16), (1920, 1080, 60.0, 12), (3840, 2160, 30.0, 4)]
+    out = []
+    k = 0
+    for (w, h, fps, n) in mix:
+        for _ in range(n):
+            nd = int(rng.integers(1, 4))
+            spec = SynthSpec(w, h, fps, seed=1000 + k,
+                             disc_freq=[float(x) for x in rng.uniform(0.5, 4.0, nd)],
+                             disc_amp=[float(x) for x in rng.uniform(0.2, 0.5, nd)],
+                             disc_radius=30.0 * min(w, h) / 480.0, noise_sigma=2.0)
+            cfg = dict(fps=fps, amp=float(rng.uniform(20.0, 150.0)), f_low=0.5, f_high=5.0,
+                       window=int(rng.integers(16, 65)), color=False, edge_aware=True)
+            out.append((spec, cfg))
+            k += 1
+    return out
