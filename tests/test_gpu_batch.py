@@ -85,6 +85,28 @@ def test_batch_matches_streams_alone(torch_cuda):
     b.close()
 
 
+def test_batch_back_to_back_ticks(torch_cuda):
+    """Ticks issued without waiting (consecutive ticks overlap on the device)
+    give the same frames as streams run alone."""
+    torch = torch_cuda
+    F = 5
+    data = [frames(w, h, F, seed=k + 31, fps=cfg.get("fps", 30.0)) for k, (w, h, cfg) in enumerate(STREAMS)]
+    b = wc.Batch(device=0, max_streams=len(STREAMS))
+    ids = [b.add(w, h, **cfg) for (w, h, cfg) in STREAMS]
+    d_in = [torch.from_numpy(u).cuda() for u in data]
+    outs = [[torch.empty((h, w, 3), dtype=torch.uint8, device="cuda") for _ in range(F)]
+            for (w, h, _) in STREAMS]
+    torch.cuda.synchronize()
+    for t in range(F):
+        b.tick(ids, [d[t] for d in d_in], [o[t] for o in outs])
+    b.sync()
+    for k, (w, h, cfg) in enumerate(STREAMS):
+        ref, _ = alone(torch, w, h, cfg, data[k])
+        for t in range(F):
+            assert np.array_equal(outs[k][t].cpu().numpy(), ref[t]), f"stream {k} frame {t}"
+    b.close()
+
+
 def test_batch_add_remove(torch_cuda):
     torch = torch_cuda
     F = 4

@@ -16,6 +16,12 @@
 // arithmetic is the per-stream path's, so a stream's frames are bit-identical
 // alone and in any mix.
 //
+// Consecutive ticks overlap: the luma transfer of tick t runs on its own
+// lower-priority CUDA stream while tick t+1's forward DWT, threshold and IIR
+// run (their blocks are placed first, the transfer's fill what is left of
+// each SM); tick t+1's inverse DWT, which rewrites the reconstructed luma the
+// transfer reads, waits for it.  The tick's done event follows its transfer.
+//
 // Supported per stream: IIR band-pass, luma (guided filter or Gaussian
 // transfer) or colour, RGB24 frames in device memory.
 #include <string.h>
@@ -74,8 +80,9 @@ public:
     int device = 0;
     int max_streams = 0;
     std::vector<Session*> streams;        // by id; null when removed
-    cudaStream_t st_main = nullptr, st_iir = nullptr;
-    cudaEvent_t ev_fwd = nullptr, ev_iir = nullptr;
+    cudaStream_t st_main = nullptr, st_iir = nullptr, st_xfer = nullptr;
+    cudaEvent_t ev_fwd = nullptr, ev_iir = nullptr, ev_inv = nullptr, ev_xfer = nullptr;
+    bool xfer_pending = false;            // ev_xfer marks a transfer tick t+1 must wait for
     static constexpr int NBUF = 3;
     struct Table {
         char* host = nullptr;
@@ -91,17 +98,17 @@ public:
     std::vector<char> image;
 
     ~Batch() {
-        if (st_main) cudaStreamSynchronize(st_main);
-        if (st_iir) cudaStreamSynchronize(st_iir);
+        for (cudaStream_t st : {st_main, st_iir, st_xfer})
+            if (st) cudaStreamSynchronize(st);
         for (Session* s : streams) delete s;
         for (Table& t : tb) {
             if (t.host) cudaFreeHost(t.host);
             if (t.dev) cudaFree(t.dev);
             if (t.done) cudaEventDestroy(t.done);
         }
-        for (cudaStream_t st : {st_main, st_iir})
+        for (cudaStream_t st : {st_main, st_iir, st_xfer})
             if (st) cudaStreamDestroy(st);
-        for (cudaEvent_t e : {ev_fwd, ev_iir})
+        for (cudaEvent_t e : {ev_fwd, ev_iir, ev_inv, ev_xfer})
             if (e) cudaEventDestroy(e);
     }
 
@@ -109,10 +116,14 @@ public:
         device = dev;
         max_streams = max_n;
         if (!ensure_device(dev)) return false;
+        int lo = 0, hi = 0;
+        if (!cuda_ok(cudaDeviceGetStreamPriorityRange(&lo, &hi), "stream priorities")) return false;
         for (cudaStream_t* st : {&st_main, &st_iir})
-            if (!cuda_ok(cudaStreamCreateWithFlags(st, cudaStreamNonBlocking), "cudaStreamCreate"))
+            if (!cuda_ok(cudaStreamCreateWithPriority(st, cudaStreamNonBlocking, hi), "cudaStreamCreate"))
                 return false;
-        for (cudaEvent_t* e : {&ev_fwd, &ev_iir})
+        if (!cuda_ok(cudaStreamCreateWithPriority(&st_xfer, cudaStreamNonBlocking, lo), "cudaStreamCreate"))
+            return false;
+        for (cudaEvent_t* e : {&ev_fwd, &ev_iir, &ev_inv, &ev_xfer})
             if (!cuda_ok(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate"))
                 return false;
         for (Table& t : tb)
@@ -153,7 +164,8 @@ public:
 
     bool sync() {
         if (!cuda_ok(cudaStreamSynchronize(st_iir), "sync")) return false;
-        return cuda_ok(cudaStreamSynchronize(st_main), "sync");
+        if (!cuda_ok(cudaStreamSynchronize(st_main), "sync")) return false;
+        return cuda_ok(cudaStreamSynchronize(st_xfer), "sync");
     }
 
     // the table image: every launch's parameter array, then its task map
@@ -350,17 +362,24 @@ public:
             if (!go(k, [&] { return launch_threshold_multi(k - L_THR_PART, P(k), M(k), L[k].total, st_main); }, "threshold"))
                 return false;
         if (!cuda_ok(cudaStreamWaitEvent(st_main, ev_iir, 0), "stream wait")) return false;
+        // the previous tick's transfer still reads its reconstructed luma
+        if (xfer_pending && !cuda_ok(cudaStreamWaitEvent(st_main, ev_xfer, 0), "stream wait")) return false;
         for (int k = L_INV3; k <= L_INV0_LUMA; k++)
             if (!go(k, [&] { return launch_dwt_inv_multi(1, kOutPlanes, (const InvLevelParams*)P(k), M(k), L[k].total, st_main); }, "inverse DWT"))
                 return false;
         if (!go(L_INV0_COLOR, [&] { return launch_dwt_inv_multi(3, kOutRgb, (const InvLevelParams*)P(L_INV0_COLOR), M(L_INV0_COLOR), L[L_INV0_COLOR].total, st_main); }, "inverse DWT"))
             return false;
-        if (!go(L_XFER_GUIDED, [&] { return launch_transfer_multi(1, (const TransferParams*)P(L_XFER_GUIDED), M(L_XFER_GUIDED), L[L_XFER_GUIDED].total, st_main); }, "luma transfer"))
+        // the transfer on its own stream, so the next tick's forward half overlaps it
+        if (!cuda_ok(cudaEventRecord(ev_inv, st_main), "event record")) return false;
+        if (!cuda_ok(cudaStreamWaitEvent(st_xfer, ev_inv, 0), "stream wait")) return false;
+        if (!go(L_XFER_GUIDED, [&] { return launch_transfer_multi(1, (const TransferParams*)P(L_XFER_GUIDED), M(L_XFER_GUIDED), L[L_XFER_GUIDED].total, st_xfer); }, "luma transfer"))
             return false;
-        if (!go(L_XFER_GAUSS, [&] { return launch_transfer_multi(0, (const TransferParams*)P(L_XFER_GAUSS), M(L_XFER_GAUSS), L[L_XFER_GAUSS].total, st_main); }, "luma transfer"))
+        if (!go(L_XFER_GAUSS, [&] { return launch_transfer_multi(0, (const TransferParams*)P(L_XFER_GAUSS), M(L_XFER_GAUSS), L[L_XFER_GAUSS].total, st_xfer); }, "luma transfer"))
             return false;
-        if (!cuda_ok(cudaEventRecord(t.done, st_main), "event record")) return false;
-        if (done && !cuda_ok(cudaEventRecord(done, st_main), "event record")) return false;
+        if (!cuda_ok(cudaEventRecord(ev_xfer, st_xfer), "event record")) return false;
+        xfer_pending = true;
+        if (!cuda_ok(cudaEventRecord(t.done, st_xfer), "event record")) return false;
+        if (done && !cuda_ok(cudaEventRecord(done, st_xfer), "event record")) return false;
         t.used = true;
         cur = (cur + 1) % NBUF;
         ticks++;
@@ -443,7 +462,7 @@ WEMA_API int wema_cuda_batch_tick(wema_cuda_batch* b, const int* ids, const void
     std::lock_guard<std::mutex> lk(b->mu);
     if (!cuda_ok(cudaSetDevice(b->b.device), "cudaSetDevice")) return -1;
     if (n == 0) {
-        if (done_event && !cuda_ok(cudaEventRecord((cudaEvent_t)done_event, b->b.st_main), "event record"))
+        if (done_event && !cuda_ok(cudaEventRecord((cudaEvent_t)done_event, b->b.st_xfer), "event record"))
             return -1;
         return 0;
     }

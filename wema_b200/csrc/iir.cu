@@ -22,6 +22,7 @@
 namespace wema {
 
 constexpr int IIR_THREADS = 256;
+constexpr int IIR_U = 4;   // positions a thread has in flight (all loads before any use)
 
 struct IirDev {
     IirParams p;
@@ -79,15 +80,35 @@ __device__ __forceinline__ void iir_preseed_body(const IirDev& a, int block, int
     }
 }
 
+// A thread takes positions u, u + B, u + 2B, u + 3B (B = the task's threads)
+// per pass, so a warp's accesses stay coalesced and four are in flight.
 __device__ __forceinline__ void iir_body(const IirDev& a, int block, int nblocks) {
     const long long pu = a.p.uoff[a.p.levels];
-    for (long long u = block * (long long)IIR_THREADS + threadIdx.x; u < pu;
-         u += (long long)nblocks * IIR_THREADS) {
-        bool tail;
-        level_of(a.p, u, tail);
-        float4 st = a.state[u];
-        a.delta_out[u] = cascade(a.p.c, st, a.coef[u], tail);
-        a.state[u] = st;
+    const long long B = (long long)nblocks * IIR_THREADS;
+    const float* __restrict__ coef = a.coef;
+    float4* __restrict__ state = a.state;
+    float* __restrict__ dout = a.delta_out;
+    for (long long u0 = block * (long long)IIR_THREADS + threadIdx.x; u0 < pu; u0 += IIR_U * B) {
+        float x[IIR_U];
+        float4 st[IIR_U];
+#pragma unroll
+        for (int j = 0; j < IIR_U; j++) {
+            const long long u = u0 + j * B;
+            if (u < pu) {
+                x[j] = __ldg(coef + u);
+                st[j] = state[u];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < IIR_U; j++) {
+            const long long u = u0 + j * B;
+            if (u < pu) {
+                bool tail;
+                level_of(a.p, u, tail);
+                dout[u] = cascade(a.p.c, st[j], x[j], tail);
+                state[u] = st[j];
+            }
+        }
     }
 }
 
@@ -118,7 +139,7 @@ __global__ void __launch_bounds__(IIR_THREADS) k_amplify(IirDev a) {
 }
 
 static int grid_for(long long n) {
-    long long b = (n + IIR_THREADS - 1) / IIR_THREADS;
+    long long b = (n + IIR_THREADS * IIR_U - 1) / (IIR_THREADS * IIR_U);
     return (int)(b < 148 * 16 ? (b > 0 ? b : 1) : 148 * 16);
 }
 

@@ -92,14 +92,32 @@ __device__ __forceinline__ float byte_f(const float* lut, uint32_t w, int k) {
     return lut[(w >> (8 * k)) & 0xffu];
 }
 
+// guide luma of 4 pixels from their 12 RGB24 bytes (words a0 a1 a2); pi = first pixel
+__device__ __forceinline__ void luma4(const float* lut, uint32_t a0, uint32_t a1, uint32_t a2,
+                                      long long pi, long long vec_end, float v[4]) {
+    float r[4], g[4], b[4];
+    r[0] = byte_f(lut, a0, 0); g[0] = byte_f(lut, a0, 1); b[0] = byte_f(lut, a0, 2);
+    r[1] = byte_f(lut, a0, 3); g[1] = byte_f(lut, a1, 0); b[1] = byte_f(lut, a1, 1);
+    r[2] = byte_f(lut, a1, 2); g[2] = byte_f(lut, a1, 3); b[2] = byte_f(lut, a2, 0);
+    r[3] = byte_f(lut, a2, 1); g[3] = byte_f(lut, a2, 2); b[3] = byte_f(lut, a2, 3);
+    if (pi + 3 < vec_end) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) v[j] = luma_vec(r[j], g[j], b[j]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            v[j] = pi + j < vec_end ? luma_vec(r[j], g[j], b[j]) : luma_tail(r[j], g[j], b[j]);
+    }
+}
+
 // Box means with the image's edges: every array holds 0 outside the image,
 // so a radius-4 window's sum is its clipped sum, and the mean is that sum
 // times 1/(clipped count).  Sums slide along segments of 8 (the last round 4)
 // outputs.  Frames whose RGB24 rows are word-aligned (width a multiple of 4)
-// move 4 pixels = 3 words per thread and access.
-__device__ __forceinline__ void guided_body(const TransferParams& p, int bx, int by) {
-    extern __shared__ __align__(16) unsigned char raw[];
-    GuidedSmem& S = *reinterpret_cast<GuidedSmem*>(raw);
+// move 4 pixels = 3 words per thread and access.  IN: the 48x48 region lies
+// inside the image, so no test is needed and every count is 9.
+template <bool IN>
+__device__ __forceinline__ void guided_tile(const TransferParams& p, GuidedSmem& S, int bx, int by) {
     const int W = p.w, H = p.h;
     const int x0 = bx * TS, y0 = by * TS;
     const int gx0 = x0 - H0, gy0 = y0 - H0;      // region origin (may be negative)
@@ -117,7 +135,7 @@ __device__ __forceinline__ void guided_body(const TransferParams& p, int bx, int
             const int k = tid + i * SP_THREADS;
             const int ly = k / 12, g = k - ly * 12;
             const int gx = gx0 + 4 * g, gy = gy0 + ly;
-            ok[i] = k < NG && gx >= 0 && gx < W && gy >= 0 && gy < H;
+            ok[i] = k < NG && (IN || (gx >= 0 && gx < W && gy >= 0 && gy < H));
             if (ok[i]) {
                 const int pi = gy * W + gx;
                 const uint32_t* q = reinterpret_cast<const uint32_t*>(p.src_u8) + 3 * (pi >> 2);
@@ -142,16 +160,8 @@ __device__ __forceinline__ void guided_body(const TransferParams& p, int bx, int
             float4 Iv = make_float4(0.f, 0.f, 0.f, 0.f), Pv = Iv;
             if (ok[i]) {
                 const uint32_t a0 = wv[i][0], a1 = wv[i][1], a2 = wv[i][2];
-                const long long pi = (long long)(gy0 + ly) * W + gx0 + 4 * g;
-                float r, gg, b, v[4];
-                r = byte_f(S.lut, a0, 0); gg = byte_f(S.lut, a0, 1); b = byte_f(S.lut, a0, 2);
-                v[0] = pi < p.vec_end ? luma_vec(r, gg, b) : luma_tail(r, gg, b);
-                r = byte_f(S.lut, a0, 3); gg = byte_f(S.lut, a1, 0); b = byte_f(S.lut, a1, 1);
-                v[1] = pi + 1 < p.vec_end ? luma_vec(r, gg, b) : luma_tail(r, gg, b);
-                r = byte_f(S.lut, a1, 2); gg = byte_f(S.lut, a1, 3); b = byte_f(S.lut, a2, 0);
-                v[2] = pi + 2 < p.vec_end ? luma_vec(r, gg, b) : luma_tail(r, gg, b);
-                r = byte_f(S.lut, a2, 1); gg = byte_f(S.lut, a2, 2); b = byte_f(S.lut, a2, 3);
-                v[3] = pi + 3 < p.vec_end ? luma_vec(r, gg, b) : luma_tail(r, gg, b);
+                float v[4];
+                luma4(S.lut, a0, a1, a2, (long long)(gy0 + ly) * W + gx0 + 4 * g, p.vec_end, v);
                 Iv = make_float4(v[0], v[1], v[2], v[3]);
                 Pv = make_float4(__fadd_rn(gv[i].x, -v[0]), __fadd_rn(gv[i].y, -v[1]),
                                  __fadd_rn(gv[i].z, -v[2]), __fadd_rn(gv[i].w, -v[3]));
@@ -187,7 +197,8 @@ __device__ __forceinline__ void guided_body(const TransferParams& p, int bx, int
     if (tid < R0 * (R1 / 8)) {
         const int ly = tid % R0, c0 = (tid / R0) * 8;
         const int gy = gy0 + ly;
-        const bool rowin = gy >= 0 && gy < H;
+        const bool rowin = IN || (gy >= 0 && gy < H);
+        const float r9 = S.rcp[2 * GR + 1];
         float Iv[16], Pv[16];
 #pragma unroll
         for (int j = 0; j < 4; j++) {
@@ -217,8 +228,8 @@ __device__ __forceinline__ void guided_body(const TransferParams& p, int bx, int
                 sII = __fmaf_rn(In, In, sII);
                 sIP = __fmaf_rn(In, Pn, sIP);
                 const int gx = x0 - GR + c0 + x;
-                const bool in = rowin && gx >= 0 && gx < W;
-                const float inv = inv_count(S.rcp, gx, W);
+                const bool in = IN || (rowin && gx >= 0 && gx < W);
+                const float inv = IN ? r9 : inv_count(S.rcp, gx, W);
                 o[0][j] = in ? __fmul_rn(sI, inv) : 0.f;
                 o[1][j] = in ? __fmul_rn(sP, inv) : 0.f;
                 o[2][j] = in ? __fmul_rn(sII, inv) : 0.f;
@@ -240,7 +251,8 @@ __device__ __forceinline__ void guided_body(const TransferParams& p, int bx, int
     if (tid < R1 * (R1 / 8)) {
         const int cx = tid % R1, r0 = (tid / R1) * 8;
         const int gx = x0 - GR + cx;
-        const bool colin = gx >= 0 && gx < W;
+        const bool colin = IN || (gx >= 0 && gx < W);
+        const float r9 = S.rcp[2 * GR + 1];
         float m[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
         for (int y = r0; y < r0 + 2 * GR; y++)
@@ -255,11 +267,12 @@ __device__ __forceinline__ void guided_body(const TransferParams& p, int bx, int
             const int gy = y0 - GR + cy;
             av[j] = 0.f;
             bv[j] = 0.f;
-            if (colin && gy >= 0 && gy < H) {
-                const float inv = inv_count(S.rcp, gy, H);
+            if (IN || (colin && gy >= 0 && gy < H)) {
+                const float inv = IN ? r9 : inv_count(S.rcp, gy, H);
                 const float mI = __fmul_rn(m[0], inv), mP = __fmul_rn(m[1], inv);
                 const float cII = __fmul_rn(m[2], inv), cIP = __fmul_rn(m[3], inv);
-                av[j] = __fdiv_rn(__fmaf_rn(-mI, mP, cIP), __fmaf_rn(-mI, mI, __fadd_rn(cII, 0.01f)));
+                // the denominator is >= 0.01 - mI^2 + E[I^2] > 0; a within 2 ulp
+                av[j] = __fdividef(__fmaf_rn(-mI, mP, cIP), __fmaf_rn(-mI, mI, __fadd_rn(cII, 0.01f)));
                 bv[j] = __fmaf_rn(-av[j], mI, mP);
             }
 #pragma unroll
@@ -276,6 +289,7 @@ __device__ __forceinline__ void guided_body(const TransferParams& p, int bx, int
     // second round, rows: 40 rows x 4 segments of 8 of the tile's 32 columns
     if (tid < R1 * (TS / 8)) {
         const int cy = tid % R1, t0 = (tid / R1) * 8;
+        const float r9 = S.rcp[2 * GR + 1];
         float Av[16], Bv[16];
 #pragma unroll
         for (int j = 0; j < 4; j++) {
@@ -299,7 +313,7 @@ __device__ __forceinline__ void guided_body(const TransferParams& p, int bx, int
                 const int x = 4 * h + j;
                 sa = __fadd_rn(sa, Av[x + 2 * GR]);
                 sb = __fadd_rn(sb, Bv[x + 2 * GR]);
-                const float inv = inv_count(S.rcp, min(x0 + t0 + x, W - 1), W);
+                const float inv = IN ? r9 : inv_count(S.rcp, min(x0 + t0 + x, W - 1), W);
                 oa[j] = __fmul_rn(sa, inv);
                 ob[j] = __fmul_rn(sb, inv);
                 sa = __fsub_rn(sa, Av[x]);
@@ -314,6 +328,7 @@ __device__ __forceinline__ void guided_body(const TransferParams& p, int bx, int
     // second round, columns -> dy: 32 columns x 8 segments of 4 rows
     {
         const int tx = tid % TS, t0 = (tid / TS) * 4;
+        const float r9 = S.rcp[2 * GR + 1];
         float sa = 0.f, sb = 0.f;
 #pragma unroll
         for (int y = t0; y < t0 + 2 * GR; y++) {
@@ -326,7 +341,7 @@ __device__ __forceinline__ void guided_body(const TransferParams& p, int bx, int
             const int ty = t0 + j;
             sa = __fadd_rn(sa, S.y.sec.ha[0][ty + 2 * GR][tx]);
             sb = __fadd_rn(sb, S.y.sec.ha[1][ty + 2 * GR][tx]);
-            const float inv = inv_count(S.rcp, min(y0 + ty, H - 1), H);
+            const float inv = IN ? r9 : inv_count(S.rcp, min(y0 + ty, H - 1), H);
             d[j] = __fmaf_rn(__fmul_rn(sa, inv), S.I[ty + H0][tx + H0], __fmul_rn(sb, inv));
             sa = __fsub_rn(sa, S.y.sec.ha[0][ty][tx]);
             sb = __fsub_rn(sb, S.y.sec.ha[1][ty][tx]);
@@ -343,7 +358,7 @@ __device__ __forceinline__ void guided_body(const TransferParams& p, int bx, int
     if (fast_out) {
         const int ty = tid >> 3, g = tid & 7;
         const int gx = x0 + 4 * g, gy = y0 + ty;
-        if (gx < W && gy < H) {
+        if (IN || (gx < W && gy < H)) {
             const int pi = gy * W + gx;
             const float4 dv = *reinterpret_cast<const float4*>(&S.y.sec.dy[ty][4 * g]);
             const float dyv[4] = {dv.x, dv.y, dv.z, dv.w};
@@ -379,6 +394,14 @@ __device__ __forceinline__ void guided_body(const TransferParams& p, int bx, int
             store_rgb(p, pi, r, g, b, S.y.sec.dy[ty][tx]);
         }
     }
+}
+
+__device__ __forceinline__ void guided_body(const TransferParams& p, int bx, int by) {
+    extern __shared__ __align__(16) unsigned char raw[];
+    GuidedSmem& S = *reinterpret_cast<GuidedSmem*>(raw);
+    const int gx0 = bx * TS - H0, gy0 = by * TS - H0;
+    if (gx0 >= 0 && gy0 >= 0 && gx0 + R0 <= p.w && gy0 + R0 <= p.h) guided_tile<true>(p, S, bx, by);
+    else guided_tile<false>(p, S, bx, by);
 }
 
 // 5-tap Gaussian fallback: halo 2
