@@ -51,6 +51,8 @@ WORKLOADS = {
                                                      f_high=0.6, color=False, edge_aware=True)),
     # 48 streams of uneven sizes advanced one frame per tick (wema_cuda_batch_*)
     "mixed_streams_48": ("mixed_streams", None),
+    # Poisson stream sessions through the served request loop (wema_cuda_server_*)
+    "served_poisson": ("served_sessions", None),
 }
 METRIC = "Mpix-frames/s"
 
@@ -73,6 +75,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="plain_fullhd_color", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-frames", type=int, default=12, help="reference frames timed on the host")
+    ap.add_argument("--served-seconds", type=float, default=20.0, help="served_poisson measured window")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -406,12 +409,122 @@ def bench_mixed(a, rank, world, local):
         dist.destroy_process_group()
 
 
+def bench_served(a, rank, world, local):
+    """Stream sessions arriving as a Poisson process (2/s, lengths log-uniform
+    5-60 s, the steady-state population open at t = 0) through the served
+    request loop in real time; frames submitted at each stream's own rate.
+    Reports completed Mpix-frames/s, per-frame latency and admission wait
+    over the window after a warm-up."""
+    import heapq
+    import torch
+    from wema_b200 import cuda as wc
+    from wema_b200 import synth as S
+
+    dev = torch.device("cuda", local)            # replicas: every rank serves its own sessions
+    torch.cuda.set_device(dev)
+    warm, window = 3.0, float(a.served_seconds)
+    horizon = warm + window
+    sess = S.served_sessions(seed=11 + rank, horizon_s=horizon)
+    K, R = 4, 12                                       # unique input frames per size; output ring
+    inputs = {}
+    for (_, _, spec, _) in sess:
+        key = (spec.width, spec.height)
+        if key not in inputs:
+            h = torch.empty((K, spec.height, spec.width, 3), dtype=torch.uint8)
+            S.SynthVideo(spec).frames(0, K, out=h.numpy())
+            inputs[key] = h.to(dev)
+    budget = 150 * 10**9
+    srv = wc.Server(device=local, budget_bytes=budget, max_streams=512)
+    rng = np.random.default_rng(5 + rank)
+    ev = []                                            # (time, order, kind, session)
+    for i, (t0, t1, _, _) in enumerate(sess):
+        heapq.heappush(ev, (t0, 2 * i, "open", i))
+        heapq.heappush(ev, (t1, 2 * i + 1, "close", i))
+    sid, nfr, refused = {}, {}, 0
+    # every session's output ring, allocated before the clock starts (clients own them)
+    outs = {i: [torch.empty((spec.height, spec.width, 3), dtype=torch.uint8, device=dev)
+                for _ in range(R)] for i, (_, _, spec, _) in enumerate(sess)}
+    order = 2 * len(sess)
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clk:
+        t_start = time.perf_counter()
+        reset_done = False
+        while ev:
+            t_ev = ev[0][0]
+            now = time.perf_counter() - t_start
+            if not reset_done and now >= warm:
+                srv.stats(reset=True)
+                reset_done = True
+            if t_ev > now:
+                time.sleep(min(t_ev - now, 0.0005))
+                continue
+            _, _, kind, i = heapq.heappop(ev)
+            t0, t1, spec, cfg = sess[i]
+            if kind == "open":
+                sid[i] = srv.open(spec.width, spec.height, **cfg)
+                nfr[i] = 0
+                order += 1
+                heapq.heappush(ev, (t0 + rng.uniform(0, 1.0 / cfg["fps"]), order, "frame", i))
+            elif kind == "frame":
+                if sid.get(i) is None:
+                    continue
+                k = nfr[i]
+                rc = srv.submit(sid[i], inputs[(spec.width, spec.height)][k % K], outs[i][k % R])
+                refused += rc != 0
+                nfr[i] = k + 1
+                t_next = t_ev + 1.0 / cfg["fps"]
+                if t_next < t1:
+                    order += 1
+                    heapq.heappush(ev, (t_next, order, "frame", i))
+            else:
+                srv.close_session(sid[i])
+                sid[i] = None
+        st = srv.stats()
+    srv.drain(120000)
+    clocks = clk.summary()
+    line = {
+        "metric": METRIC, "value": round(st["mpix_frames"] / st["seconds"], 2), "unit": METRIC,
+        "n_gpus": world, "steps": int(st["ticks"]), "warmup": 0,
+        "ms_per_step": round(st["seconds"] * 1e3 / max(st["ticks"], 1), 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "served_poisson", "arrivals_per_s": 2.0, "session_s": "log-uniform 5-60",
+                   "mix": "480p 40%, 720p 30%, 1080p 25%, 2160p 5%; 30/60 fps",
+                   "mode": "IIR 0.5-5 Hz, luma, edge-aware guided filter",
+                   "window_s": window, "warmup_s": warm, "budget_bytes": budget,
+                   "sessions": len(sess), "step": "one tick of the dispatcher",
+                   "parallelism": f"replicas x{world}"},
+        "frames": int(st["frames"]), "frames_refused": int(refused),
+        "latency_ms": {"p50": round(st["latency_p50_ms"], 3), "p99": round(st["latency_p99_ms"], 3),
+                       "max": round(st["latency_max_ms"], 3),
+                       "frame_period_ms": {"60fps": 16.667, "30fps": 33.333}},
+        "admission_wait_ms": {"p50": round(st["admission_wait_p50_ms"], 3),
+                              "max": round(st["admission_wait_max_ms"], 3)},
+        "sessions_admitted": int(st["sessions_admitted"]), "bytes_used_at_end": int(st["bytes_used"]),
+        "dispatcher_ms": {k: round(st[k], 3) for k in ("tick_host_ms_mean", "tick_host_ms_max",
+                                                       "tick_span_ms_mean", "tick_span_ms_max",
+                                                       "admit_ms_max", "retire_ms_max")},
+        "frames_per_tick": round(st["frames"] / max(st["ticks"], 1), 2),
+        "gpu_launches": int(st["launches"]), "clocks": clocks,
+    }
+    srv.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     synth_name, kw = WORKLOADS[a.workload]
+    if a.workload == "served_poisson":
+        if a.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference has no served "
+                                  "form; its CPU path is timed on the mixed_streams_48 sample"}))
+            return
+        return bench_served(a, rank, world, local)
     if a.workload == "mixed_streams_48":
         if a.impl != "reference":
             return bench_mixed(a, rank, world, local)

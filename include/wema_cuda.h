@@ -168,6 +168,68 @@ int wema_cuda_batch_stats(wema_cuda_batch *b, long long *ticks, long long *launc
 /* WEMA_CUDA_READ_THRESHOLD of a stream's last frame (waits for the batch). */
 int wema_cuda_batch_read(wema_cuda_batch *b, int id, int what, int channel, void *host, size_t bytes);
 
+/* ---- Served request loop -------------------------------------------------
+ * No counterpart in the reference (a single-file CLI).  Camera-stream
+ * sessions are admitted against a device-memory budget by their state bytes
+ * (wema_cuda_batch_stream_bytes), queued first-in first-out while the budget
+ * is full, and keep their state on the device until closed.  Frames submitted
+ * at each stream's own rate are batched continuously: a dispatcher thread
+ * puts the oldest pending frame of every live session into the next tick
+ * whenever fewer than three ticks are in flight.  A session's outputs are
+ * bit-identical to the same stream run alone. */
+typedef struct wema_cuda_server wema_cuda_server;
+
+enum {
+    WEMA_CUDA_SESSION_QUEUED = 0,   /* waiting for budget */
+    WEMA_CUDA_SESSION_LIVE = 1,     /* admitted: frames are accepted */
+    WEMA_CUDA_SESSION_CLOSED = 2,   /* closed, state freed */
+    WEMA_CUDA_SESSION_FAILED = 3    /* admission failed (device allocation) */
+};
+
+typedef struct {
+    int state;                      /* WEMA_CUDA_SESSION_* */
+    long long submitted, completed; /* frames accepted / whose output is written */
+    long long dropped;              /* submissions refused (queued, or 8 pending) */
+    size_t state_bytes;             /* the session's admission cost */
+    double admission_wait_ms;       /* open -> admitted (-1 while queued) */
+} wema_cuda_session_status;
+
+typedef struct {
+    double seconds;                 /* since creation or the last reset */
+    long long ticks, frames, launches;
+    double mpix_frames;             /* sum of W*H/1e6 over completed frames */
+    float latency_p50_ms, latency_p99_ms, latency_max_ms;   /* submit -> output written */
+    float admission_wait_p50_ms, admission_wait_max_ms;
+    long long sessions_admitted;
+    int sessions_live, sessions_queued;
+    size_t bytes_used, budget_bytes;
+    /* dispatcher: host time per tick issue, issue -> completion per tick,
+     * longest session admission (state allocation) and retirement */
+    float tick_host_ms_mean, tick_host_ms_max, tick_span_ms_mean, tick_span_ms_max;
+    float admit_ms_max, retire_ms_max;
+} wema_cuda_serve_stats;
+
+int wema_cuda_server_create(int device, size_t budget_bytes, int max_streams, wema_cuda_server **out);
+/* Waits for every issued tick, frees every session. */
+void wema_cuda_server_destroy(wema_cuda_server *srv);
+/* Fails when the config is invalid or its state alone exceeds the budget;
+ * otherwise *sid names the session (admitted now or queued). */
+int wema_cuda_server_open(wema_cuda_server *srv, const wema_cuda_config *cfg, int *sid);
+/* One frame (H x W x 3 RGB24 on the device); both buffers must stay valid
+ * until the session's completed count passes it.  0: accepted; 1: refused,
+ * the session is still queued; 2: refused, 8 frames already pending. */
+int wema_cuda_server_submit(wema_cuda_server *srv, int sid, const void *d_in_u8, void *d_out_u8);
+/* Pending frames still run; then the state is freed and the queue advances. */
+int wema_cuda_server_close(wema_cuda_server *srv, int sid);
+int wema_cuda_server_poll(wema_cuda_server *srv, int sid, wema_cuda_session_status *st);
+/* hold != 0: issue no new ticks (submitted frames collect; admission goes
+ * on); 0 resumes.  For maintenance windows and for tests of tick mixing. */
+int wema_cuda_server_hold(wema_cuda_server *srv, int hold);
+/* Waits until no frame is pending or in flight and no session is queued. */
+int wema_cuda_server_drain(wema_cuda_server *srv, int timeout_ms);
+/* reset != 0 starts a new measurement window after filling *out. */
+int wema_cuda_server_stats(wema_cuda_server *srv, int reset, wema_cuda_serve_stats *out);
+
 /* Message of the last failure on this thread ("" if none). */
 const char *wema_cuda_last_error(void);
 

@@ -1,404 +1,9 @@
-// batch.cu - many video streams advanced one frame per tick, with one launch
-// per kernel type and tick over every stream's (uneven) pyramid.
-//
-// Each stream keeps its own state (a Session holding one buffer set: pyramid,
-// deltas, IIR state, threshold scratch and binade history) resident on the
-// device.  A tick takes one frame of each listed stream and issues, on one
-// CUDA stream, the same kernels as the per-stream path - forward DWT level 0
-// (luma and colour streams apart), levels 1..3, threshold monoids and walk,
-// the IIR filter (on a second CUDA stream, beside the threshold), inverse
-// levels 3..1, inverse level 0 and the luma transfer - but each launch covers
-// all streams: its grid is the concatenation of the streams' grids and a task
-// map in device memory sends every block to its stream's parameters
-// (multi.cuh).  The per-stream parameters and the maps of one tick are built on
-// the host into one pinned table and copied with a single H2D copy; three
-// tables rotate so the host can build tick t+1 while tick t runs.  The
-// arithmetic is the per-stream path's, so a stream's frames are bit-identical
-// alone and in any mix.
-//
-// Consecutive ticks overlap: the luma transfer of tick t runs on its own
-// lower-priority CUDA stream while tick t+1's forward DWT, threshold and IIR
-// run (their blocks are placed first, the transfer's fill what is left of
-// each SM); tick t+1's inverse DWT, which rewrites the reconstructed luma the
-// transfer reads, waits for it.  The tick's done event follows its transfer.
-//
-// Supported per stream: IIR band-pass, luma (guided filter or Gaussian
-// transfer) or colour, RGB24 frames in device memory.
-#include <string.h>
-
-#include <algorithm>
+// batch.cu - C ABI of the batched streams (wema_cuda_batch_*); the Batch
+// class itself is in batch.h.
 #include <mutex>
 #include <new>
-#include <vector>
 
-#include "session.h"
-#include "wema_cuda.h"
-
-namespace wema {
-
-namespace {
-
-// one batched launch being assembled: per-task parameter structs + grids
-struct Launch {
-    size_t elem = 0;
-    std::vector<char> params;
-    std::vector<int> gx, gy, nblk;
-    unsigned total = 0;
-    size_t params_off = 0, map_off = 0;   // device offsets in the tick's table
-    void reset(size_t e) {
-        elem = e;
-        params.clear();
-        gx.clear();
-        gy.clear();
-        nblk.clear();
-        total = 0;
-    }
-    void add(const void* p, unsigned x, unsigned y, unsigned blocks) {
-        if (blocks == 0) return;
-        params.insert(params.end(), (const char*)p, (const char*)p + elem);
-        gx.push_back((int)x);
-        gy.push_back((int)y);
-        nblk.push_back((int)blocks);
-        total += blocks;
-    }
-    int n() const { return (int)gx.size(); }
-};
-
-enum {
-    L_FWD0_LUMA, L_FWD0_COLOR, L_FWD1, L_FWD2, L_FWD3,
-    L_THR_PART, L_THR_PREFIX, L_THR_MON, L_THR_WALK,
-    L_IIR_PRESEED, L_IIR,
-    L_INV3, L_INV2, L_INV1, L_INV0_LUMA, L_INV0_COLOR,
-    L_XFER_GUIDED, L_XFER_GAUSS,
-    L_COUNT
-};
-
-}  // namespace
-
-class Batch {
-public:
-    int device = 0;
-    int max_streams = 0;
-    std::vector<Session*> streams;        // by id; null when removed
-    cudaStream_t st_main = nullptr, st_iir = nullptr, st_xfer = nullptr;
-    cudaEvent_t ev_fwd = nullptr, ev_iir = nullptr, ev_inv = nullptr, ev_xfer = nullptr;
-    bool xfer_pending = false;            // ev_xfer marks a transfer tick t+1 must wait for
-    static constexpr int NBUF = 3;
-    struct Table {
-        char* host = nullptr;
-        char* dev = nullptr;
-        size_t cap = 0;
-        cudaEvent_t done = nullptr;
-        bool used = false;
-    } tb[NBUF];
-    int cur = 0;
-    long long launches = 0;
-    long long ticks = 0;
-    Launch L[L_COUNT];
-    std::vector<char> image;
-
-    ~Batch() {
-        for (cudaStream_t st : {st_main, st_iir, st_xfer})
-            if (st) cudaStreamSynchronize(st);
-        for (Session* s : streams) delete s;
-        for (Table& t : tb) {
-            if (t.host) cudaFreeHost(t.host);
-            if (t.dev) cudaFree(t.dev);
-            if (t.done) cudaEventDestroy(t.done);
-        }
-        for (cudaStream_t st : {st_main, st_iir, st_xfer})
-            if (st) cudaStreamDestroy(st);
-        for (cudaEvent_t e : {ev_fwd, ev_iir, ev_inv, ev_xfer})
-            if (e) cudaEventDestroy(e);
-    }
-
-    bool init(int dev, int max_n) {
-        device = dev;
-        max_streams = max_n;
-        if (!ensure_device(dev)) return false;
-        int lo = 0, hi = 0;
-        if (!cuda_ok(cudaDeviceGetStreamPriorityRange(&lo, &hi), "stream priorities")) return false;
-        for (cudaStream_t* st : {&st_main, &st_iir})
-            if (!cuda_ok(cudaStreamCreateWithPriority(st, cudaStreamNonBlocking, hi), "cudaStreamCreate"))
-                return false;
-        if (!cuda_ok(cudaStreamCreateWithPriority(&st_xfer, cudaStreamNonBlocking, lo), "cudaStreamCreate"))
-            return false;
-        for (cudaEvent_t* e : {&ev_fwd, &ev_iir, &ev_inv, &ev_xfer})
-            if (!cuda_ok(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate"))
-                return false;
-        for (Table& t : tb)
-            if (!cuda_ok(cudaEventCreateWithFlags(&t.done, cudaEventDisableTiming), "cudaEventCreate"))
-                return false;
-        return true;
-    }
-
-    int live() const {
-        int n = 0;
-        for (Session* s : streams) n += s != nullptr;
-        return n;
-    }
-
-    int add(const wema_cuda_config& c) {
-        if (!c.use_iir) { set_error("batched streams use the IIR filter (use_iir = 1)"); return -1; }
-        if (c.device != device) { set_error("stream device %d differs from the batch's %d", c.device, device); return -1; }
-        if (live() >= max_streams) { set_error("batch holds %d streams already", max_streams); return -1; }
-        Session* s = new (std::nothrow) Session();
-        if (!s) { set_error("out of host memory"); return -1; }
-        if (!s->init(c, 1)) {
-            delete s;
-            return -1;
-        }
-        for (size_t i = 0; i < streams.size(); i++)
-            if (!streams[i]) { streams[i] = s; return (int)i; }
-        streams.push_back(s);
-        return (int)streams.size() - 1;
-    }
-
-    bool remove(int id) {
-        if (id < 0 || id >= (int)streams.size() || !streams[id]) { set_error("no stream %d", id); return false; }
-        if (!sync()) return false;
-        delete streams[id];
-        streams[id] = nullptr;
-        return true;
-    }
-
-    bool sync() {
-        if (!cuda_ok(cudaStreamSynchronize(st_iir), "sync")) return false;
-        if (!cuda_ok(cudaStreamSynchronize(st_main), "sync")) return false;
-        return cuda_ok(cudaStreamSynchronize(st_xfer), "sync");
-    }
-
-    // the table image: every launch's parameter array, then its task map
-    size_t put(const void* p, size_t n) {
-        size_t off = (image.size() + 15) & ~(size_t)15;
-        image.resize(off + n);
-        if (n) memcpy(image.data() + off, p, n);
-        return off;
-    }
-    void emit(Launch& l) {
-        if (l.n() == 0) return;
-        l.params_off = put(l.params.data(), l.params.size());
-        const int n = l.n();
-        std::vector<int> map(3 * n + 2);
-        map[0] = n;
-        int start = 0;
-        for (int i = 0; i < n; i++) {
-            map[1 + i] = start;
-            start += l.nblk[i];
-        }
-        map[1 + n] = start;
-        for (int i = 0; i < n; i++) {
-            map[n + 2 + i] = l.gx[i];
-            map[2 * n + 2 + i] = l.gy[i];
-        }
-        l.map_off = put(map.data(), map.size() * sizeof(int));
-    }
-
-    bool tick(const int* ids, const uint8_t* const* in, uint8_t* const* out, int n, cudaEvent_t wait,
-              cudaEvent_t done) {
-        for (int k = 0; k < n; k++) {
-            if (ids[k] < 0 || ids[k] >= (int)streams.size() || !streams[ids[k]]) {
-                set_error("no stream %d", ids[k]);
-                return false;
-            }
-            if (!in[k] || !out[k]) { set_error("stream %d: null frame", ids[k]); return false; }
-            for (int q = 0; q < k; q++)
-                if (ids[q] == ids[k]) { set_error("stream %d listed twice in one tick", ids[k]); return false; }
-        }
-        L[L_FWD0_LUMA].reset(sizeof(FwdLevelParams));
-        L[L_FWD0_COLOR].reset(sizeof(FwdLevelParams));
-        for (int l = 1; l <= 3; l++) L[L_FWD0_COLOR + l].reset(sizeof(FwdLevelParams));
-        for (int k = L_THR_PART; k <= L_THR_WALK; k++) L[k].reset(thr_args_bytes());
-        L[L_IIR_PRESEED].reset(iir_args_bytes());
-        L[L_IIR].reset(iir_args_bytes());
-        for (int k = L_INV3; k <= L_INV0_COLOR; k++) L[k].reset(sizeof(InvLevelParams));
-        L[L_XFER_GUIDED].reset(sizeof(TransferParams));
-        L[L_XFER_GAUSS].reset(sizeof(TransferParams));
-        std::vector<char> targs(thr_args_bytes()), iargs(iir_args_bytes());
-
-        for (int k = 0; k < n; k++) {
-            Session& S = *streams[ids[k]];
-            const Geom& g = S.g;
-            const int LV = g.levels, nch = S.nch;
-            Slot& q = S.slot[0];
-            // ---- forward DWT
-            for (int l = 0; l < LV; l++) {
-                FwdLevelParams p{};
-                p.iw = g.in_w[l];
-                p.ih = g.in_h[l];
-                p.sw = g.sw[l];
-                p.sh = g.sh[l];
-                p.n = g.n[l];
-                p.vec_end = vec_cover(g.pixels);
-                if (l == 0) p.src_u8 = in[k];
-                else
-                    for (int c = 0; c < nch; c++) p.src_planes[c] = q.ll[c][l - 1];
-                for (int c = 0; c < nch; c++) {
-                    p.coef[c] = q.coef[c] + g.uoff[l];
-                    p.prev[c] = l > 0 ? q.coef[c] + g.uoff[l - 1] : nullptr;
-                    p.ll_out[c] = q.ll[c][l];
-                }
-                p.prev_n = l > 0 ? g.n[l - 1] : 0;
-                unsigned gx, gy;
-                if (l == 0) {
-                    const unsigned b = dwt_fwd_grid(p, 1, gx, gy);
-                    L[nch == 3 ? L_FWD0_COLOR : L_FWD0_LUMA].add(&p, gx, gy, b);
-                } else {
-                    const unsigned b = dwt_fwd_grid(p, nch, gx, gy);
-                    L[L_FWD0_COLOR + l].add(&p, gx, gy, b);
-                }
-            }
-            // ---- threshold
-            PyrView views[3];
-            for (int c = 0; c < nch; c++) views[c] = S.view(0, c);
-            unsigned grids[4][2];
-            if (!cuda_ok(thr_args_fill(targs.data(), views, nch, S.thr_s, q.thr, q.thr + 4,
-                                       S.cfg.threshold_form, S.thr_hist ? 1 : 0, grids),
-                         "threshold setup"))
-                return false;
-            for (int st = 0; st < 4; st++) {
-                if (st < 2 && S.thr_hist) continue;   // partial sums + prefix: first frame only
-                L[L_THR_PART + st].add(targs.data(), grids[st][0], grids[st][1],
-                                       grids[st][0] * grids[st][1]);
-            }
-            // ---- IIR (first frame: preseed), fade-in alpha
-            const bool first = S.frames_processed == 0;
-            for (int c = 0; c < nch; c++) {
-                const unsigned b = iir_args_fill(iargs.data(), S.ip, q.coef[c], S.state[c], q.delta[c],
-                                                 S.warmup);
-                if (first) L[L_IIR_PRESEED].add(iargs.data(), b, 1, b);
-                L[L_IIR].add(iargs.data(), b, 1, b);
-            }
-            // ---- inverse DWT (+ colour output) and the luma transfer
-            const float amp = fade_amp(S.cfg.amp_factor, first ? S.warmup : S.frames_processed, S.warmup);
-            q.alpha[0] = amp;
-            q.alpha[1] = q.alpha[2] = amp * 0.5f;
-            for (int l = LV - 1; l >= 0; l--) {
-                InvLevelParams iq{};
-                iq.ow = g.in_w[l];
-                iq.oh = g.in_h[l];
-                iq.sw = g.sw[l];
-                iq.sh = g.sh[l];
-                iq.n = g.n[l];
-                iq.thr = q.thr;
-                for (int c = 0; c < nch; c++) {
-                    iq.ll[c] = (l == LV - 1) ? q.ll[c][LV - 1] : q.rec[c][l + 1];
-                    iq.coef[c] = q.coef[c] + g.uoff[l];
-                    iq.delta[c] = q.delta[c] + g.uoff[l];
-                    iq.alpha[c] = l == 0 ? q.alpha[c] * 0.5f : q.alpha[c];
-                    iq.out_planes[c] = (l > 0 || nch == 1) ? q.rec[c][l] : nullptr;
-                }
-                unsigned gx, gy;
-                if (l == 0 && nch == 3) {
-                    iq.out_u8 = out[k];
-                    const unsigned b = dwt_inv_grid(iq, 1, gx, gy);
-                    L[L_INV0_COLOR].add(&iq, gx, gy, b);
-                } else {
-                    const unsigned b = dwt_inv_grid(iq, nch, gx, gy);
-                    L[l == 0 ? L_INV0_LUMA : L_INV1 - (l - 1)].add(&iq, gx, gy, b);
-                }
-            }
-            if (nch == 1) {
-                TransferParams tp{};
-                tp.w = g.w;
-                tp.h = g.h;
-                tp.vec_end = vec_cover(g.pixels);
-                tp.src_u8 = in[k];
-                tp.gray_out = q.rec[0][0];
-                tp.out_u8 = out[k];
-                tp.edge_aware = S.cfg.edge_aware;
-                unsigned gx, gy;
-                const unsigned b = transfer_grid(tp, gx, gy);
-                L[tp.edge_aware ? L_XFER_GUIDED : L_XFER_GAUSS].add(&tp, gx, gy, b);
-            }
-        }
-        // ---- the table image, its buffer, one H2D copy
-        image.clear();
-        for (Launch& l : L) emit(l);
-        Table& t = tb[cur];
-        if (t.used && !cuda_ok(cudaEventSynchronize(t.done), "table reuse")) return false;
-        if (image.size() > t.cap) {
-            if (t.host) cudaFreeHost(t.host);
-            if (t.dev) cudaFree(t.dev);
-            t.host = nullptr;
-            t.dev = nullptr;
-            t.cap = 0;
-            const size_t cap = std::max<size_t>(image.size() * 2, 1 << 16);
-            if (!cuda_ok(cudaMallocHost(&t.host, cap), "cudaMallocHost(table)")) return false;
-            if (!cuda_ok(cudaMalloc(&t.dev, cap), "cudaMalloc(table)")) return false;
-            t.cap = cap;
-        }
-        memcpy(t.host, image.data(), image.size());
-        if (wait && !cuda_ok(cudaStreamWaitEvent(st_main, wait, 0), "stream wait")) return false;
-        if (!cuda_ok(cudaMemcpyAsync(t.dev, t.host, image.size(), cudaMemcpyHostToDevice, st_main), "table copy"))
-            return false;
-        auto P = [&](int k) { return (const void*)(t.dev + L[k].params_off); };
-        auto M = [&](int k) { return (const int*)(t.dev + L[k].map_off); };
-        auto ok = [&](cudaError_t e, const char* what) {
-            launches += 1;
-            return cuda_ok(e, what);
-        };
-        auto go = [&](int k, auto fn, const char* what) {
-            if (L[k].n() == 0) return true;
-            return ok(fn(), what);
-        };
-
-        // forward, then the filter beside the threshold
-        if (!go(L_FWD0_LUMA, [&] { return launch_dwt_fwd_multi(kSrcRgbU8, 1, (const FwdLevelParams*)P(L_FWD0_LUMA), M(L_FWD0_LUMA), L[L_FWD0_LUMA].total, st_main); }, "forward DWT"))
-            return false;
-        if (!go(L_FWD0_COLOR, [&] { return launch_dwt_fwd_multi(kSrcRgbU8, 3, (const FwdLevelParams*)P(L_FWD0_COLOR), M(L_FWD0_COLOR), L[L_FWD0_COLOR].total, st_main); }, "forward DWT"))
-            return false;
-        for (int k = L_FWD1; k <= L_FWD3; k++)
-            if (!go(k, [&] { return launch_dwt_fwd_multi(kSrcPlanes, 1, (const FwdLevelParams*)P(k), M(k), L[k].total, st_main); }, "forward DWT"))
-                return false;
-        if (!cuda_ok(cudaEventRecord(ev_fwd, st_main), "event record")) return false;
-        if (!cuda_ok(cudaStreamWaitEvent(st_iir, ev_fwd, 0), "stream wait")) return false;
-        if (!go(L_IIR_PRESEED, [&] { return launch_iir_multi(P(L_IIR_PRESEED), M(L_IIR_PRESEED), L[L_IIR_PRESEED].total, 1, st_iir); }, "IIR preseed"))
-            return false;
-        if (!go(L_IIR, [&] { return launch_iir_multi(P(L_IIR), M(L_IIR), L[L_IIR].total, 0, st_iir); }, "IIR"))
-            return false;
-        if (!cuda_ok(cudaEventRecord(ev_iir, st_iir), "event record")) return false;
-        for (int k = L_THR_PART; k <= L_THR_WALK; k++)
-            if (!go(k, [&] { return launch_threshold_multi(k - L_THR_PART, P(k), M(k), L[k].total, st_main); }, "threshold"))
-                return false;
-        if (!cuda_ok(cudaStreamWaitEvent(st_main, ev_iir, 0), "stream wait")) return false;
-        // the previous tick's transfer still reads its reconstructed luma
-        if (xfer_pending && !cuda_ok(cudaStreamWaitEvent(st_main, ev_xfer, 0), "stream wait")) return false;
-        for (int k = L_INV3; k <= L_INV0_LUMA; k++)
-            if (!go(k, [&] { return launch_dwt_inv_multi(1, kOutPlanes, (const InvLevelParams*)P(k), M(k), L[k].total, st_main); }, "inverse DWT"))
-                return false;
-        if (!go(L_INV0_COLOR, [&] { return launch_dwt_inv_multi(3, kOutRgb, (const InvLevelParams*)P(L_INV0_COLOR), M(L_INV0_COLOR), L[L_INV0_COLOR].total, st_main); }, "inverse DWT"))
-            return false;
-        // the transfer on its own stream, so the next tick's forward half overlaps it
-        if (!cuda_ok(cudaEventRecord(ev_inv, st_main), "event record")) return false;
-        if (!cuda_ok(cudaStreamWaitEvent(st_xfer, ev_inv, 0), "stream wait")) return false;
-        if (!go(L_XFER_GUIDED, [&] { return launch_transfer_multi(1, (const TransferParams*)P(L_XFER_GUIDED), M(L_XFER_GUIDED), L[L_XFER_GUIDED].total, st_xfer); }, "luma transfer"))
-            return false;
-        if (!go(L_XFER_GAUSS, [&] { return launch_transfer_multi(0, (const TransferParams*)P(L_XFER_GAUSS), M(L_XFER_GAUSS), L[L_XFER_GAUSS].total, st_xfer); }, "luma transfer"))
-            return false;
-        if (!cuda_ok(cudaEventRecord(ev_xfer, st_xfer), "event record")) return false;
-        xfer_pending = true;
-        if (!cuda_ok(cudaEventRecord(t.done, st_xfer), "event record")) return false;
-        if (done && !cuda_ok(cudaEventRecord(done, st_xfer), "event record")) return false;
-        t.used = true;
-        cur = (cur + 1) % NBUF;
-        ticks++;
-
-        // per-stream frame bookkeeping, as the per-stream path does it
-        for (int k = 0; k < n; k++) {
-            Session& S = *streams[ids[k]];
-            if (S.frames_processed == 0) S.frames_processed = S.warmup;
-            S.frames_processed++;
-            S.thr_hist = true;
-            S.slot[0].valid = true;
-            S.last_slot = 0;
-            S.frames_run++;
-        }
-        return true;
-    }
-};
-
-}  // namespace wema
+#include "batch.h"
 
 // ===================================================================== C ABI
 using namespace wema;

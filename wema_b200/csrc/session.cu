@@ -175,7 +175,8 @@ Session::~Session() {
         if (e) cudaEventDestroy(e);
     for (auto& e : ev)
         if (e) cudaEventDestroy(e);
-    if (arena) cudaFree(arena);
+    if (arena && arena_stream) cudaFreeAsync(arena, arena_stream);
+    else if (arena) cudaFree(arena);
     if (stage_u8) cudaFree(stage_u8);
     if (stage_f32) cudaFree(stage_f32);
 }
@@ -193,7 +194,7 @@ bool Session::collect_timing() {
     return true;
 }
 
-bool Session::init(const wema_cuda_config& c, int ns) {
+bool Session::init(const wema_cuda_config& c, int ns, cudaStream_t alloc_stream) {
     if (!valid_config(c)) return false;
     nslots = ns < 1 ? 1 : (ns > kSlots ? kSlots : ns);
     cfg = c;
@@ -215,6 +216,16 @@ bool Session::init(const wema_cuda_config& c, int ns) {
     Arena A;
     layout(A, *this);
     arena_bytes = A.off;
+    if (alloc_stream) {
+        if (!cuda_ok(cudaMallocAsync(&arena, arena_bytes, alloc_stream), "cudaMallocAsync(session)"))
+            return false;
+        arena_stream = alloc_stream;
+        if (!cuda_ok(cudaMemsetAsync(arena, 0, arena_bytes, alloc_stream), "cudaMemsetAsync")) return false;
+        A = Arena();
+        A.base = (char*)arena;
+        layout(A, *this);
+        return true;
+    }
     if (!cuda_ok(cudaMalloc(&arena, arena_bytes), "cudaMalloc(session)")) return false;
     if (!cuda_ok(cudaMemset(arena, 0, arena_bytes), "cudaMemset")) return false;
     A = Arena();

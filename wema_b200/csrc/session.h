@@ -60,6 +60,7 @@ public:
 
     void* arena = nullptr;
     size_t arena_bytes = 0;
+    cudaStream_t arena_stream = nullptr;   // set: arena from the stream-ordered pool (batched)
     Slot slot[kSlots];
     float4* state[3] = {};             // IIR state (shared by the slots, updated in frame order)
     float* ring[3] = {};               // window ring
@@ -84,7 +85,10 @@ public:
     ~Session();
     int nslots = kSlots;               // buffer sets in use (a batched stream keeps one)
     static size_t bytes_for(const wema_cuda_config& c, int nslots = kSlots);
-    bool init(const wema_cuda_config& c, int nslots = kSlots);
+    // alloc_stream set (a batched stream): the state comes from the device's
+    // stream-ordered pool, zeroed in order on that stream, and the session
+    // creates no streams or events of its own; no call synchronises the device
+    bool init(const wema_cuda_config& c, int nslots = kSlots, cudaStream_t alloc_stream = nullptr);
     // One frame, asynchronous: waits for `wait` (may be null) before touching
     // in/out, records `done` (may be null) once out is written and in is no
     // longer read.  Exactly one of in_u8 / in_f32 is set; outputs optional.

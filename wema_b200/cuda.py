@@ -29,6 +29,30 @@ class Config(C.Structure):
 _lib = None
 
 
+class SessionStatus(C.Structure):
+    """wema_cuda_session_status"""
+    _fields_ = [("state", C.c_int), ("submitted", C.c_longlong), ("completed", C.c_longlong),
+                ("dropped", C.c_longlong), ("state_bytes", C.c_size_t),
+                ("admission_wait_ms", C.c_double)]
+
+
+class ServeStats(C.Structure):
+    """wema_cuda_serve_stats"""
+    _fields_ = [("seconds", C.c_double), ("ticks", C.c_longlong), ("frames", C.c_longlong),
+                ("launches", C.c_longlong), ("mpix_frames", C.c_double),
+                ("latency_p50_ms", C.c_float), ("latency_p99_ms", C.c_float),
+                ("latency_max_ms", C.c_float), ("admission_wait_p50_ms", C.c_float),
+                ("admission_wait_max_ms", C.c_float), ("sessions_admitted", C.c_longlong),
+                ("sessions_live", C.c_int), ("sessions_queued", C.c_int),
+                ("bytes_used", C.c_size_t), ("budget_bytes", C.c_size_t),
+                ("tick_host_ms_mean", C.c_float), ("tick_host_ms_max", C.c_float),
+                ("tick_span_ms_mean", C.c_float), ("tick_span_ms_max", C.c_float),
+                ("admit_ms_max", C.c_float), ("retire_ms_max", C.c_float)]
+
+
+SESSION_QUEUED, SESSION_LIVE, SESSION_CLOSED, SESSION_FAILED = 0, 1, 2, 3
+
+
 def lib() -> C.CDLL:
     global _lib
     if _lib is None:
@@ -70,6 +94,16 @@ def lib() -> C.CDLL:
                                             C.POINTER(i)]
         L.wema_cuda_batch_read.argtypes = [vp, i, i, i, vp, sz]
         L.wema_cuda_batch_read.restype = C.c_long
+        L.wema_cuda_server_create.argtypes = [i, sz, i, C.POINTER(vp)]
+        L.wema_cuda_server_destroy.argtypes = [vp]
+        L.wema_cuda_server_destroy.restype = None
+        L.wema_cuda_server_open.argtypes = [vp, C.POINTER(Config), C.POINTER(i)]
+        L.wema_cuda_server_submit.argtypes = [vp, i, vp, vp]
+        L.wema_cuda_server_close.argtypes = [vp, i]
+        L.wema_cuda_server_poll.argtypes = [vp, i, C.POINTER(SessionStatus)]
+        L.wema_cuda_server_drain.argtypes = [vp, i]
+        L.wema_cuda_server_hold.argtypes = [vp, i]
+        L.wema_cuda_server_stats.argtypes = [vp, i, C.POINTER(ServeStats)]
         _lib = L
     return _lib
 
@@ -274,6 +308,61 @@ class Batch:
         if getattr(self, "h", None):
             lib().wema_cuda_batch_destroy(self.h)
             self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """The served request loop (wema_cuda_server_*): sessions admitted against
+    a device-memory budget, frames batched continuously by a native
+    dispatcher thread."""
+
+    def __init__(self, device=0, budget_bytes=150 * 10**9, max_streams=256):
+        self.h = C.c_void_p()
+        self.device = device
+        _check(lib().wema_cuda_server_create(int(device), int(budget_bytes), int(max_streams),
+                                             C.byref(self.h)), "server_create")
+
+    def open(self, width, height, **kw) -> int:
+        c = make_config(width, height, device=self.device, **kw)
+        sid = C.c_int()
+        _check(lib().wema_cuda_server_open(self.h, C.byref(c), C.byref(sid)), "server_open")
+        return sid.value
+
+    def submit(self, sid, d_in, d_out) -> int:
+        """0 accepted, 1 refused (session queued), 2 refused (8 pending)."""
+        rc = lib().wema_cuda_server_submit(self.h, int(sid), _ptr(d_in), _ptr(d_out))
+        if rc < 0:
+            raise RuntimeError(f"server_submit failed: {last_error()}")
+        return rc
+
+    def close_session(self, sid):
+        _check(lib().wema_cuda_server_close(self.h, int(sid)), "server_close")
+
+    def poll(self, sid) -> dict:
+        st = SessionStatus()
+        _check(lib().wema_cuda_server_poll(self.h, int(sid), C.byref(st)), "server_poll")
+        return {k: getattr(st, k) for k, _ in SessionStatus._fields_}
+
+    def hold(self, on=True):
+        _check(lib().wema_cuda_server_hold(self.h, int(bool(on))), "server_hold")
+
+    def drain(self, timeout_ms=60000):
+        _check(lib().wema_cuda_server_drain(self.h, int(timeout_ms)), "server_drain")
+
+    def stats(self, reset=False) -> dict:
+        st = ServeStats()
+        _check(lib().wema_cuda_server_stats(self.h, int(bool(reset)), C.byref(st)), "server_stats")
+        return {k: getattr(st, k) for k, _ in ServeStats._fields_}
+
+    def close(self):
+        if self.h:
+            lib().wema_cuda_server_destroy(self.h)
+            self.h = C.c_void_p()
 
     def __del__(self):
         try:

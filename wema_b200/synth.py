@@ -137,3 +137,44 @@ def mixed_streams(seed: int = 7):
             out.append((spec, cfg))
             k += 1
     return out
+
+
+SERVED_RES = [((640, 480), 0.40), ((1280, 720), 0.30), ((1920, 1080), 0.25), ((3840, 2160), 0.05)]
+
+
+def served_sessions(seed: int = 11, horizon_s: float = 30.0, rate_per_s: float = 2.0,
+                    len_s=(5.0, 60.0)):
+    """The served workload's session list: a Poisson process of stream
+    sessions (mean `rate_per_s` arrivals per second) with lengths log-uniform
+    in `len_s`, resolution drawn from 480p 40% / 720p 30% / 1080p 25% /
+    2160p 5%, 30 or 60 fps, contents and settings as the mixed workload.
+    Arrivals start at -len_s[1] so the sessions alive at t = 0 are a draw
+    from the steady state; each is returned with its open time clipped to 0.
+    Returns [(t_open, t_close, SynthSpec, settings)] for sessions alive in
+    [0, horizon_s), ordered by open time."""
+    rng = np.random.default_rng(seed)
+    t = -float(len_s[1])
+    out = []
+    k = 0
+    lo, hi = np.log(len_s[0]), np.log(len_s[1])
+    while True:
+        t += float(rng.exponential(1.0 / rate_per_s))
+        if t >= horizon_s:
+            break
+        length = float(np.exp(rng.uniform(lo, hi)))
+        ri = int(rng.choice(len(SERVED_RES), p=[p for _, p in SERVED_RES]))
+        (w, h) = SERVED_RES[ri][0]
+        fps = float(rng.choice([30.0, 60.0]))
+        nd = int(rng.integers(1, 4))
+        spec = SynthSpec(w, h, fps, seed=5000 + k,
+                         disc_freq=[float(x) for x in rng.uniform(0.5, 4.0, nd)],
+                         disc_amp=[float(x) for x in rng.uniform(0.2, 0.5, nd)],
+                         disc_radius=30.0 * min(w, h) / 480.0, noise_sigma=2.0)
+        cfg = dict(fps=fps, amp=float(rng.uniform(20.0, 150.0)), f_low=0.5, f_high=5.0,
+                   window=int(rng.integers(16, 65)), color=False, edge_aware=True)
+        k += 1
+        if t + length <= 0.0:
+            continue
+        out.append((max(t, 0.0), min(t + length, horizon_s), spec, cfg))
+    out.sort(key=lambda x: x[0])
+    return out
