@@ -43,6 +43,9 @@ typedef struct {
     int   use_iir;           /* 1: IIR band-pass (default), 0: window ("--haar") mode */
     int   threshold_form;    /* WEMA_CUDA_THR_SINGLE or WEMA_CUDA_THR_BATCH */
     int   device;            /* CUDA device ordinal */
+    int   iir_state_fp64;    /* precision variant: biquad state and its update in FP64
+                                (the FP32-designed coefficients promoted; 32 B of state
+                                per position instead of 16).  0: the reference's FP32 */
 } wema_cuda_config;
 
 /* Fills *cfg with the reference CLI's defaults for a stream of the given

@@ -297,7 +297,7 @@ public:
             // ---- IIR (first frame: preseed), fade-in alpha
             const bool first = S.frames_processed == 0;
             for (int c = 0; c < nch; c++) {
-                const unsigned b = iir_args_fill(iargs.data(), S.ip, q.coef[c], S.state[c], q.delta[c],
+                const unsigned b = iir_args_fill(iargs.data(), S.ip, q.coef[c], S.state[c], S.cfg.iir_state_fp64, q.delta[c],
                                                  S.warmup);
                 if (first) L[L_IIR_PRESEED].add(iargs.data(), b, 1, b);
                 L[L_IIR].add(iargs.data(), b, 1, b);

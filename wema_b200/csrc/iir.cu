@@ -13,6 +13,12 @@
 //   out = |x| > thr ? fma(delta, alpha_l, x) : x,  alpha_0 = alpha/2;
 // the per-frame path applies it inside the inverse DWT's staging (dwt.cu), so
 // the filter need not wait for the threshold.
+//
+// Precision variant (fp64): the state and the whole cascade step in double,
+// from the FP32-designed coefficients promoted; the band-passed delta is
+// rounded to FP32 once.  Poles near the unit circle (a low f_low at a high
+// frame rate) accumulate FP32 rounding in the recursive state; this keeps it
+// out.  State: {w1_hp, w2_hp} and {w1_lp, w2_lp} as two double2.
 #include "common.cuh"
 #include "kernels.h"
 #include "multi.cuh"
@@ -29,7 +35,8 @@ struct IirDev {
     const float* coef;
     long long frame_stride;
     int frames;
-    float4* state;
+    void* state;           // float4 per position, or (fp64) double2[2] per position
+    int fp64;
     float* amplified;
     float* delta_out;
     const float* thr;
@@ -55,6 +62,19 @@ __device__ __forceinline__ float cascade(const float* c, float4& st, float x, bo
     return y;
 }
 
+// the fp64 variant of cascade(): one rounding, at the end
+__device__ __forceinline__ float cascade64(const float* c, double2& hp, double2& lp, float xf) {
+    const double x = (double)xf;
+    double y = fma((double)c[0], x, hp.x);
+    hp.x = fma(-(double)c[3], y, fma((double)c[1], x, hp.y));
+    hp.y = fma(-(double)c[4], y, (double)c[2] * x);
+    const double x2 = y;
+    y = fma((double)c[5], x2, lp.x);
+    lp.x = fma(-(double)c[8], y, fma((double)c[6], x2, lp.y));
+    lp.y = fma(-(double)c[9], y, (double)c[7] * x2);
+    return __double2float_rn(y);
+}
+
 // level of unique position u, and whether its 6-slot index is in the
 // reference's scalar tail
 __device__ __forceinline__ int level_of(const IirParams& p, long long u, bool& tail) {
@@ -71,22 +91,65 @@ __device__ __forceinline__ void iir_preseed_body(const IirDev& a, int block, int
     const long long pu = a.p.uoff[a.p.levels];
     for (long long u = block * (long long)IIR_THREADS + threadIdx.x; u < pu;
          u += (long long)nblocks * IIR_THREADS) {
-        bool tail;
-        level_of(a.p, u, tail);
         const float x = a.coef[u];
-        float4 st = a.state[u];
-        for (int it = 0; it < a.warmup; it++) cascade(a.p.c, st, x, tail);
-        a.state[u] = st;
+        if (a.fp64) {
+            double2* s = static_cast<double2*>(a.state) + 2 * u;
+            double2 hp = s[0], lp = s[1];
+            for (int it = 0; it < a.warmup; it++) cascade64(a.p.c, hp, lp, x);
+            s[0] = hp;
+            s[1] = lp;
+        } else {
+            bool tail;
+            level_of(a.p, u, tail);
+            float4* s = static_cast<float4*>(a.state) + u;
+            float4 st = *s;
+            for (int it = 0; it < a.warmup; it++) cascade(a.p.c, st, x, tail);
+            *s = st;
+        }
     }
 }
 
 // A thread takes positions u, u + B, u + 2B, u + 3B (B = the task's threads)
 // per pass, so a warp's accesses stay coalesced and four are in flight.
-__device__ __forceinline__ void iir_body(const IirDev& a, int block, int nblocks) {
+__device__ __forceinline__ void iir_body64(const IirDev& a, int block, int nblocks) {
     const long long pu = a.p.uoff[a.p.levels];
     const long long B = (long long)nblocks * IIR_THREADS;
     const float* __restrict__ coef = a.coef;
-    float4* __restrict__ state = a.state;
+    double2* __restrict__ state = static_cast<double2*>(a.state);
+    float* __restrict__ dout = a.delta_out;
+    for (long long u0 = block * (long long)IIR_THREADS + threadIdx.x; u0 < pu; u0 += IIR_U * B) {
+        float x[IIR_U];
+        double2 hp[IIR_U], lp[IIR_U];
+#pragma unroll
+        for (int j = 0; j < IIR_U; j++) {
+            const long long u = u0 + j * B;
+            if (u < pu) {
+                x[j] = __ldg(coef + u);
+                hp[j] = state[2 * u];
+                lp[j] = state[2 * u + 1];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < IIR_U; j++) {
+            const long long u = u0 + j * B;
+            if (u < pu) {
+                dout[u] = cascade64(a.p.c, hp[j], lp[j], x[j]);
+                state[2 * u] = hp[j];
+                state[2 * u + 1] = lp[j];
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void iir_body(const IirDev& a, int block, int nblocks) {
+    if (a.fp64) {
+        iir_body64(a, block, nblocks);
+        return;
+    }
+    const long long pu = a.p.uoff[a.p.levels];
+    const long long B = (long long)nblocks * IIR_THREADS;
+    const float* __restrict__ coef = a.coef;
+    float4* __restrict__ state = static_cast<float4*>(a.state);
     float* __restrict__ dout = a.delta_out;
     for (long long u0 = block * (long long)IIR_THREADS + threadIdx.x; u0 < pu; u0 += IIR_U * B) {
         float x[IIR_U];
@@ -143,23 +206,25 @@ static int grid_for(long long n) {
     return (int)(b < 148 * 16 ? (b > 0 ? b : 1) : 148 * 16);
 }
 
-cudaError_t launch_iir_preseed(const IirParams& p, const float* coef, float4* state, int warmup,
+cudaError_t launch_iir_preseed(const IirParams& p, const float* coef, void* state, int fp64, int warmup,
                                cudaStream_t st) {
     IirDev a{};
     a.p = p;
     a.coef = coef;
     a.state = state;
+    a.fp64 = fp64;
     a.warmup = warmup;
     k_iir_preseed<<<grid_for(p.uoff[p.levels]), IIR_THREADS, 0, st>>>(a);
     return cudaGetLastError();
 }
 
-cudaError_t launch_iir(const IirParams& p, const float* coef, float4* state, float* delta,
+cudaError_t launch_iir(const IirParams& p, const float* coef, void* state, int fp64, float* delta,
                        cudaStream_t st) {
     IirDev a{};
     a.p = p;
     a.coef = coef;
     a.state = state;
+    a.fp64 = fp64;
     a.delta_out = delta;
     k_iir<<<grid_for(p.uoff[p.levels]), IIR_THREADS, 0, st>>>(a);
     return cudaGetLastError();
@@ -181,12 +246,13 @@ cudaError_t launch_amplify(const IirParams& p, const float* coef, const float* d
 // ---- batched filter (the host fills one IirDev per stream and channel)
 size_t iir_args_bytes() { return sizeof(IirDev); }
 
-unsigned iir_args_fill(void* dst, const IirParams& p, const float* coef, float4* state, float* delta,
+unsigned iir_args_fill(void* dst, const IirParams& p, const float* coef, void* state, int fp64, float* delta,
                        int warmup) {
     IirDev a{};
     a.p = p;
     a.coef = coef;
     a.state = state;
+    a.fp64 = fp64;
     a.delta_out = delta;
     a.warmup = warmup;
     memcpy(dst, &a, sizeof a);

@@ -83,11 +83,12 @@ struct IirParams {
     long long simd_end;         // 6-slot positions >= simd_end take the scalar-tail form
 };
 // preseed: run `warmup` iterations with the current coefficients as input
-cudaError_t launch_iir_preseed(const IirParams& p, const float* coef, float4* state, int warmup,
+// state: float4 per position, or (fp64) two double2 per position
+cudaError_t launch_iir_preseed(const IirParams& p, const float* coef, void* state, int fp64, int warmup,
                                cudaStream_t st);
 // one frame: delta = cascade(coef); the amplification is applied where the
 // inverse DWT stages the coefficients (launch_dwt_inv) or by launch_amplify
-cudaError_t launch_iir(const IirParams& p, const float* coef, float4* state, float* delta,
+cudaError_t launch_iir(const IirParams& p, const float* coef, void* state, int fp64, float* delta,
                        cudaStream_t st);
 // amplified = |coef| > thr ? fma(delta, alpha_l, coef) : coef over all unique
 // positions (inspection, and the batch route)
@@ -138,7 +139,7 @@ cudaError_t thr_args_fill(void* dst, const PyrView* views, int nch, const ThrScr
 cudaError_t launch_threshold_multi(int stage, const void* d_args, const int* d_map, unsigned blocks,
                                    cudaStream_t st);
 size_t iir_args_bytes();
-unsigned iir_args_fill(void* dst, const IirParams& p, const float* coef, float4* state, float* delta,
+unsigned iir_args_fill(void* dst, const IirParams& p, const float* coef, void* state, int fp64, float* delta,
                        int warmup);   // returns the task's block count
 cudaError_t launch_iir_multi(const void* d_args, const int* d_map, unsigned blocks, int preseed,
                              cudaStream_t st);

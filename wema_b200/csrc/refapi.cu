@@ -441,12 +441,12 @@ static bool iir_frames(IIRTemporalFilter* filt, const float* in, float* out, int
     if (!cuda_ok(cudaMemcpyAsync(d_in, in, bytes, cudaMemcpyHostToDevice, st), "H2D")) return false;
     const IirParams ip = flat_params(im->c, n);
     if (preseed) {
-        if (!cuda_ok(launch_iir_preseed(ip, d_in, im->d_state, filt->warmup_frames, st), "preseed"))
+        if (!cuda_ok(launch_iir_preseed(ip, d_in, im->d_state, 0, filt->warmup_frames, st), "preseed"))
             return false;
         return sync(st);
     }
     for (int f = 0; f < frames; f++)
-        if (!cuda_ok(launch_iir(ip, d_in + f * n, im->d_state, d_out + f * n, st), "IIR")) return false;
+        if (!cuda_ok(launch_iir(ip, d_in + f * n, im->d_state, 0, d_out + f * n, st), "IIR")) return false;
     if (!cuda_ok(cudaMemcpyAsync(out, d_out, bytes, cudaMemcpyDeviceToHost, st), "D2H")) return false;
     return sync(st);
 }

@@ -131,7 +131,7 @@ static void layout(Arena& A, Session& s) {
         q.thr = A.take<float>(8);
     }
     for (int c = 0; c < s.nch; c++) {
-        if (s.cfg.use_iir) s.state[c] = A.take<float4>(pu);
+        if (s.cfg.use_iir) s.state[c] = A.take<float4>(s.cfg.iir_state_fp64 ? 2 * pu : pu);
         else s.ring[c] = A.take<float>((size_t)pu * s.cfg.temporal_window);
         s.ampl[c] = A.take<float>(pu);
         void* t = A.take<char>(thr_scratch_bytes(n6));
@@ -147,6 +147,7 @@ static bool valid_config(const wema_cuda_config& c) {
         set_error("temporal window must be in [4, 256]");
         return false;
     }
+    if (c.iir_state_fp64 != 0 && c.iir_state_fp64 != 1) { set_error("iir_state_fp64 must be 0 or 1"); return false; }
     return true;
 }
 
@@ -343,7 +344,7 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
     if (cfg.use_iir) {
         if (frames_processed == 0) {   // iir_temporal_preseed on the first frame
             for (int c = 0; c < nch; c++)
-                if (!cuda_ok(launch_iir_preseed(ip, q.coef[c], state[c], warmup, s_tmp), "preseed"))
+                if (!cuda_ok(launch_iir_preseed(ip, q.coef[c], state[c], cfg.iir_state_fp64, warmup, s_tmp), "preseed"))
                     return false;
             launches += nch;
             frames_processed = warmup;
@@ -353,7 +354,7 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
         q.alpha[0] = amp;
         q.alpha[1] = q.alpha[2] = amp * 0.5f;
         for (int c = 0; c < nch; c++)
-            if (!cuda_ok(launch_iir(ip, q.coef[c], state[c], q.delta[c], s_tmp), "IIR")) return false;
+            if (!cuda_ok(launch_iir(ip, q.coef[c], state[c], cfg.iir_state_fp64, q.delta[c], s_tmp), "IIR")) return false;
         launches += nch;
     } else {
         for (int c = 0; c < nch; c++)
