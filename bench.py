@@ -53,6 +53,8 @@ WORKLOADS = {
     "mixed_streams_48": ("mixed_streams", None),
     # Poisson stream sessions through the served request loop (wema_cuda_server_*)
     "served_poisson": ("served_sessions", None),
+    # error report of the precision variants against the FP64 re-evaluation
+    "precision_report": ("precision_720p", None),
 }
 METRIC = "Mpix-frames/s"
 
@@ -76,6 +78,7 @@ def parse():
     ap.add_argument("--workload", default="plain_fullhd_color", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-frames", type=int, default=12, help="reference frames timed on the host")
     ap.add_argument("--served-seconds", type=float, default=20.0, help="served_poisson measured window")
+    ap.add_argument("--precision-frames", type=int, default=480, help="precision_report frames")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -512,12 +515,149 @@ def bench_served(a, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+def _unique(flat6, dims):
+    out, k6 = [], 0
+    for (sw, sh) in dims:
+        n = sw * sh
+        out.append(flat6[k6: k6 + 3 * n])
+        k6 += 6 * n
+    return np.concatenate(out)
+
+
+def bench_precision(a, rank, world, local):
+    """Error report of the precision variants on the precision-stress stream
+    (1280x720 @240 fps, one disc 0.4 Hz / 0.15 px, noise 3 LSB, band
+    0.2-0.6 Hz, amp 200).  IIR: FP32 and FP64 biquad state, each frame's
+    band-passed delta against the FP64 cascade fed the same coefficients, and
+    the last frame's output against the FP64 pipeline (same threshold) and
+    against the reference (its C restatement, bit-exact to it).  Window mode,
+    ws 64: FP32 and FP16 ring, the last frame's delta against the FP64 window
+    filter over the same coefficients (every 8th position), the output
+    difference and the temporal stage's device time per frame."""
+    if rank != 0:
+        return
+    import torch
+    from wema_b200 import cuda as wc
+    from wema_b200 import synth as S
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import fp64
+    from oracle import Oracle
+    orc = Oracle()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    F = int(a.precision_frames)
+    spec = S.precision_720p()
+    w, h = spec.width, spec.height
+    host = np.empty((F, h, w, 3), np.uint8)
+    S.SynthVideo(spec).frames(0, F, out=host)
+    d_in = torch.from_numpy(host).to(dev)
+    dims = orc.subband_dims(w, h)
+    band = dict(fps=240.0, amp=200.0, f_low=0.2, f_high=0.6)
+    c32, warm = orc.iir_design(0.2, 0.6, 240.0)
+    t0 = time.perf_counter()
+
+    # ---- IIR: FP32 vs FP64 state
+    sess = {v: wc.Session(width=w, height=h, device=local, state_fp64=v, **band) for v in (False, True)}
+    ref64 = fp64.Stream64(w, h, coef=c32, **band)
+    rel = {False: [], True: []}
+    absmax = {False: 0.0, True: 0.0}
+    outs = {}
+    o = torch.empty((h, w, 3), dtype=torch.uint8, device=dev)
+    coef = None
+    for t in range(F):
+        got = {}
+        for v, s in sess.items():
+            s.process_u8(d_in[t], o)
+            torch.cuda.synchronize(dev)
+            if v is False:
+                coef = _unique(s.read(wc.READ_ORIG6), dims).astype(np.float64)
+            got[v] = _unique(s.read(wc.READ_DELTA6), dims).astype(np.float64)
+            if t == F - 1:
+                outs[v] = o.cpu().numpy()
+        d64 = ref64.step(coef)
+        for v in sess:
+            rel[v].append(float(np.linalg.norm(got[v] - d64) / np.linalg.norm(d64)))
+            absmax[v] = max(absmax[v], float(np.abs(got[v] - d64).max()))
+    thr = float(sess[False].read(wc.READ_THRESHOLD)[0])
+    # the last frame through the FP64 pipeline: FP64 DWT, the FP64 delta, the same threshold
+    flat, bands, low, I, rgb = ref64.coefficients(host[F - 1])
+    amp = fp64.fade_amp(200.0, warm + F - 1, warm)
+    nb, k = [], 0
+    for l, lvl in enumerate(bands):
+        al = amp * 0.5 if l == 0 else amp
+        cur = []
+        for b in lvl:
+            dd = d64[k: k + b.size].reshape(b.shape)
+            cur.append(np.where(np.abs(b) > thr, b + al * dd, b))
+            k += b.size
+        nb.append(tuple(cur))
+    g64 = fp64.dwt_inverse(nb, low, w, h)
+    out64 = fp64.to_u8(np.clip(rgb + fp64.guided(I, g64 - I)[..., None], 0.0, 1.0)).astype(int)
+    so = orc.stream(width=w, height=h, **band)
+    rgbf = orc.u8_to_float(host)
+    for t in range(F):
+        r = so.process(rgbf[t])
+    out_ref = orc.float_to_u8(r).astype(int)
+
+    def cmp(x, y):
+        d = np.abs(x.astype(int) - y)
+        return {"max_lsb": int(d.max()), "rms_lsb": round(float(np.sqrt((d.astype(float) ** 2).mean())), 5),
+                "frac_gt1": float((d > 1).mean())}
+    iir = {}
+    for v, name in ((False, "fp32_state"), (True, "fp64_state")):
+        iir[name] = {"state_bytes_per_position": 32 if v else 16,
+                     "delta_rel_l2_vs_fp64": {"max": float(max(rel[v])), "last": rel[v][-1]},
+                     "delta_max_abs_vs_fp64": absmax[v],
+                     "output_vs_fp64": cmp(outs[v], out64), "output_vs_reference": cmp(outs[v], out_ref)}
+    for s in sess.values():
+        s.close()
+
+    # ---- window mode ws 64: FP32 vs FP16 ring
+    ws = 64
+    Fw = ws + 16
+    wcfg = dict(fps=240.0, amp=200.0, use_iir=False, window=ws)
+    ws_sess = {v: wc.Session(width=w, height=h, device=local, ring_fp16=v, **wcfg) for v in (False, True)}
+    hist = []
+    wouts = {}
+    for t in range(Fw):
+        for v, s in ws_sess.items():
+            if t == ws:
+                s.set_timing(True)
+            s.process_u8(d_in[t % F], o)
+            torch.cuda.synchronize(dev)
+            if t == Fw - 1:
+                wouts[v] = o.cpu().numpy()
+        c = _unique(ws_sess[False].read(wc.READ_ORIG6), dims)
+        hist.append(c[::8].copy())
+    dw64 = fp64.window_delta(np.stack(hist[-ws:]), False)
+    pu = sum(3 * sw * sh for (sw, sh) in dims)
+    win = {}
+    for v, name in ((False, "fp32_ring"), (True, "fp16_ring")):
+        s = ws_sess[v]
+        dv = _unique(s.read(wc.READ_DELTA6), dims)[::8].astype(np.float64)
+        times, nfr = s.stage_times()
+        ms = times["temporal_amplify"] / max(nfr, 1)
+        win[name] = {"ring_bytes_per_frame": (ws + 1) * pu * (2 if v else 4),
+                     "delta_rel_l2_vs_fp64": float(np.linalg.norm(dv - dw64) / np.linalg.norm(dw64)),
+                     "temporal_stage_ms_per_frame": round(ms, 4)}
+    win["fp16_ring"]["output_vs_fp32_ring"] = cmp(wouts[True], wouts[False].astype(int))
+    for s in ws_sess.values():
+        s.close()
+    print(json.dumps({"metric": "precision", "workload": "precision_720p_240fps", "frames": F,
+                      "config": {"size": f"{w}x{h}", "fps": 240, "band_hz": [0.2, 0.6], "amp": 200,
+                                 "warmup": warm, "window": ws},
+                      "iir": iir, "window_ws64": win, "seconds": round(time.perf_counter() - t0, 1)}),
+          flush=True)
+
+
 def main():
     a = parse()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     synth_name, kw = WORKLOADS[a.workload]
+    if a.workload == "precision_report":
+        return bench_precision(a, rank, world, local)
     if a.workload == "served_poisson":
         if a.impl == "reference":
             if rank == 0:

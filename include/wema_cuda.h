@@ -46,6 +46,9 @@ typedef struct {
     int   iir_state_fp64;    /* precision variant: biquad state and its update in FP64
                                 (the FP32-designed coefficients promoted; 32 B of state
                                 per position instead of 16).  0: the reference's FP32 */
+    int   ring_fp16;         /* precision variant, window mode: the temporal ring stored
+                                in FP16 (round to nearest), arithmetic in FP32; halves
+                                the ring's bytes (read ws times per position per frame) */
 } wema_cuda_config;
 
 /* Fills *cfg with the reference CLI's defaults for a stream of the given

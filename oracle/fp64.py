@@ -180,6 +180,16 @@ def cascade(c, st, x):
     return y
 
 
+def preseed(c, warmup: int, x: np.ndarray) -> np.ndarray:
+    """State after `warmup` cascade steps from zero with the constant input x.
+    The cascade is linear and time-invariant, so that state is x times the
+    state reached from input 1 (iterated once, on scalars)."""
+    one = np.zeros((4, 1))
+    for _ in range(warmup):
+        cascade(c, one, 1.0)
+    return one * np.asarray(x, dtype=np.float64)[None, :]
+
+
 def fade_amp(amp: float, frames_before: int, warmup: int) -> float:
     g = frames_before - warmup
     if g < 0:
@@ -187,6 +197,29 @@ def fade_amp(amp: float, frames_before: int, warmup: int) -> float:
     if g >= 15:
         return amp
     return ((g + 1) / 15.0) ** 2 * amp
+
+
+# ------------------------------------------------------ window filter
+def window_delta(x: np.ndarray, bilateral: bool) -> np.ndarray:
+    """Window-mode delta (temporal_filter.c:170-319) of x = [ws, n], oldest
+    sample first: x_c - mean with c = ws / 2, or with bilateral weighting
+    w_t = exp(-(x_t - x_c)^2 / (2 s^2)) exp(-(t - c)^2 / (2 (0.15 ws)^2)),
+    s = max(0.5 mean |x_t - x_c|, 1e-3): sum w (x - mean) / sum w."""
+    x = np.asarray(x, dtype=np.float64)
+    ws = x.shape[0]
+    c = ws // 2
+    mean = x.mean(axis=0)
+    cur = x[c]
+    d = cur - mean
+    if not bilateral:
+        return d
+    sigma = np.maximum(0.5 * np.abs(x - cur).mean(axis=0), 1e-3)
+    t = np.arange(ws, dtype=np.float64)[:, None]
+    tw = np.exp(-((t - c) ** 2) / (2.0 * (0.15 * ws) ** 2))
+    w = np.exp(-((x - cur) ** 2) / (2.0 * sigma ** 2)) * tw
+    sw = w.sum(axis=0)
+    res = (w * (x - mean)).sum(axis=0)
+    return np.where(sw > 1e-8, res / np.where(sw > 1e-8, sw, 1.0), d)
 
 
 # ----------------------------------------------------------- guided filter
@@ -242,9 +275,7 @@ class Stream64:
     def step(self, flat: np.ndarray) -> np.ndarray:
         """The band-passed delta of one frame's coefficients (preseed first)."""
         if self.state is None:
-            self.state = np.zeros((4, flat.size))
-            for _ in range(self.warmup):
-                cascade(self.c, self.state, flat)
+            self.state = preseed(self.c, self.warmup, flat)
             self.frames = self.warmup
         return cascade(self.c, self.state, flat)
 

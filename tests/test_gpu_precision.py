@@ -6,7 +6,9 @@ state variant (wema_cuda_config.iir_state_fp64) must follow the FP64 cascade
 to FP32 rounding of its output, and so must sit far closer to it than the
 FP32 state does.  Both cascades are fed the same (GPU, FP32) coefficients, so
 the comparison isolates the state precision.  A batched FP64-state stream must
-also equal the same stream alone, bit for bit."""
+also equal the same stream alone, bit for bit.  In window mode the FP16 ring
+variant (wema_cuda_config.ring_fp16) must stay within FP16 rounding of the
+FP64 window filter over the same coefficients."""
 import numpy as np
 import pytest
 
@@ -95,3 +97,41 @@ def test_fp64_state_batched_equals_alone(torch_cuda):
             assert np.array_equal(o.cpu().numpy(), outs[k][t].cpu().numpy()), f"stream {k} frame {t}"
         s.close()
     b.close()
+
+
+@pytest.mark.parametrize("bilateral", [False, True])
+def test_fp16_ring_against_fp64_window(oracle, torch_cuda, bilateral):
+    torch = torch_cuda
+    w, h, ws = 160, 96, 16
+    F = ws + 6
+    cfg = dict(fps=30.0, amp=60.0, use_iir=False, window=ws, bilateral=bilateral)
+    u8 = SynthVideo(SynthSpec(w, h, 30.0, 5, [1.3], [0.4], 14.0, 2.0)).frames(0, F)
+    d_in = torch.from_numpy(u8).cuda()
+    dims = oracle.subband_dims(w, h)
+    sess = {v: wc.Session(width=w, height=h, ring_fp16=v, **cfg) for v in (False, True)}
+    hist = []
+    worst = {False: 0.0, True: 0.0}
+    lsb = 0
+    for t in range(F):
+        outs = {}
+        for v, s in sess.items():
+            o = torch.empty((h, w, 3), dtype=torch.uint8, device="cuda")
+            s.process_u8(d_in[t], o)
+            torch.cuda.synchronize()
+            outs[v] = o.cpu().numpy().astype(int)
+            coef = unique_slots(s.read(wc.READ_ORIG6), dims)
+        hist.append(coef)
+        if t < ws - 1:
+            assert np.array_equal(outs[True], u8[t])       # passthrough until the ring is full
+            continue
+        d64 = fp64.window_delta(np.stack(hist[-ws:]), bilateral)
+        scale = np.linalg.norm(coef)
+        for v, s in sess.items():
+            d = unique_slots(s.read(wc.READ_DELTA6), dims)
+            worst[v] = max(worst[v], float(np.linalg.norm(d - d64) / scale))
+        lsb = max(lsb, int(np.abs(outs[True] - outs[False]).max()))
+    assert worst[False] < 1e-6, f"FP32 ring {worst[False]:.2e}"
+    assert worst[True] < 1e-3, f"FP16 ring {worst[True]:.2e}"    # FP16 rounds to 2^-11 relative
+    assert lsb <= 2, f"FP16 vs FP32 ring output differs by {lsb} LSB"
+    for s in sess.values():
+        s.close()

@@ -117,10 +117,11 @@ struct WindowParams {
     long long pu;               // unique positions
     int ws, head;               // window size, ring slot of the oldest sample
     int bilateral;
+    int fp16;                   // ring elements are __half (else float)
     float time_w[256];
 };
-cudaError_t launch_ring_push(const float* coef, float* ring, long long pu, int slot, cudaStream_t st);
-cudaError_t launch_window(const WindowParams& wp, const float* ring, float* delta,
+cudaError_t launch_ring_push(const float* coef, void* ring, int fp16, long long pu, int slot, cudaStream_t st);
+cudaError_t launch_window(const WindowParams& wp, const void* ring, float* delta,
                           cudaStream_t st);
 
 // ---- batched launches: one launch of a kernel over many streams --------------

@@ -132,6 +132,7 @@ static void layout(Arena& A, Session& s) {
     }
     for (int c = 0; c < s.nch; c++) {
         if (s.cfg.use_iir) s.state[c] = A.take<float4>(s.cfg.iir_state_fp64 ? 2 * pu : pu);
+        else if (s.cfg.ring_fp16) s.ring[c] = A.take<uint16_t>((size_t)pu * s.cfg.temporal_window);
         else s.ring[c] = A.take<float>((size_t)pu * s.cfg.temporal_window);
         s.ampl[c] = A.take<float>(pu);
         void* t = A.take<char>(thr_scratch_bytes(n6));
@@ -148,6 +149,7 @@ static bool valid_config(const wema_cuda_config& c) {
         return false;
     }
     if (c.iir_state_fp64 != 0 && c.iir_state_fp64 != 1) { set_error("iir_state_fp64 must be 0 or 1"); return false; }
+    if (c.ring_fp16 != 0 && c.ring_fp16 != 1) { set_error("ring_fp16 must be 0 or 1"); return false; }
     return true;
 }
 
@@ -358,7 +360,7 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
         launches += nch;
     } else {
         for (int c = 0; c < nch; c++)
-            if (!cuda_ok(launch_ring_push(q.coef[c], ring[c], pu, head, s_tmp), "ring push"))
+            if (!cuda_ok(launch_ring_push(q.coef[c], ring[c], cfg.ring_fp16, pu, head, s_tmp), "ring push"))
                 return false;
         launches += nch;
         head = (head + 1) % cfg.temporal_window;
@@ -372,6 +374,7 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
             wp.ws = cfg.temporal_window;
             wp.head = head;   // oldest sample (temporal_filter.c:221)
             wp.bilateral = cfg.bilateral_temp;
+            wp.fp16 = cfg.ring_fp16;
             const int ws = cfg.temporal_window, center = ws / 2;
             const float ts = (float)ws * 0.15f;
             const float inv2 = 0.5f / (ts * ts);

@@ -63,7 +63,7 @@ public:
     cudaStream_t arena_stream = nullptr;   // set: arena from the stream-ordered pool (batched)
     Slot slot[kSlots];
     float4* state[3] = {};             // IIR state (shared by the slots, updated in frame order)
-    float* ring[3] = {};               // window ring
+    void* ring[3] = {};                // window ring (float, or __half with ring_fp16)
     float* ampl[3] = {};               // materialised amplified coefficients (inspection)
     ThrScratch thr_s[3] = {};          // threshold scratch + binade history (frame order)
     bool thr_hist = false;

@@ -12,6 +12,13 @@
 //              delta = sum w_t (x_t - mean) / sum w_t  (if sum w_t > 1e-8).
 // The reference's vectorised reductions and vector expf order these sums
 // differently; deltas agree to a few ulp, the bar for this stage.
+//
+// Precision variant (fp16): the ring's samples are stored as FP16 (rounded to
+// nearest on the push) and widened to FP32 as they are read; every sum, the
+// mean, the weights and the delta stay FP32.  The ring is the window mode's
+// dominant traffic (ws reads per position per frame), so this halves it.
+#include <cuda_fp16.h>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -19,20 +26,28 @@ namespace wema {
 
 constexpr int WIN_THREADS = 256;
 
-__global__ void k_ring_push(const float* coef, float* ring, long long pu, int slot) {
-    float* dst = ring + (long long)slot * pu;
+__device__ __forceinline__ void put(float* p, float v) { *p = v; }
+__device__ __forceinline__ void put(__half* p, float v) { *p = __float2half_rn(v); }
+__device__ __forceinline__ float get(const float* p) { return *p; }
+__device__ __forceinline__ float get(const __half* p) { return __half2float(*p); }
+
+template <class T>
+__global__ void k_ring_push(const float* coef, T* ring, long long pu, int slot) {
+    T* dst = ring + (long long)slot * pu;
     for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < pu;
          u += (long long)gridDim.x * blockDim.x)
-        dst[u] = coef[u];
+        put(dst + u, coef[u]);
 }
 
+template <class T>
 struct WinDev {
     WindowParams w;
-    const float* ring;
+    const T* ring;
     float* delta_out;
 };
 
-__global__ void __launch_bounds__(WIN_THREADS) k_window(WinDev a) {
+template <class T>
+__global__ void __launch_bounds__(WIN_THREADS) k_window(WinDev<T> a) {
     const long long pu = a.w.pu;
     const int ws = a.w.ws, head = a.w.head, center = ws / 2;
     const float inv_ws = __fdiv_rn(1.0f, (float)ws);
@@ -42,7 +57,7 @@ __global__ void __launch_bounds__(WIN_THREADS) k_window(WinDev a) {
         for (int t = 0; t < ws; t++) {
             int slot = head + t;
             if (slot >= ws) slot -= ws;
-            const float v = a.ring[(long long)slot * pu + u];
+            const float v = get(a.ring + (long long)slot * pu + u);
             sum = __fadd_rn(sum, v);
             if (t == center) cur = v;
         }
@@ -53,7 +68,7 @@ __global__ void __launch_bounds__(WIN_THREADS) k_window(WinDev a) {
             for (int t = 0; t < ws; t++) {
                 int slot = head + t;
                 if (slot >= ws) slot -= ws;
-                mad = __fadd_rn(mad, fabsf(__fadd_rn(a.ring[(long long)slot * pu + u], -cur)));
+                mad = __fadd_rn(mad, fabsf(__fadd_rn(get(a.ring + (long long)slot * pu + u), -cur)));
             }
             const float sigma = fmaxf(__fmul_rn(__fmul_rn(inv_ws, 0.5f), mad), 0.001f);
             const float inv2 = __fdiv_rn(0.5f, __fmul_rn(sigma, sigma));
@@ -61,7 +76,7 @@ __global__ void __launch_bounds__(WIN_THREADS) k_window(WinDev a) {
             for (int t = 0; t < ws; t++) {
                 int slot = head + t;
                 if (slot >= ws) slot -= ws;
-                const float v = a.ring[(long long)slot * pu + u];
+                const float v = get(a.ring + (long long)slot * pu + u);
                 const float df = __fadd_rn(v, -cur);
                 const float wt = __fmul_rn(expf(-__fmul_rn(__fmul_rn(df, df), inv2)), a.w.time_w[t]);
                 wsum = __fadd_rn(wsum, wt);
@@ -73,18 +88,26 @@ __global__ void __launch_bounds__(WIN_THREADS) k_window(WinDev a) {
     }
 }
 
-cudaError_t launch_ring_push(const float* coef, float* ring, long long pu, int slot,
+cudaError_t launch_ring_push(const float* coef, void* ring, int fp16, long long pu, int slot,
                              cudaStream_t st) {
     long long b = (pu + 255) / 256;
-    k_ring_push<<<(int)(b < 148 * 8 ? (b > 0 ? b : 1) : 148 * 8), 256, 0, st>>>(coef, ring, pu, slot);
+    const int g = (int)(b < 148 * 8 ? (b > 0 ? b : 1) : 148 * 8);
+    if (fp16) k_ring_push<__half><<<g, 256, 0, st>>>(coef, static_cast<__half*>(ring), pu, slot);
+    else k_ring_push<float><<<g, 256, 0, st>>>(coef, static_cast<float*>(ring), pu, slot);
     return cudaGetLastError();
 }
 
-cudaError_t launch_window(const WindowParams& wp, const float* ring, float* delta,
+cudaError_t launch_window(const WindowParams& wp, const void* ring, float* delta,
                           cudaStream_t st) {
-    WinDev a{wp, ring, delta};
     long long b = (wp.pu + WIN_THREADS - 1) / WIN_THREADS;
-    k_window<<<(int)(b < 148 * 16 ? (b > 0 ? b : 1) : 148 * 16), WIN_THREADS, 0, st>>>(a);
+    const int g = (int)(b < 148 * 16 ? (b > 0 ? b : 1) : 148 * 16);
+    if (wp.fp16) {
+        WinDev<__half> a{wp, static_cast<const __half*>(ring), delta};
+        k_window<__half><<<g, WIN_THREADS, 0, st>>>(a);
+    } else {
+        WinDev<float> a{wp, static_cast<const float*>(ring), delta};
+        k_window<float><<<g, WIN_THREADS, 0, st>>>(a);
+    }
     return cudaGetLastError();
 }
 
