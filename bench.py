@@ -1,26 +1,33 @@
 """Benchmark: WEMA per-frame amplification on B200.
 
-Workload (default): one 1920x1080 RGB24 stream at 30 fps - the reference's
-plain full-HD configuration: amp 120, band 0.5-3.0 Hz, colour mode (IIR
-band-pass on Y, Cb and Cr; the reference routes --color through
-wema_process_frame, so bilateral and edge-aware are inert there), FP32.
-Seeded synthetic frames with that configuration's content (three discs at
-0.8/1.5/2.5 Hz, +-1 LSB flicker at 0.1 Hz, 2 LSB noise) stand in for the
-600-frame lossless input file.
-
-A step is one frame of the stream through the whole path (RGB24 in ->
-forward DWT -> exact threshold -> IIR + amplify -> inverse DWT -> RGB24 out).
-* value: Mpix-frames/s with the input frames already resident in HBM,
-  device-timed with CUDA events on the session's stream.
-* e2e:   same through the C ABI from pinned host frames: every step copies
-  its RGB24 frame host->device and the output frame device->host.
-* roofline: the dominant stage's algorithmic bytes per frame over its mean
-  duration (CUDA events around each stage on the launching stream) against
-  the measured HBM copy bandwidth.
+Workload (default, mixed_streams_48): 48 camera streams of uneven sizes
+(16 x 640x480@30, 16 x 1280x720@30, 12 x 1920x1080@60, 4 x 3840x2160@30),
+each with its own seed, 1-3 discs at 0.5-4 Hz, amp 20-150, IIR band 0.5-5 Hz,
+luma with the edge-aware guided filter, FP32.  A step is one tick: one frame
+of every stream through the batched path (one launch per kernel type over all
+48 pyramids: RGB24 in -> forward DWT -> exact threshold -> IIR + amplify ->
+inverse DWT -> guided filter -> RGB24 out).
+* value: Mpix-frames/s of back-to-back ticks, inputs resident in HBM,
+  device-timed with CUDA events.
+* plain_gpu / batched_over_plain: the same frames through one session per
+  stream, one stream at a time, each frame waited for.
+* latency_ms: p50/p99 per-frame latency with ticks paced at 60 Hz (30 fps
+  streams in every other tick).
+* e2e: the same ticks with every frame copied in from pinned host memory
+  and every output copied back.
+* roofline: the dominant stage's algorithmic bytes per tick over its mean
+  device time (events around each stage on its stream, a separate pass)
+  against the measured HBM copy bandwidth.
 * cpu_baseline: the reference's own C path (compiled from its sources with
-  its Makefile flags, oracle/_ref) on this host, a bounded sample of frames.
+  its Makefile flags, oracle/_ref) on this host, a bounded sample of the mix.
 
-Multi-GPU (torchrun): every rank runs an independent stream (replicas; the
+Other workloads (--workload): plain_fullhd_color (one 1920x1080 colour
+stream, the reference's plain full-HD configuration), plain_fullhd_luma,
+plain_qvga_luma, precision_720p_240fps, served_poisson (Poisson sessions
+through the served request loop in real time) and precision_report (errors
+of the precision variants against the FP64 re-evaluation).
+
+Multi-GPU (torchrun): every rank runs independent streams (replicas; the
 path has no cross-stream exchange), value = all ranks' pixels / max time.
 """
 from __future__ import annotations
@@ -63,6 +70,10 @@ METRIC = "Mpix-frames/s"
 # profiles/k_thr_monoids_plain_fullhd_color.txt, k_thr_walk_..., k_dwt_inv_level0_...
 # and k_dwt_fwd_level0_... hold the captures and the commands that made them.
 TRAFFIC_NCU = {
+    # k_guided_transfer_multi: 133.39 MB read + 37.21 MB written for a tick of
+    # 16 streams (8 x 640x480 + 8 x 1920x1080, 19.05 Mpix), scaled by pixels
+    # to the 77.72 Mpix of the 48-stream tick
+    ("mixed_streams_48", "luma_transfer"): int((133387008 + 37206784) * 77.722 / 19.046),
     ("plain_fullhd_color", "threshold"): 25081088 + 2323456,
     ("plain_fullhd_color", "inv_dwt_level0"): 43630080 + 278784,
     ("plain_fullhd_color", "fwd_dwt_level0"): 6266624 + 7168,
@@ -75,7 +86,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=8)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="plain_fullhd_color", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="mixed_streams_48", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-frames", type=int, default=12, help="reference frames timed on the host")
     ap.add_argument("--served-seconds", type=float, default=20.0, help="served_poisson measured window")
     ap.add_argument("--precision-frames", type=int, default=480, help="precision_report frames")
@@ -176,6 +187,17 @@ def stage_bytes(w, h, channels, levels_dims, pu):
             "inv_dwt_level0": inv[0], "luma_transfer": xfer}
 
 
+# kernels behind each stage of a batched tick (one launch per tick over every stream)
+STAGE_KERNELS_MULTI = {
+    "fwd_dwt_level0": "k_dwt_fwd_multi<1,1> (level 0, RGB in)",
+    "fwd_dwt_levels": "k_dwt_fwd_multi<1,0> x 3",
+    "threshold": "k_thr_monoids_multi + k_thr_walk_multi",
+    "temporal_amplify": "k_iir_multi",
+    "inv_dwt_levels": "k_dwt_inv_multi<1,0> x 3",
+    "inv_dwt_level0": "k_dwt_inv_multi<1,0> (level 0)",
+    "luma_transfer": "k_guided_transfer_multi",
+}
+
 # kernels behind each stage (one launch per frame unless noted)
 STAGE_KERNELS = {
     "fwd_dwt_level0": "k_dwt_fwd<1|2> (level 0, RGB in)",
@@ -242,6 +264,38 @@ def cpu_reference_rate(name, frames_u8, kw, nframes):
     value = w * h * nframes / dt / 1e6
     return {"value": round(value, 4), "unit": METRIC, "cores": cores_used, "kind": kind,
             "sample": f"{nframes} frames of {name} ({w}x{h}), first-frame preseed included"}
+
+
+def mixed_cpu_sample():
+    """The reference's CPU path on a bounded sample of the mix: 3 frames of
+    one stream of each size, one after another (Mpix-frames/s)."""
+    from wema_b200 import synth as S
+    picks, seen = [], set()
+    for spec, cfg in S.mixed_streams(seed=7):
+        if (spec.width, spec.height) not in seen:
+            seen.add((spec.width, spec.height))
+            picks.append((spec, cfg))
+    tot_pix, tot_s, cores, r = 0, 0.0, 1, {}
+    for spec, cfg in picks:
+        fr = S.SynthVideo(spec).frames(0, 3)
+        r = cpu_reference_rate("mixed_streams_48", fr, cfg, 3)
+        tot_pix += spec.width * spec.height * 3
+        tot_s += spec.width * spec.height * 3 / (r["value"] * 1e6)
+        cores = r["cores"]
+    return {"value": round(tot_pix / tot_s / 1e6, 4), "unit": METRIC, "cores": cores,
+            "kind": r.get("kind"),
+            "sample": "3 frames each of one 640x480, 1280x720, 1920x1080 and 3840x2160 stream "
+                      "of the mix, first-frame preseed included"}
+
+
+def mixed_config(world):
+    from wema_b200 import synth as S
+    pix = sum(spec.width * spec.height for spec, _ in S.mixed_streams(seed=7))
+    return {"workload": "mixed_streams_48", "streams": 48,
+            "mix": "16x640x480@30, 16x1280x720@30, 12x1920x1080@60, 4x3840x2160@30",
+            "mode": "IIR 0.5-5 Hz, luma, edge-aware guided filter",
+            "mpix_per_tick": round(pix / 1e6, 3), "step": "one tick = one frame of every stream",
+            "parallelism": f"replicas x{world}", "l2": "per-tick working set > 126 MB L2 (no flush)"}
 
 
 def bench_mixed(a, rank, world, local):
@@ -359,6 +413,37 @@ def bench_mixed(a, rank, world, local):
         per_frame += [starts[i].elapsed_time(ends[i])] * m
     p50, p99 = float(np.percentile(per_frame, 50)), float(np.percentile(per_frame, 99))
 
+    # ---- per-stage device time of the batched tick (a separate pass, so the
+    # events do not touch the timed region; each tick alone, so a stage's time
+    # is not stretched by the next tick's overlapping work)
+    b.set_timing(True)
+    for i in range(10):
+        tick(i)
+        b.sync()
+    stage_tot, nt = b.stage_times()
+    b.set_timing(False)
+    per_tick = {k: v / max(nt, 1) for k, v in stage_tot.items()}
+    sb = {}
+    for spec, _ in mix:
+        dims = dims_of(spec.width, spec.height)
+        pu = sum(3 * sw * sh for sw, sh in dims)
+        for k, v in stage_bytes(spec.width, spec.height, 1, dims, pu).items():
+            sb[k] = sb.get(k, 0) + v
+    peak, peak_kind = peaks()
+    dom = max(per_tick, key=per_tick.get)
+    achieved = sb[dom] / (per_tick[dom] * 1e-3) / 1e9
+    total_bytes = sum(sb.values())
+    roofline = {"bound": "hbm", "kernel": dom, "kernels": STAGE_KERNELS_MULTI[dom],
+                "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                "traffic": TRAFFIC_NCU.get(("mixed_streams_48", dom)),
+                "algorithmic_bytes_per_launch": sb[dom]}
+    pipeline = {"algorithmic_bytes_per_tick": total_bytes,
+                "stage_ms_per_tick": {k: round(v, 4) for k, v in per_tick.items()},
+                "stage_frac_of_hbm": {k: round(sb[k] / (per_tick[k] * 1e-3) / 1e9 / peak, 4)
+                                      for k in per_tick if per_tick[k] > 0 and sb[k] > 0},
+                "frac_of_hbm_roofline": round(total_bytes / (ms / a.steps * 1e-3) / 1e9 / peak, 4)}
+
     # ---- the plain one-stream-at-a-time GPU path: each stream's frame alone
     # through its own session, one after another, each waited for
     b.close()
@@ -391,11 +476,7 @@ def bench_mixed(a, rank, world, local):
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms / a.steps, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": "mixed_streams_48", "streams": n,
-                   "mix": "16x640x480@30, 16x1280x720@30, 12x1920x1080@60, 4x3840x2160@30",
-                   "mode": "IIR 0.5-5 Hz, luma, edge-aware guided filter",
-                   "mpix_per_tick": round(sum(pix) / 1e6, 3), "step": "one tick = one frame of every stream",
-                   "parallelism": f"replicas x{world}", "l2": "per-tick working set > 126 MB L2 (no flush)"},
+        "config": mixed_config(world),
         "plain_gpu": {"value": round(plain, 2), "unit": METRIC,
                       "how": "each stream's frame through its own session, one at a time, waited for"},
         "batched_over_plain": round(value / plain, 3),
@@ -404,8 +485,14 @@ def bench_mixed(a, rank, world, local):
         "e2e": {"value": round(e2e, 2), "unit": METRIC, "h2d_bytes_per_step": 3 * sum(pix),
                 "d2h_bytes_per_step": 3 * sum(pix)},
         "gpu_launches": launches, "frames_timed": frames_timed,
+        "roofline": roofline, "pipeline": pipeline,
         "clocks": clocks,
     }
+    if rank == 0 and not a.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = mixed_cpu_sample()
+        except Exception as ex:   # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "error": str(ex)[:200]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -670,30 +757,12 @@ def main():
             return bench_mixed(a, rank, world, local)
         if rank != 0:
             return
-        # the reference's CPU path on a bounded sample of the mix: 3 frames of
-        # one stream of each size, one after another
-        from wema_b200 import synth as S
-        mix = S.mixed_streams(seed=7)
-        picks, seen = [], set()
-        for spec, cfg in mix:
-            if (spec.width, spec.height) not in seen:
-                seen.add((spec.width, spec.height))
-                picks.append((spec, cfg))
-        tot_pix, tot_s, cores = 0, 0.0, 1
-        for spec, cfg in picks:
-            fr = S.SynthVideo(spec).frames(0, 3)
-            r = cpu_reference_rate("mixed_streams_48", fr, cfg, 3)
-            tot_pix += spec.width * spec.height * 3
-            tot_s += spec.width * spec.height * 3 / (r["value"] * 1e6)
-            cores = r["cores"]
-        v = round(tot_pix / tot_s / 1e6, 4)
-        cb = {"value": v, "unit": METRIC, "cores": cores, "kind": r["kind"],
-              "sample": "3 frames each of one 640x480, 1280x720, 1920x1080 and 3840x2160 stream "
-                        "of the mix, first-frame preseed included"}
+        cb = mixed_cpu_sample()
+        v = cb["value"]
         print(json.dumps({"metric": METRIC, "value": v, "unit": METRIC, "n_gpus": a.gpus,
                           "steps": 3, "warmup": 0, "higher_is_better": True, "scaling": "weak",
                           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                          "impl": "reference", "config": {"workload": a.workload},
+                          "impl": "reference", "config": mixed_config(a.gpus),
                           "cpu_baseline": cb,
                           "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0,
                                   "d2h_bytes_per_step": 0}}), flush=True)

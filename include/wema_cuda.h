@@ -169,6 +169,12 @@ int wema_cuda_batch_remove(wema_cuda_batch *b, int id);
 int wema_cuda_batch_tick(wema_cuda_batch *b, const int *ids, const void *const *d_in_u8,
                          void *const *d_out_u8, int n, void *wait_event, void *done_event);
 int wema_cuda_batch_sync(wema_cuda_batch *b);
+/* Per-stage device timing of the batched ticks (CUDA events on each stage's
+ * stream, the WEMA_CUDA_STAGES order of wema_cuda_stage_times): times_ms[7]
+ * receives the milliseconds summed over every timed tick, *ticks their
+ * count.  Both wait for the batch. */
+int wema_cuda_batch_set_timing(wema_cuda_batch *b, int enable);
+int wema_cuda_batch_stage_times(wema_cuda_batch *b, double *times_ms, long long *ticks);
 /* Ticks issued, kernels launched, streams held. */
 int wema_cuda_batch_stats(wema_cuda_batch *b, long long *ticks, long long *launches, int *live);
 /* WEMA_CUDA_READ_THRESHOLD of a stream's last frame (waits for the batch). */

@@ -77,6 +77,26 @@ WEMA_API int wema_cuda_batch_tick(wema_cuda_batch* b, const int* ids, const void
                : -1;
 }
 
+WEMA_API int wema_cuda_batch_set_timing(wema_cuda_batch* b, int enable) {
+    clear_error();
+    if (!b) { set_error("null argument"); return -1; }
+    std::lock_guard<std::mutex> lk(b->mu);
+    if (!cuda_ok(cudaSetDevice(b->b.device), "cudaSetDevice")) return -1;
+    if (!b->b.sync()) return -1;
+    for (auto& t : b->b.tb)
+        if (!b->b.collect(t)) return -1;
+    b->b.timing = enable != 0;
+    return 0;
+}
+
+WEMA_API int wema_cuda_batch_stage_times(wema_cuda_batch* b, double* times_ms, long long* ticks) {
+    clear_error();
+    if (!b || !times_ms || !ticks) { set_error("null argument"); return -1; }
+    std::lock_guard<std::mutex> lk(b->mu);
+    if (!cuda_ok(cudaSetDevice(b->b.device), "cudaSetDevice")) return -1;
+    return b->b.stage_times(times_ms, ticks) ? 0 : -1;
+}
+
 WEMA_API int wema_cuda_batch_sync(wema_cuda_batch* b) {
     clear_error();
     if (!b) { set_error("null argument"); return -1; }

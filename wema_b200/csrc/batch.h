@@ -74,6 +74,9 @@ enum {
     L_COUNT
 };
 
+// timed stages (the per-stream path's order, WEMA_CUDA_STAGES)
+enum { T_FWD0, T_FWD, T_THR, T_IIR, T_INV, T_INV0, T_XFER, T_COUNT };
+
 }  // namespace batch_detail
 using namespace batch_detail;
 
@@ -92,7 +95,12 @@ public:
         size_t cap = 0;
         cudaEvent_t done = nullptr;
         bool used = false;
+        cudaEvent_t tev[T_COUNT][2] = {};  // stage start / end (timing on)
+        bool timed = false;               // tev holds a tick not yet added to stage_ms
     } tb[NBUF];
+    bool timing = false;
+    double stage_ms[T_COUNT] = {};
+    long long ticks_timed = 0;
     int cur = 0;
     long long launches = 0;
     long long ticks = 0;
@@ -107,6 +115,9 @@ public:
             if (t.host) cudaFreeHost(t.host);
             if (t.dev) cudaFree(t.dev);
             if (t.done) cudaEventDestroy(t.done);
+            for (auto& p : t.tev)
+                for (cudaEvent_t e : p)
+                    if (e) cudaEventDestroy(e);
         }
         for (cudaStream_t st : {st_main, st_iir, st_xfer})
             if (st) cudaStreamDestroy(st);
@@ -187,6 +198,29 @@ public:
         if (wait && !sync()) return false;
         delete streams[id];
         streams[id] = nullptr;
+        return true;
+    }
+
+    // adds a completed table's stage times to the totals
+    bool collect(Table& t) {
+        if (!t.timed) return true;
+        for (int k = 0; k < T_COUNT; k++) {
+            float ms = 0.f;
+            if (!cuda_ok(cudaEventElapsedTime(&ms, t.tev[k][0], t.tev[k][1]), "stage time")) return false;
+            stage_ms[k] += ms;
+        }
+        ticks_timed++;
+        t.timed = false;
+        return true;
+    }
+
+    // totals over every timed tick (waits for the batch)
+    bool stage_times(double* ms, long long* n) {
+        if (!sync()) return false;
+        for (Table& t : tb)
+            if (!collect(t)) return false;
+        for (int k = 0; k < T_COUNT; k++) ms[k] = stage_ms[k];
+        *n = ticks_timed;
         return true;
     }
 
@@ -350,6 +384,7 @@ public:
         for (Launch& l : L) emit(l);
         Table& t = tb[cur];
         if (t.used && !cuda_ok(cudaEventSynchronize(t.done), "table reuse")) return false;
+        if (!collect(t)) return false;
         if (image.size() > t.cap) {
             if (t.host) cudaFreeHost(t.host);
             if (t.dev) cudaFree(t.dev);
@@ -375,42 +410,64 @@ public:
             if (L[k].n() == 0) return true;
             return ok(fn(), what);
         };
+        auto mark = [&](int stage, int end, cudaStream_t st) {
+            return !timing || cuda_ok(cudaEventRecord(t.tev[stage][end], st), "event record");
+        };
+        if (timing && !t.tev[0][0])
+            for (auto& p : t.tev)
+                for (cudaEvent_t& e : p)
+                    if (!cuda_ok(cudaEventCreate(&e), "cudaEventCreate")) return false;
 
         // forward, then the filter beside the threshold
+        if (!mark(T_FWD0, 0, st_main)) return false;
         if (!go(L_FWD0_LUMA, [&] { return launch_dwt_fwd_multi(kSrcRgbU8, 1, (const FwdLevelParams*)P(L_FWD0_LUMA), M(L_FWD0_LUMA), L[L_FWD0_LUMA].total, st_main); }, "forward DWT"))
             return false;
         if (!go(L_FWD0_COLOR, [&] { return launch_dwt_fwd_multi(kSrcRgbU8, 3, (const FwdLevelParams*)P(L_FWD0_COLOR), M(L_FWD0_COLOR), L[L_FWD0_COLOR].total, st_main); }, "forward DWT"))
             return false;
+        if (!mark(T_FWD0, 1, st_main) || !mark(T_FWD, 0, st_main)) return false;
         for (int k = L_FWD1; k <= L_FWD3; k++)
             if (!go(k, [&] { return launch_dwt_fwd_multi(kSrcPlanes, 1, (const FwdLevelParams*)P(k), M(k), L[k].total, st_main); }, "forward DWT"))
                 return false;
+        if (!mark(T_FWD, 1, st_main)) return false;
         if (!cuda_ok(cudaEventRecord(ev_fwd, st_main), "event record")) return false;
         if (!cuda_ok(cudaStreamWaitEvent(st_iir, ev_fwd, 0), "stream wait")) return false;
+        if (!mark(T_IIR, 0, st_iir)) return false;
         if (!go(L_IIR_PRESEED, [&] { return launch_iir_multi(P(L_IIR_PRESEED), M(L_IIR_PRESEED), L[L_IIR_PRESEED].total, 1, st_iir); }, "IIR preseed"))
             return false;
         if (!go(L_IIR, [&] { return launch_iir_multi(P(L_IIR), M(L_IIR), L[L_IIR].total, 0, st_iir); }, "IIR"))
             return false;
+        if (!mark(T_IIR, 1, st_iir)) return false;
         if (!cuda_ok(cudaEventRecord(ev_iir, st_iir), "event record")) return false;
+        if (!mark(T_THR, 0, st_main)) return false;
         for (int k = L_THR_PART; k <= L_THR_WALK; k++)
             if (!go(k, [&] { return launch_threshold_multi(k - L_THR_PART, P(k), M(k), L[k].total, st_main); }, "threshold"))
                 return false;
+        if (!mark(T_THR, 1, st_main)) return false;
         if (!cuda_ok(cudaStreamWaitEvent(st_main, ev_iir, 0), "stream wait")) return false;
         // the previous tick's transfer still reads its reconstructed luma
         if (xfer_pending && !cuda_ok(cudaStreamWaitEvent(st_main, ev_xfer, 0), "stream wait")) return false;
-        for (int k = L_INV3; k <= L_INV0_LUMA; k++)
+        if (!mark(T_INV, 0, st_main)) return false;
+        for (int k = L_INV3; k <= L_INV1; k++)
             if (!go(k, [&] { return launch_dwt_inv_multi(1, kOutPlanes, (const InvLevelParams*)P(k), M(k), L[k].total, st_main); }, "inverse DWT"))
                 return false;
+        if (!mark(T_INV, 1, st_main) || !mark(T_INV0, 0, st_main)) return false;
+        if (!go(L_INV0_LUMA, [&] { return launch_dwt_inv_multi(1, kOutPlanes, (const InvLevelParams*)P(L_INV0_LUMA), M(L_INV0_LUMA), L[L_INV0_LUMA].total, st_main); }, "inverse DWT"))
+            return false;
         if (!go(L_INV0_COLOR, [&] { return launch_dwt_inv_multi(3, kOutRgb, (const InvLevelParams*)P(L_INV0_COLOR), M(L_INV0_COLOR), L[L_INV0_COLOR].total, st_main); }, "inverse DWT"))
             return false;
+        if (!mark(T_INV0, 1, st_main)) return false;
         // the transfer on its own stream, so the next tick's forward half overlaps it
         if (!cuda_ok(cudaEventRecord(ev_inv, st_main), "event record")) return false;
         if (!cuda_ok(cudaStreamWaitEvent(st_xfer, ev_inv, 0), "stream wait")) return false;
+        if (!mark(T_XFER, 0, st_xfer)) return false;
         if (!go(L_XFER_GUIDED, [&] { return launch_transfer_multi(1, (const TransferParams*)P(L_XFER_GUIDED), M(L_XFER_GUIDED), L[L_XFER_GUIDED].total, st_xfer); }, "luma transfer"))
             return false;
         if (!go(L_XFER_GAUSS, [&] { return launch_transfer_multi(0, (const TransferParams*)P(L_XFER_GAUSS), M(L_XFER_GAUSS), L[L_XFER_GAUSS].total, st_xfer); }, "luma transfer"))
             return false;
+        if (!mark(T_XFER, 1, st_xfer)) return false;
         if (!cuda_ok(cudaEventRecord(ev_xfer, st_xfer), "event record")) return false;
         xfer_pending = true;
+        t.timed = timing;
         if (!cuda_ok(cudaEventRecord(t.done, st_xfer), "event record")) return false;
         if (done && !cuda_ok(cudaEventRecord(done, st_xfer), "event record")) return false;
         t.used = true;

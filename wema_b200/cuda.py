@@ -91,6 +91,8 @@ def lib() -> C.CDLL:
         L.wema_cuda_batch_remove.argtypes = [vp, i]
         L.wema_cuda_batch_tick.argtypes = [vp, C.POINTER(i), C.POINTER(vp), C.POINTER(vp), i, vp, vp]
         L.wema_cuda_batch_sync.argtypes = [vp]
+        L.wema_cuda_batch_set_timing.argtypes = [vp, i]
+        L.wema_cuda_batch_stage_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
         L.wema_cuda_batch_stats.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                                             C.POINTER(i)]
         L.wema_cuda_batch_read.argtypes = [vp, i, i, i, vp, sz]
@@ -293,6 +295,16 @@ class Batch:
 
     def sync(self):
         _check(lib().wema_cuda_batch_sync(self.h), "batch_sync")
+
+    def set_timing(self, enable: bool):
+        _check(lib().wema_cuda_batch_set_timing(self.h, int(bool(enable))), "batch_set_timing")
+
+    def stage_times(self):
+        """-> (dict stage -> total ms over the timed ticks, ticks timed)"""
+        t = (C.c_double * len(Session.STAGES))()
+        n = C.c_longlong()
+        _check(lib().wema_cuda_batch_stage_times(self.h, t, C.byref(n)), "batch_stage_times")
+        return dict(zip(Session.STAGES, list(t))), n.value
 
     def stats(self):
         t, l, n = C.c_longlong(), C.c_longlong(), C.c_int()
