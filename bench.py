@@ -306,12 +306,9 @@ def bench_mixed(a, rank, world, local):
     from wema_b200 import cuda as wc
     from wema_b200 import synth as S
 
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", init_method="env://",
-                                timeout=__import__("datetime").timedelta(seconds=120))
+    from wema_b200 import replicas
+    torch.cuda.set_device(local)
+    dist = replicas.init("nccl")                 # replicas: every rank its own 48 streams
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     mix = S.mixed_streams(seed=7 + rank)

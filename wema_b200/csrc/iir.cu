@@ -125,8 +125,8 @@ __device__ __forceinline__ void iir_body64(const IirDev& a, int block, int nbloc
             const long long u = u0 + j * B;
             if (u < pu) {
                 x[j] = __ldg(coef + u);
-                hp[j] = state[2 * u];
-                lp[j] = state[2 * u + 1];
+                hp[j] = __ldcs(state + 2 * u);
+                lp[j] = __ldcs(state + 2 * u + 1);
             }
         }
 #pragma unroll
@@ -134,8 +134,8 @@ __device__ __forceinline__ void iir_body64(const IirDev& a, int block, int nbloc
             const long long u = u0 + j * B;
             if (u < pu) {
                 dout[u] = cascade64(a.p.c, hp[j], lp[j], x[j]);
-                state[2 * u] = hp[j];
-                state[2 * u + 1] = lp[j];
+                __stcs(state + 2 * u, hp[j]);
+                __stcs(state + 2 * u + 1, lp[j]);
             }
         }
     }
@@ -159,7 +159,7 @@ __device__ __forceinline__ void iir_body(const IirDev& a, int block, int nblocks
             const long long u = u0 + j * B;
             if (u < pu) {
                 x[j] = __ldg(coef + u);
-                st[j] = state[u];
+                st[j] = __ldcs(state + u);          // touched once per frame: evict first
             }
         }
 #pragma unroll
@@ -169,7 +169,7 @@ __device__ __forceinline__ void iir_body(const IirDev& a, int block, int nblocks
                 bool tail;
                 level_of(a.p, u, tail);
                 dout[u] = cascade(a.p.c, st[j], x[j], tail);
-                state[u] = st[j];
+                __stcs(state + u, st[j]);
             }
         }
     }
@@ -178,9 +178,10 @@ __device__ __forceinline__ void iir_body(const IirDev& a, int block, int nblocks
 __global__ void __launch_bounds__(IIR_THREADS) k_iir_preseed(IirDev a) {
     iir_preseed_body(a, blockIdx.x, gridDim.x);
 }
-__global__ void __launch_bounds__(IIR_THREADS) k_iir(IirDev a) { iir_body(a, blockIdx.x, gridDim.x); }
+// (4 CTAs per SM: 64 registers, 32 warps to keep the loads in flight)
+__global__ void __launch_bounds__(IIR_THREADS, 4) k_iir(IirDev a) { iir_body(a, blockIdx.x, gridDim.x); }
 // batched: task = one (stream, channel); the task's grid x is its block count
-__global__ void __launch_bounds__(IIR_THREADS)
+__global__ void __launch_bounds__(IIR_THREADS, 4)
     k_iir_multi(const IirDev* __restrict__ as, const int* __restrict__ map, int preseed) {
     const TaskBlock t = task_block(map, blockIdx.x);
     const int nb = map[map[0] + 2 + t.task];
