@@ -210,18 +210,23 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
                 }
             }
         }
+        float* pout[C];
+#pragma unroll
+        for (int cc = 0; cc < C; cc++) pout[cc] = p.plane_out[cc];
+        const long long vec_end = p.vec_end;
 #pragma unroll
         for (int r = 0; r < RPW; r++) {
             const int ly = warp + r * NWARP;
             if (ly >= RH) continue;
             const int rowpix = (ry0 + ly) * iw + rx0;
+            const bool rowvec = rowpix + RW <= vec_end;   // the whole staged row in the vector body
             float* dst = planes + prow(ly) * RS;
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 const int lx = lane + 32 * h;
                 if (lx >= RW) continue;
                 const int pi = rowpix + lx;
-                const bool vec = pi < p.vec_end;
+                const bool vec = rowvec || pi < vec_end;
                 const float rr = rgb[r][h][0], gg = rgb[r][h][1], bb = rgb[r][h][2];
                 float out[3];
                 if (C == 1) {
@@ -234,7 +239,7 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
 #pragma unroll
                 for (int cc = 0; cc < C; cc++) {
                     dst[cc * PLANE + pcol(lx)] = out[cc];
-                    if (p.plane_out[cc]) p.plane_out[cc][pi] = out[cc];
+                    if (pout[cc]) pout[cc][pi] = out[cc];
                 }
             }
         }
