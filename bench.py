@@ -62,6 +62,9 @@ WORKLOADS = {
     "served_poisson": ("served_sessions", None),
     # error report of the precision variants against the FP64 re-evaluation
     "precision_report": ("precision_720p", None),
+    # a small batched case for full ncu captures: 8 x 640x480 + 8 x 1920x1080
+    # streams of the mix, 6 ticks, each synchronised (not a benchmark line)
+    "profile_batch16": ("mixed_streams", None),
 }
 METRIC = "Mpix-frames/s"
 
@@ -755,12 +758,40 @@ def bench_precision(a, rank, world, local):
           flush=True)
 
 
+def profile_batch16(a, rank, local):
+    """6 synchronised ticks of 16 streams of the mix (the first 8 of 640x480
+    and the first 8 of 1920x1080, seed 7): small enough for ncu --set full."""
+    if rank != 0:
+        return
+    import torch
+    from wema_b200 import cuda as wc
+    from wema_b200 import synth as S
+    torch.cuda.set_device(local)
+    mall = S.mixed_streams(seed=7)
+    mix = [m for m in mall if m[0].width == 640][:8] + [m for m in mall if m[0].width == 1920][:8]
+    b = wc.Batch(device=local, max_streams=len(mix))
+    ids, d_in, d_out = [], [], []
+    for spec, cfg in mix:
+        ids.append(b.add(spec.width, spec.height, **cfg))
+        h = torch.empty((2, spec.height, spec.width, 3), dtype=torch.uint8)
+        S.SynthVideo(spec).frames(0, 2, out=h.numpy())
+        d_in.append(h.cuda())
+        d_out.append(torch.empty((spec.height, spec.width, 3), dtype=torch.uint8, device="cuda"))
+    for i in range(6):
+        b.tick(ids, [d[i % 2] for d in d_in], d_out)
+        b.sync()
+    print(json.dumps({"workload": "profile_batch16", "streams": len(mix), "ticks": b.stats()["ticks"]}))
+    b.close()
+
+
 def main():
     a = parse()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     synth_name, kw = WORKLOADS[a.workload]
+    if a.workload == "profile_batch16":
+        return profile_batch16(a, rank, local)
     if a.workload == "precision_report":
         return bench_precision(a, rank, world, local)
     if a.workload == "served_poisson":
