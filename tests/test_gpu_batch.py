@@ -169,3 +169,32 @@ def test_batch_against_oracle(oracle, torch_cuda, color):
         else:
             assert diff.max() <= 1, f"frame {t}: {diff.max()} LSB"
     b.close()
+
+
+def test_batch_stage_timing(torch_cuda):
+    """Per-stage device times of batched ticks: every stage the tick ran is
+    timed, and timing does not change the frames."""
+    torch = torch_cuda
+    (w, h, cfg) = STREAMS[0]
+    u8 = frames(w, h, 4, seed=51)
+    d = torch.from_numpy(u8).cuda()
+    outs = {}
+    for timed in (False, True):
+        b = wc.Batch(device=0, max_streams=1)
+        sid = b.add(w, h, **cfg)
+        b.set_timing(timed)
+        o = [torch.empty((h, w, 3), dtype=torch.uint8, device="cuda") for _ in range(4)]
+        for t in range(4):
+            b.tick([sid], [d[t]], [o[t]])
+        times, n = b.stage_times()
+        if timed:
+            assert n == 4
+            for k in ("fwd_dwt_level0", "fwd_dwt_levels", "threshold", "temporal_amplify",
+                      "inv_dwt_levels", "inv_dwt_level0", "luma_transfer"):
+                assert times[k] > 0, k
+        else:
+            assert n == 0
+        outs[timed] = [x.cpu().numpy() for x in o]
+        b.close()
+    for t in range(4):
+        assert np.array_equal(outs[False][t], outs[True][t])
