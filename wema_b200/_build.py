@@ -4,6 +4,8 @@ live in ``wema_b200/lib`` and travel with the repository snapshot).
 * ``libwema_cuda.so`` - the C-ABI library (CUDA kernels for sm_100a plus the
   host runtime), compiled by nvcc straight from ``csrc/``.
 * ``libwema_synth.so`` - the seeded synthetic video generator (gcc).
+* ``wema-cuda-cli`` - the reference CLI's command line over raw RGB24 frames,
+  linked against libwema_cuda (gcc).
 """
 from __future__ import annotations
 
@@ -84,6 +86,21 @@ def build_cuda(force: bool = False, verbose: bool = False) -> str:
     return out
 
 
+def cli_path() -> str:
+    return os.path.join(LIB_DIR, "wema-cuda-cli")
+
+
+def build_cli(force: bool = False) -> str:
+    lib = build_cuda()
+    out = cli_path()
+    src = os.path.join(PKG, "cli", "wema_cuda_cli.c")
+    if force or _stale(out, [src, lib, os.path.join(INCLUDE, "wema_cuda.h")]):
+        subprocess.run(["gcc", "-std=c11", "-O2", "-Wall", "-Wextra", "-I", INCLUDE, src, "-o", out,
+                        "-L", LIB_DIR, "-lwema_cuda", "-Wl,-rpath,$ORIGIN"], check=True)
+    return out
+
+
 def build_all(force: bool = False) -> None:
     build_synth(force)
     build_cuda(force)
+    build_cli(force)
