@@ -87,6 +87,17 @@ int wema_cuda_process_host_u8(wema_cuda_session *s, const uint8_t *h_in, uint8_t
 /* Waits for the session's queued work. */
 int wema_cuda_session_sync(wema_cuda_session *s);
 
+/* Snapshot / restore of a stream's whole state (no counterpart in the
+ * reference; for moving a stream between processes or devices and for
+ * recovery): the frame counters and every device buffer (IIR state or window
+ * ring, threshold history, pyramids) copied to caller-owned host memory of
+ * wema_cuda_session_snapshot_bytes() bytes.  Restore into a session of the same
+ * configuration (any device): its next frame continues the stream exactly as
+ * the original would have.  Both wait for the session's work. */
+size_t wema_cuda_session_snapshot_bytes(wema_cuda_session *s);
+int wema_cuda_session_snapshot(wema_cuda_session *s, void *host, size_t cap);
+int wema_cuda_session_restore(wema_cuda_session *s, const void *host, size_t bytes);
+
 /* Keep each frame's converted input planes and (colour) reconstructed planes
  * so WEMA_CUDA_READ_GRAY_IN / _GRAY_OUT can return them (off by default: they
  * cost two extra plane writes per channel and frame). */
@@ -175,6 +186,11 @@ int wema_cuda_batch_sync(wema_cuda_batch *b);
  * count.  Both wait for the batch. */
 int wema_cuda_batch_set_timing(wema_cuda_batch *b, int enable);
 int wema_cuda_batch_stage_times(wema_cuda_batch *b, double *times_ms, long long *ticks);
+/* Snapshot / restore of one batched stream (as the session calls; a batched
+ * stream's snapshot restores into a batched stream of the same config). */
+size_t wema_cuda_batch_snapshot_bytes(wema_cuda_batch *b, int id);
+int wema_cuda_batch_snapshot(wema_cuda_batch *b, int id, void *host, size_t cap);
+int wema_cuda_batch_restore(wema_cuda_batch *b, int id, const void *host, size_t bytes);
 /* Ticks issued, kernels launched, streams held. */
 int wema_cuda_batch_stats(wema_cuda_batch *b, long long *ticks, long long *launches, int *live);
 /* WEMA_CUDA_READ_THRESHOLD of a stream's last frame (waits for the batch). */

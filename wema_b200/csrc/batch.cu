@@ -97,6 +97,32 @@ WEMA_API int wema_cuda_batch_stage_times(wema_cuda_batch* b, double* times_ms, l
     return b->b.stage_times(times_ms, ticks) ? 0 : -1;
 }
 
+WEMA_API size_t wema_cuda_batch_snapshot_bytes(wema_cuda_batch* b, int id) {
+    clear_error();
+    if (!b) { set_error("null argument"); return 0; }
+    std::lock_guard<std::mutex> lk(b->mu);
+    if (id < 0 || id >= (int)b->b.streams.size() || !b->b.streams[id]) { set_error("no stream %d", id); return 0; }
+    return b->b.streams[id]->snapshot_bytes();
+}
+
+WEMA_API int wema_cuda_batch_snapshot(wema_cuda_batch* b, int id, void* host, size_t cap) {
+    clear_error();
+    if (!b) { set_error("null argument"); return -1; }
+    std::lock_guard<std::mutex> lk(b->mu);
+    if (id < 0 || id >= (int)b->b.streams.size() || !b->b.streams[id]) { set_error("no stream %d", id); return -1; }
+    if (!cuda_ok(cudaSetDevice(b->b.device), "cudaSetDevice") || !b->b.sync()) return -1;
+    return b->b.streams[id]->snapshot(host, cap) ? 0 : -1;
+}
+
+WEMA_API int wema_cuda_batch_restore(wema_cuda_batch* b, int id, const void* host, size_t bytes) {
+    clear_error();
+    if (!b) { set_error("null argument"); return -1; }
+    std::lock_guard<std::mutex> lk(b->mu);
+    if (id < 0 || id >= (int)b->b.streams.size() || !b->b.streams[id]) { set_error("no stream %d", id); return -1; }
+    if (!cuda_ok(cudaSetDevice(b->b.device), "cudaSetDevice") || !b->b.sync()) return -1;
+    return b->b.streams[id]->restore(host, bytes) ? 0 : -1;
+}
+
 WEMA_API int wema_cuda_batch_sync(wema_cuda_batch* b) {
     clear_error();
     if (!b) { set_error("null argument"); return -1; }

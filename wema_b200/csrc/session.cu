@@ -492,6 +492,79 @@ bool Session::run_on(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8,
 // ===================================================================== C ABI
 using namespace wema;
 
+// ---------------------------------------------------------------- snapshot
+namespace {
+struct SnapHeader {
+    char magic[8];                     // "WEMASNAP"
+    int version, nslots;
+    wema_cuda_config cfg;
+    unsigned long long arena_bytes;
+    long long frames_run;
+    int frames_processed, head, filled, last_slot, thr_hist;
+    int valid[kSlots], passthrough[kSlots];
+    float alpha[kSlots][3];
+};
+constexpr int kSnapVersion = 1;
+}  // namespace
+
+size_t Session::snapshot_bytes() const { return sizeof(SnapHeader) + arena_bytes; }
+
+bool Session::snapshot(void* host, size_t cap) const {
+    if (!host || cap < snapshot_bytes()) { set_error("snapshot needs %zu bytes", snapshot_bytes()); return false; }
+    SnapHeader h{};
+    memcpy(h.magic, "WEMASNAP", 8);
+    h.version = kSnapVersion;
+    h.nslots = nslots;
+    h.cfg = cfg;
+    h.arena_bytes = arena_bytes;
+    h.frames_run = frames_run;
+    h.frames_processed = frames_processed;
+    h.head = head;
+    h.filled = filled;
+    h.last_slot = last_slot;
+    h.thr_hist = thr_hist;
+    for (int i = 0; i < kSlots; i++) {
+        h.valid[i] = slot[i].valid;
+        h.passthrough[i] = slot[i].passthrough;
+        for (int c = 0; c < 3; c++) h.alpha[i][c] = slot[i].alpha[c];
+    }
+    memcpy(host, &h, sizeof h);
+    return cuda_ok(cudaMemcpy((char*)host + sizeof h, arena, arena_bytes, cudaMemcpyDeviceToHost),
+                   "snapshot copy");
+}
+
+bool Session::restore(const void* host, size_t bytes) {
+    SnapHeader h;
+    if (!host || bytes < sizeof h) { set_error("not a session snapshot"); return false; }
+    memcpy(&h, host, sizeof h);
+    if (memcmp(h.magic, "WEMASNAP", 8) || h.version != kSnapVersion) {
+        set_error("not a session snapshot (or another version)");
+        return false;
+    }
+    wema_cuda_config a = h.cfg, b = cfg;
+    a.device = b.device = 0;             // a snapshot may move to another device
+    if (memcmp(&a, &b, sizeof a) || h.nslots != nslots || h.arena_bytes != arena_bytes ||
+        bytes < sizeof h + arena_bytes) {
+        set_error("snapshot is of another stream configuration");
+        return false;
+    }
+    if (!cuda_ok(cudaMemcpy(arena, (const char*)host + sizeof h, arena_bytes, cudaMemcpyHostToDevice),
+                 "restore copy"))
+        return false;
+    frames_run = h.frames_run;
+    frames_processed = h.frames_processed;
+    head = h.head;
+    filled = h.filled;
+    last_slot = h.last_slot;
+    thr_hist = h.thr_hist != 0;
+    for (int i = 0; i < kSlots; i++) {
+        slot[i].valid = h.valid[i] != 0;
+        slot[i].passthrough = h.passthrough[i] != 0;
+        for (int c = 0; c < 3; c++) slot[i].alpha[c] = h.alpha[i][c];
+    }
+    return true;
+}
+
 struct wema_cuda_session {
     Session s;
 };
@@ -592,6 +665,26 @@ WEMA_API int wema_cuda_session_sync(wema_cuda_session* s) {
     if (!s) { set_error("null session"); return -1; }
     if (!cuda_ok(cudaSetDevice(s->s.cfg.device), "cudaSetDevice")) return -1;
     return s->s.sync_all() ? 0 : -1;
+}
+
+WEMA_API size_t wema_cuda_session_snapshot_bytes(wema_cuda_session* s) {
+    clear_error();
+    if (!s) { set_error("null session"); return 0; }
+    return s->s.snapshot_bytes();
+}
+
+WEMA_API int wema_cuda_session_snapshot(wema_cuda_session* s, void* host, size_t cap) {
+    clear_error();
+    if (!s) { set_error("null session"); return -1; }
+    if (!cuda_ok(cudaSetDevice(s->s.cfg.device), "cudaSetDevice") || !s->s.sync_all()) return -1;
+    return s->s.snapshot(host, cap) ? 0 : -1;
+}
+
+WEMA_API int wema_cuda_session_restore(wema_cuda_session* s, const void* host, size_t bytes) {
+    clear_error();
+    if (!s) { set_error("null session"); return -1; }
+    if (!cuda_ok(cudaSetDevice(s->s.cfg.device), "cudaSetDevice") || !s->s.sync_all()) return -1;
+    return s->s.restore(host, bytes) ? 0 : -1;
 }
 
 WEMA_API int wema_cuda_set_inspect(wema_cuda_session* s, int enable) {

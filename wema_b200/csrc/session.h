@@ -101,6 +101,13 @@ public:
     PyrView view(int b, int c) const;
     bool ensure_staging();
     bool materialize_amplified();      // ampl[] = amplified coefficients of the last frame
+
+    // snapshot / restore of the whole stream state (the caller has waited for
+    // the session's work): a header of the host-side frame counters, then the
+    // device state.  Restore needs a session of the same config and buffer sets.
+    size_t snapshot_bytes() const;
+    bool snapshot(void* host, size_t cap) const;
+    bool restore(const void* host, size_t bytes);
 };
 
 }  // namespace wema

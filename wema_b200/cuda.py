@@ -91,6 +91,14 @@ def lib() -> C.CDLL:
         L.wema_cuda_batch_remove.argtypes = [vp, i]
         L.wema_cuda_batch_tick.argtypes = [vp, C.POINTER(i), C.POINTER(vp), C.POINTER(vp), i, vp, vp]
         L.wema_cuda_batch_sync.argtypes = [vp]
+        L.wema_cuda_session_snapshot_bytes.argtypes = [vp]
+        L.wema_cuda_session_snapshot_bytes.restype = sz
+        L.wema_cuda_session_snapshot.argtypes = [vp, vp, sz]
+        L.wema_cuda_session_restore.argtypes = [vp, vp, sz]
+        L.wema_cuda_batch_snapshot_bytes.argtypes = [vp, i]
+        L.wema_cuda_batch_snapshot_bytes.restype = sz
+        L.wema_cuda_batch_snapshot.argtypes = [vp, i, vp, sz]
+        L.wema_cuda_batch_restore.argtypes = [vp, i, vp, sz]
         L.wema_cuda_batch_set_timing.argtypes = [vp, i]
         L.wema_cuda_batch_stage_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
         L.wema_cuda_batch_stats.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
@@ -182,6 +190,17 @@ class Session:
         _check(lib().wema_cuda_process_host_u8(self.h, frame.ctypes.data, out.ctypes.data),
                "process_host_u8")
         return out
+
+    def snapshot(self) -> np.ndarray:
+        """The stream's whole state as host bytes (wema_cuda_session_snapshot)."""
+        n = lib().wema_cuda_session_snapshot_bytes(self.h)
+        buf = np.empty(n, np.uint8)
+        _check(lib().wema_cuda_session_snapshot(self.h, buf.ctypes.data, n), "session_snapshot")
+        return buf
+
+    def restore(self, snap: np.ndarray):
+        snap = np.ascontiguousarray(snap, np.uint8)
+        _check(lib().wema_cuda_session_restore(self.h, snap.ctypes.data, snap.size), "session_restore")
 
     def sync(self):
         _check(lib().wema_cuda_session_sync(self.h), "sync")
@@ -292,6 +311,16 @@ class Batch:
         w = C.c_void_p(wait_event.cuda_event) if wait_event is not None else None
         d = C.c_void_p(done_event.cuda_event) if done_event is not None else None
         _check(lib().wema_cuda_batch_tick(self.h, ia, pin, pout, n, w, d), "batch_tick")
+
+    def snapshot(self, sid: int) -> np.ndarray:
+        n = lib().wema_cuda_batch_snapshot_bytes(self.h, int(sid))
+        buf = np.empty(n, np.uint8)
+        _check(lib().wema_cuda_batch_snapshot(self.h, int(sid), buf.ctypes.data, n), "batch_snapshot")
+        return buf
+
+    def restore(self, sid: int, snap: np.ndarray):
+        snap = np.ascontiguousarray(snap, np.uint8)
+        _check(lib().wema_cuda_batch_restore(self.h, int(sid), snap.ctypes.data, snap.size), "batch_restore")
 
     def sync(self):
         _check(lib().wema_cuda_batch_sync(self.h), "batch_sync")
