@@ -363,38 +363,19 @@ def bench_mixed(a, rank, world, local):
     frames_timed = a.steps * n + 2
     pix_timed = a.steps * sum(pix) + 2 * pix[0]
 
-    # ---- e2e: every tick copies its frames in from pinned host memory and
-    # its outputs back, on two side streams gated by events: tick i's inputs
-    # come in once tick i-1 has read its own, tick i's outputs go out while
-    # tick i+1 runs (two output sets, so no tick writes a set still being
-    # copied).  The host link carries 2 x 233 MB per tick and bounds this.
-    s_h2d, s_d2h = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
-    NB = 2
-    h_out = [torch.empty_like(host[k][0]).pin_memory() for k in range(n)]
-    staged = [torch.empty_like(d_in[k][0]) for k in range(n)]
-    outs = [[torch.empty_like(d_out[k]) for k in range(n)] for _ in range(NB)]
-    ready, done = ev(), ev()
-    drained = [ev() for _ in range(NB)]          # output set j copied out
+    # ---- e2e through the host-frame tick (wema_cuda_batch_tick_host): every
+    # tick's frames are copied in from pinned host memory and its outputs back,
+    # double-buffered inside the library (tick i's inputs come in while tick
+    # i-1 runs, its outputs go out while tick i+1 runs).  The host link
+    # carries 2 x 233 MB per tick and bounds this.
+    h_out = [[torch.empty_like(host[k][0]).pin_memory() for k in range(n)] for _ in range(2)]
     barrier()
     E = max(4, a.steps // 4)
     g0, g1 = ev(), ev()
-    g0.record(s_h2d)
+    g0.record(t_stream)
     for i in range(E):
-        j = i % NB
-        with torch.cuda.stream(s_h2d):
-            s_h2d.wait_event(done)                     # the previous tick read its inputs
-            if i >= NB:
-                s_h2d.wait_event(drained[j])           # output set j is out
-            for k in range(n):
-                staged[k].copy_(host[k][i % K], non_blocking=True)
-            ready.record(s_h2d)
-        b.tick(ids, staged, outs[j], wait_event=ready, done_event=done)
-        with torch.cuda.stream(s_d2h):
-            s_d2h.wait_event(done)
-            for k in range(n):
-                h_out[k].copy_(outs[j][k], non_blocking=True)
-            drained[j].record(s_d2h)
-    g1.record(s_d2h)
+        b.tick_host(ids, [host[k][i % K] for k in range(n)], h_out[i % 2],
+                    wait_event=g0 if i == 0 else None, done_event=g1 if i == E - 1 else None)
     g1.synchronize()
     e2e_ms = g0.elapsed_time(g1)
     barrier()

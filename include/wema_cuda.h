@@ -180,6 +180,16 @@ int wema_cuda_batch_remove(wema_cuda_batch *b, int id);
 int wema_cuda_batch_tick(wema_cuda_batch *b, const int *ids, const void *const *d_in_u8,
                          void *const *d_out_u8, int n, void *wait_event, void *done_event);
 int wema_cuda_batch_sync(wema_cuda_batch *b);
+/* The same tick with HOST frames (RGB24; pin them, e.g. with cudaHostAlloc,
+ * for the copies to overlap): each stream's frame is copied into one of two
+ * device staging sets the batch keeps per stream, the tick runs, the output
+ * is copied back - so tick i's inputs come in while tick i-1 runs and its
+ * outputs go out while tick i+1 runs (the reference's async_io.c double
+ * buffering, on copy engines).  Asynchronous: the copies in wait for
+ * wait_event (may be NULL); a host buffer may be reused once done_event (may
+ * be NULL) has completed, or after wema_cuda_batch_sync. */
+int wema_cuda_batch_tick_host(wema_cuda_batch *b, const int *ids, const void *const *h_in_u8,
+                              void *const *h_out_u8, int n, void *wait_event, void *done_event);
 /* Per-stage device timing of the batched ticks (CUDA events on each stage's
  * stream, the WEMA_CUDA_STAGES order of wema_cuda_stage_times): times_ms[7]
  * receives the milliseconds summed over every timed tick, *ticks their

@@ -198,3 +198,34 @@ def test_batch_stage_timing(torch_cuda):
         b.close()
     for t in range(4):
         assert np.array_equal(outs[False][t], outs[True][t])
+
+
+def test_batch_tick_host_equals_device(torch_cuda):
+    """Host-frame ticks (pinned and pageable buffers, double-buffered staging)
+    give the device ticks' frames."""
+    torch = torch_cuda
+    F = 5
+    sel = [STREAMS[0], STREAMS[2], STREAMS[4]]
+    data = [frames(w, h, F, seed=k + 61, fps=cfg.get("fps", 30.0)) for k, (w, h, cfg) in enumerate(sel)]
+    dev = wc.Batch(device=0, max_streams=4)
+    hst = wc.Batch(device=0, max_streams=4)
+    ids_d = [dev.add(w, h, **cfg) for (w, h, cfg) in sel]
+    ids_h = [hst.add(w, h, **cfg) for (w, h, cfg) in sel]
+    d_in = [torch.from_numpy(u).cuda() for u in data]
+    ref = [[torch.empty((h, w, 3), dtype=torch.uint8, device="cuda") for _ in range(F)] for (w, h, _) in sel]
+    # stream 0 pinned tensors, the others pageable numpy arrays
+    h_in = [[torch.from_numpy(data[0][t]).pin_memory() for t in range(F)]] + \
+           [[np.ascontiguousarray(data[k][t]) for t in range(F)] for k in (1, 2)]
+    h_out = [[torch.empty((sel[0][1], sel[0][0], 3), dtype=torch.uint8).pin_memory() for _ in range(F)]] + \
+            [[np.empty((h, w, 3), np.uint8) for _ in range(F)] for (w, h, _) in sel[1:]]
+    for t in range(F):
+        dev.tick(ids_d, [d[t] for d in d_in], [r[t] for r in ref])
+        hst.tick_host(ids_h, [x[t] for x in h_in], [x[t] for x in h_out])
+    dev.sync()
+    hst.sync()
+    for k in range(len(sel)):
+        for t in range(F):
+            got = h_out[k][t].numpy() if hasattr(h_out[k][t], "numpy") else h_out[k][t]
+            assert np.array_equal(got, ref[k][t].cpu().numpy()), f"stream {k} frame {t}"
+    dev.close()
+    hst.close()

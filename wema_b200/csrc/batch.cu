@@ -77,6 +77,18 @@ WEMA_API int wema_cuda_batch_tick(wema_cuda_batch* b, const int* ids, const void
                : -1;
 }
 
+WEMA_API int wema_cuda_batch_tick_host(wema_cuda_batch* b, const int* ids, const void* const* h_in_u8,
+                                       void* const* h_out_u8, int n, void* wait_event, void* done_event) {
+    clear_error();
+    if (!b || n < 1 || !ids || !h_in_u8 || !h_out_u8) { set_error("bad argument"); return -1; }
+    std::lock_guard<std::mutex> lk(b->mu);
+    if (!cuda_ok(cudaSetDevice(b->b.device), "cudaSetDevice")) return -1;
+    return b->b.tick_host(ids, (const uint8_t* const*)h_in_u8, (uint8_t* const*)h_out_u8, n,
+                          (cudaEvent_t)wait_event, (cudaEvent_t)done_event)
+               ? 0
+               : -1;
+}
+
 WEMA_API int wema_cuda_batch_set_timing(wema_cuda_batch* b, int enable) {
     clear_error();
     if (!b) { set_error("null argument"); return -1; }

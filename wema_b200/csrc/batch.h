@@ -28,6 +28,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <array>
 #include <mutex>
 #include <new>
 #include <vector>
@@ -101,6 +102,18 @@ public:
     bool timing = false;
     double stage_ms[T_COUNT] = {};
     long long ticks_timed = 0;
+
+    // host-frame ticks: two device staging sets (frames in and out) per stream,
+    // copies on their own streams, so tick i's inputs come in while tick i-1
+    // runs and its outputs go out while tick i+1 runs (async_io.c's double
+    // buffering, on copy engines instead of threads)
+    struct HostSet {
+        cudaEvent_t h2d = nullptr, tick = nullptr, d2h = nullptr;
+        bool used = false;
+    } hs[2];
+    cudaStream_t st_h2d = nullptr, st_d2h = nullptr;
+    int hcur = 0;
+    std::vector<std::array<uint8_t*, 4>> hstage;   // by stream id: in0, out0, in1, out1
     int cur = 0;
     long long launches = 0;
     long long ticks = 0;
@@ -108,8 +121,9 @@ public:
     std::vector<char> image;
 
     ~Batch() {
-        for (cudaStream_t st : {st_main, st_iir, st_xfer})
+        for (cudaStream_t st : {st_main, st_iir, st_xfer, st_h2d, st_d2h})
             if (st) cudaStreamSynchronize(st);
+        for (size_t i = 0; i < hstage.size(); i++) free_stage((int)i);
         for (Session* s : streams) delete s;
         for (Table& t : tb) {
             if (t.host) cudaFreeHost(t.host);
@@ -119,10 +133,13 @@ public:
                 for (cudaEvent_t e : p)
                     if (e) cudaEventDestroy(e);
         }
-        for (cudaStream_t st : {st_main, st_iir, st_xfer})
+        for (cudaStream_t st : {st_main, st_iir, st_xfer, st_h2d, st_d2h})
             if (st) cudaStreamDestroy(st);
         for (cudaEvent_t e : {ev_fwd, ev_iir, ev_inv, ev_xfer})
             if (e) cudaEventDestroy(e);
+        for (HostSet& h : hs)
+            for (cudaEvent_t e : {h.h2d, h.tick, h.d2h})
+                if (e) cudaEventDestroy(e);
     }
 
     bool init(int dev, int max_n) {
@@ -143,6 +160,13 @@ public:
                 return false;
         if (!cuda_ok(cudaStreamCreateWithPriority(&st_xfer, cudaStreamNonBlocking, lo), "cudaStreamCreate"))
             return false;
+        for (cudaStream_t* st : {&st_h2d, &st_d2h})
+            if (!cuda_ok(cudaStreamCreateWithFlags(st, cudaStreamNonBlocking), "cudaStreamCreate"))
+                return false;
+        for (HostSet& h : hs)
+            for (cudaEvent_t* e : {&h.h2d, &h.tick, &h.d2h})
+                if (!cuda_ok(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate"))
+                    return false;
         for (cudaEvent_t* e : {&ev_fwd, &ev_iir, &ev_inv, &ev_xfer})
             if (!cuda_ok(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate"))
                 return false;
@@ -192,10 +216,25 @@ public:
         return (int)streams.size() - 1;
     }
 
+    // a stream's host-tick staging back to the pool (its copies have completed)
+    void free_stage(int id) {
+        if (id >= (int)hstage.size()) return;
+        for (uint8_t*& p : hstage[id])
+            if (p) {
+                cudaFreeAsync(p, st_main);
+                p = nullptr;
+            }
+    }
+
     // wait = false: the caller knows the stream's last tick has completed
     bool remove(int id, bool wait = true) {
         if (id < 0 || id >= (int)streams.size() || !streams[id]) { set_error("no stream %d", id); return false; }
         if (wait && !sync()) return false;
+        if (id < (int)hstage.size() && hstage[id][0]) {
+            if (!cuda_ok(cudaStreamSynchronize(st_h2d), "sync") || !cuda_ok(cudaStreamSynchronize(st_d2h), "sync"))
+                return false;
+            free_stage(id);
+        }
         delete streams[id];
         streams[id] = nullptr;
         return true;
@@ -230,9 +269,56 @@ public:
     }
 
     bool sync() {
+        if (!cuda_ok(cudaStreamSynchronize(st_h2d), "sync")) return false;
         if (!cuda_ok(cudaStreamSynchronize(st_iir), "sync")) return false;
         if (!cuda_ok(cudaStreamSynchronize(st_main), "sync")) return false;
-        return cuda_ok(cudaStreamSynchronize(st_xfer), "sync");
+        if (!cuda_ok(cudaStreamSynchronize(st_xfer), "sync")) return false;
+        return cuda_ok(cudaStreamSynchronize(st_d2h), "sync");
+    }
+
+    // One tick with host frames (RGB24, pinned for the copies to be
+    // asynchronous): copies in on st_h2d, the tick, copies out on st_d2h.
+    // `done` (may be null) is recorded once every output is in host memory.
+    bool tick_host(const int* ids, const uint8_t* const* h_in, uint8_t* const* h_out, int n,
+                   cudaEvent_t wait, cudaEvent_t done) {
+        HostSet& S = hs[hcur];
+        std::vector<const uint8_t*> din(n);
+        std::vector<uint8_t*> dout(n);
+        for (int k = 0; k < n; k++) {
+            const int id = ids[k];
+            if (id < 0 || id >= (int)streams.size() || !streams[id]) { set_error("no stream %d", id); return false; }
+            if (!h_in[k] || !h_out[k]) { set_error("stream %d: null frame", id); return false; }
+            if ((int)hstage.size() <= id) hstage.resize(id + 1, {nullptr, nullptr, nullptr, nullptr});
+            const size_t fb = 3 * (size_t)streams[id]->g.pixels;
+            if (!hstage[id][0])
+                for (uint8_t*& p : hstage[id])
+                    if (!cuda_ok(cudaMallocAsync((void**)&p, fb, st_h2d), "cudaMallocAsync(host staging)"))
+                        return false;
+            din[k] = hstage[id][2 * hcur];
+            dout[k] = hstage[id][2 * hcur + 1];
+        }
+        // this set was last used two ticks ago: its tick read the inputs and
+        // its outputs went out before they are overwritten
+        if (S.used && (!cuda_ok(cudaStreamWaitEvent(st_h2d, S.tick, 0), "stream wait") ||
+                       !cuda_ok(cudaStreamWaitEvent(st_h2d, S.d2h, 0), "stream wait")))
+            return false;
+        if (wait && !cuda_ok(cudaStreamWaitEvent(st_h2d, wait, 0), "stream wait")) return false;
+        for (int k = 0; k < n; k++)
+            if (!cuda_ok(cudaMemcpyAsync((void*)din[k], h_in[k], 3 * (size_t)streams[ids[k]]->g.pixels,
+                                         cudaMemcpyHostToDevice, st_h2d), "copy in"))
+                return false;
+        if (!cuda_ok(cudaEventRecord(S.h2d, st_h2d), "event record")) return false;
+        if (!tick(ids, din.data(), dout.data(), n, S.h2d, S.tick)) return false;
+        if (!cuda_ok(cudaStreamWaitEvent(st_d2h, S.tick, 0), "stream wait")) return false;
+        for (int k = 0; k < n; k++)
+            if (!cuda_ok(cudaMemcpyAsync(h_out[k], dout[k], 3 * (size_t)streams[ids[k]]->g.pixels,
+                                         cudaMemcpyDeviceToHost, st_d2h), "copy out"))
+                return false;
+        if (!cuda_ok(cudaEventRecord(S.d2h, st_d2h), "event record")) return false;
+        if (done && !cuda_ok(cudaEventRecord(done, st_d2h), "event record")) return false;
+        S.used = true;
+        hcur ^= 1;
+        return true;
     }
 
     // the table image: every launch's parameter array, then its task map

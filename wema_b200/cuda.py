@@ -91,6 +91,7 @@ def lib() -> C.CDLL:
         L.wema_cuda_batch_remove.argtypes = [vp, i]
         L.wema_cuda_batch_tick.argtypes = [vp, C.POINTER(i), C.POINTER(vp), C.POINTER(vp), i, vp, vp]
         L.wema_cuda_batch_sync.argtypes = [vp]
+        L.wema_cuda_batch_tick_host.argtypes = [vp, C.POINTER(i), C.POINTER(vp), C.POINTER(vp), i, vp, vp]
         L.wema_cuda_session_snapshot_bytes.argtypes = [vp]
         L.wema_cuda_session_snapshot_bytes.restype = sz
         L.wema_cuda_session_snapshot.argtypes = [vp, vp, sz]
@@ -324,6 +325,16 @@ class Batch:
 
     def sync(self):
         _check(lib().wema_cuda_batch_sync(self.h), "batch_sync")
+
+    def tick_host(self, ids, inputs, outputs, wait_event=None, done_event=None):
+        """One tick with host frames (numpy arrays or pinned CPU tensors)."""
+        n = len(ids)
+        ia = (C.c_int * n)(*ids)
+        pin = (C.c_void_p * n)(*[_ptr(t) for t in inputs])
+        pout = (C.c_void_p * n)(*[_ptr(t) for t in outputs])
+        w = C.c_void_p(wait_event.cuda_event) if wait_event is not None else None
+        d = C.c_void_p(done_event.cuda_event) if done_event is not None else None
+        _check(lib().wema_cuda_batch_tick_host(self.h, ia, pin, pout, n, w, d), "batch_tick_host")
 
     def set_timing(self, enable: bool):
         _check(lib().wema_cuda_batch_set_timing(self.h, int(bool(enable))), "batch_set_timing")
