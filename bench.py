@@ -732,10 +732,43 @@ def bench_precision(a, rank, world, local):
     win["fp16_ring"]["output_vs_fp32_ring"] = cmp(wouts[True], wouts[False].astype(int))
     for s in ws_sess.values():
         s.close()
+    # ---- the plain 320x240 luma configuration (amp 50, 0.5-3 Hz, 300 frames):
+    # every frame's output against the FP64 pipeline, with the GPU's threshold
+    # (mask identical) and with the FP64 threshold (mask flips included)
+    qs = S.plain_qvga(seed=1)
+    qw, qh, QF = qs.width, qs.height, 300
+    qu8 = S.SynthVideo(qs).frames(0, QF)
+    qd = torch.from_numpy(qu8).to(dev)
+    qcfg = dict(fps=30.0, amp=50.0, f_low=0.5, f_high=3.0)
+    qsess = wc.Session(width=qw, height=qh, device=local, **qcfg)
+    qc32, _ = orc.iir_design(0.5, 3.0, 30.0)
+    q64 = {m: fp64.Stream64(qw, qh, coef=qc32, **qcfg) for m in ("gpu_thr", "fp64_thr")}
+    qso = orc.stream(width=qw, height=qh, **qcfg)
+    qrgb = orc.u8_to_float(qu8)
+    acc = {m: [] for m in ("gpu_thr", "fp64_thr", "reference")}
+    qo = torch.empty((qh, qw, 3), dtype=torch.uint8, device=dev)
+    for t in range(QF):
+        qsess.process_u8(qd[t], qo)
+        torch.cuda.synchronize(dev)
+        g = qo.cpu().numpy().astype(int)
+        thr_t = float(qsess.read(wc.READ_THRESHOLD)[0])
+        acc["gpu_thr"].append(np.abs(g - fp64.to_u8(q64["gpu_thr"].process(qu8[t], thr=thr_t)).astype(int)))
+        acc["fp64_thr"].append(np.abs(g - fp64.to_u8(q64["fp64_thr"].process(qu8[t])).astype(int)))
+        acc["reference"].append(np.abs(g - orc.float_to_u8(qso.process(qrgb[t])).astype(int)))
+    qsess.close()
+    qvga = {}
+    for m, v in acc.items():
+        d = np.stack(v)
+        qvga[m] = {"max_lsb": int(d.max()), "rms_lsb": round(float(np.sqrt((d.astype(float) ** 2).mean())), 5),
+                   "frac_gt1": float((d > 1).mean())}
     print(json.dumps({"metric": "precision", "workload": "precision_720p_240fps", "frames": F,
                       "config": {"size": f"{w}x{h}", "fps": 240, "band_hz": [0.2, 0.6], "amp": 200,
                                  "warmup": warm, "window": ws},
-                      "iir": iir, "window_ws64": win, "seconds": round(time.perf_counter() - t0, 1)}),
+                      "iir": iir, "window_ws64": win,
+                      "plain_qvga_luma_300_frames_output_error": {
+                          "vs_fp64_same_threshold": qvga["gpu_thr"], "vs_fp64_own_threshold": qvga["fp64_thr"],
+                          "vs_reference": qvga["reference"]},
+                      "seconds": round(time.perf_counter() - t0, 1)}),
           flush=True)
 
 
