@@ -298,10 +298,15 @@ public:
             dout[k] = hstage[id][2 * hcur + 1];
         }
         // this set was last used two ticks ago: its tick read the inputs and
-        // its outputs went out before they are overwritten
+        // its outputs went out before they are overwritten.  The copies in also
+        // wait for the previous tick to finish: overlapping them with that
+        // tick's kernels measured slower here (the two copy directions then
+        // contend on the host link while the kernels run)
         if (S.used && (!cuda_ok(cudaStreamWaitEvent(st_h2d, S.tick, 0), "stream wait") ||
                        !cuda_ok(cudaStreamWaitEvent(st_h2d, S.d2h, 0), "stream wait")))
             return false;
+        const HostSet& P = hs[hcur ^ 1];
+        if (P.used && !cuda_ok(cudaStreamWaitEvent(st_h2d, P.tick, 0), "stream wait")) return false;
         if (wait && !cuda_ok(cudaStreamWaitEvent(st_h2d, wait, 0), "stream wait")) return false;
         for (int k = 0; k < n; k++)
             if (!cuda_ok(cudaMemcpyAsync((void*)din[k], h_in[k], 3 * (size_t)streams[ids[k]]->g.pixels,
