@@ -183,9 +183,9 @@ int wema_cuda_batch_sync(wema_cuda_batch *b);
 /* The same tick with HOST frames (RGB24; pin them, e.g. with cudaHostAlloc,
  * for the copies to overlap): each stream's frame is copied into one of two
  * device staging sets the batch keeps per stream, the tick runs, the output
- * is copied back - so tick i's inputs come in while tick i-1 runs and its
- * outputs go out while tick i+1 runs (the reference's async_io.c double
- * buffering, on copy engines).  Asynchronous: the copies in wait for
+ * is copied back - so tick i's outputs go out while tick i+1's inputs come in
+ * and it runs (the reference's async_io.c double buffering, on copy
+ * engines; a tick's copies in start once the previous tick has finished).  Asynchronous: the copies in wait for
  * wait_event (may be NULL); a host buffer may be reused once done_event (may
  * be NULL) has completed, or after wema_cuda_batch_sync. */
 int wema_cuda_batch_tick_host(wema_cuda_batch *b, const int *ids, const void *const *h_in_u8,

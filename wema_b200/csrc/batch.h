@@ -104,9 +104,9 @@ public:
     long long ticks_timed = 0;
 
     // host-frame ticks: two device staging sets (frames in and out) per stream,
-    // copies on their own streams, so tick i's inputs come in while tick i-1
-    // runs and its outputs go out while tick i+1 runs (async_io.c's double
-    // buffering, on copy engines instead of threads)
+    // copies on their own streams, so tick i's outputs go out while tick i+1's
+    // inputs come in and it runs (async_io.c's double buffering, on copy
+    // engines instead of threads)
     struct HostSet {
         cudaEvent_t h2d = nullptr, tick = nullptr, d2h = nullptr;
         bool used = false;
