@@ -365,9 +365,9 @@ def bench_mixed(a, rank, world, local):
 
     # ---- e2e through the host-frame tick (wema_cuda_batch_tick_host): every
     # tick's frames are copied in from pinned host memory and its outputs back,
-    # double-buffered inside the library (tick i's inputs come in while tick
-    # i-1 runs, its outputs go out while tick i+1 runs).  The host link
-    # carries 2 x 233 MB per tick and bounds this.
+    # double-buffered inside the library (tick i's outputs go out while tick
+    # i+1's inputs come in and it runs).  The host link carries 2 x 233 MB per
+    # tick and bounds this.
     h_out = [[torch.empty_like(host[k][0]).pin_memory() for k in range(n)] for _ in range(2)]
     barrier()
     E = max(4, a.steps // 4)
