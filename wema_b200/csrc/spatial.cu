@@ -10,9 +10,10 @@
 // One CTA produces a TS x TS output tile.  The guided filter's two rounds of
 // radius-4 box means need an 8-pixel halo; every box mean is the clipped
 // window's sum divided by the clipped count, rows first then columns (the
-// reference's definition), computed here by direct 9-term sums in shared
-// memory rather than by the reference's FP32 running prefix sums - the two
-// differ in the last bits only, which the u8 output absorbs (<= 1 LSB).
+// reference's definition), computed here by window sums sliding along short
+// segments in shared memory rather than by the reference's FP32 running
+// prefix sums - the two differ in the last bits only, which the u8 output
+// absorbs (<= 1 LSB).
 #include "common.cuh"
 #include "kernels.h"
 #include "multi.cuh"
