@@ -314,6 +314,7 @@ def bench_mixed(a, rank, world, local):
     dist = replicas.init("nccl")                 # replicas: every rank its own 48 streams
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    _, tune_report = wc.autotune(local)          # the filter's positions per thread, this device
     mix = S.mixed_streams(seed=7 + rank)
     K = 4                                             # unique frames per stream, cycled
     host, d_in, d_out = [], [], []
@@ -476,7 +477,7 @@ def bench_mixed(a, rank, world, local):
         "e2e": {"value": round(e2e, 2), "unit": METRIC, "h2d_bytes_per_step": 3 * sum(pix),
                 "d2h_bytes_per_step": 3 * sum(pix)},
         "gpu_launches": launches, "frames_timed": frames_timed,
-        "roofline": roofline, "pipeline": pipeline,
+        "roofline": roofline, "pipeline": pipeline, "autotune": tune_report,
         "clocks": clocks,
     }
     if rank == 0 and not a.no_cpu_baseline:

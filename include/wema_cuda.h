@@ -268,6 +268,18 @@ int wema_cuda_server_drain(wema_cuda_server *srv, int timeout_ms);
 /* reset != 0 starts a new measurement window after filling *out. */
 int wema_cuda_server_stats(wema_cuda_server *srv, int reset, wema_cuda_serve_stats *out);
 
+/* Autotuner (no counterpart in the reference): times the temporal filter's
+ * step at 2, 4 and 8 coefficient positions per thread on this device
+ * (allocating ~200 MB for the trial and freeing it) and keeps the fastest for
+ * every later launch on the device (4, the default, unless another is more
+ * than 3% faster); returns it (or -1), and writes the timings
+ * to `report` (may be NULL).  Results do not depend on the choice - each
+ * position's arithmetic is the same - only speed does.  Until a call, 4.
+ * set / get fix or read the choice directly (2, 4 or 8). */
+int wema_cuda_autotune(int device, char *report, size_t cap);
+int wema_cuda_set_iir_positions(int device, int positions);
+int wema_cuda_get_iir_positions(int device);
+
 /* Message of the last failure on this thread ("" if none). */
 const char *wema_cuda_last_error(void);
 

@@ -25,10 +25,14 @@
 
 #include <string.h>
 
+#include <atomic>
+
 namespace wema {
 
 constexpr int IIR_THREADS = 256;
-constexpr int IIR_U = 4;   // positions a thread has in flight (all loads before any use)
+// Positions a thread has in flight (all loads before any use): 2, 4 or 8,
+// picked per device by iir_autotune (4 until then).
+constexpr int IIR_U = 4;
 
 struct IirDev {
     IirParams p;
@@ -109,19 +113,20 @@ __device__ __forceinline__ void iir_preseed_body(const IirDev& a, int block, int
     }
 }
 
-// A thread takes positions u, u + B, u + 2B, u + 3B (B = the task's threads)
-// per pass, so a warp's accesses stay coalesced and four are in flight.
+// A thread takes positions u, u + B, ..., u + (U-1)B (B = the task's threads)
+// per pass, so a warp's accesses stay coalesced and U are in flight.
+template <int U>
 __device__ __forceinline__ void iir_body64(const IirDev& a, int block, int nblocks) {
     const long long pu = a.p.uoff[a.p.levels];
     const long long B = (long long)nblocks * IIR_THREADS;
     const float* __restrict__ coef = a.coef;
     double2* __restrict__ state = static_cast<double2*>(a.state);
     float* __restrict__ dout = a.delta_out;
-    for (long long u0 = block * (long long)IIR_THREADS + threadIdx.x; u0 < pu; u0 += IIR_U * B) {
-        float x[IIR_U];
-        double2 hp[IIR_U], lp[IIR_U];
+    for (long long u0 = block * (long long)IIR_THREADS + threadIdx.x; u0 < pu; u0 += U * B) {
+        float x[U];
+        double2 hp[U], lp[U];
 #pragma unroll
-        for (int j = 0; j < IIR_U; j++) {
+        for (int j = 0; j < U; j++) {
             const long long u = u0 + j * B;
             if (u < pu) {
                 x[j] = __ldg(coef + u);
@@ -130,7 +135,7 @@ __device__ __forceinline__ void iir_body64(const IirDev& a, int block, int nbloc
             }
         }
 #pragma unroll
-        for (int j = 0; j < IIR_U; j++) {
+        for (int j = 0; j < U; j++) {
             const long long u = u0 + j * B;
             if (u < pu) {
                 dout[u] = cascade64(a.p.c, hp[j], lp[j], x[j]);
@@ -141,9 +146,10 @@ __device__ __forceinline__ void iir_body64(const IirDev& a, int block, int nbloc
     }
 }
 
+template <int U>
 __device__ __forceinline__ void iir_body(const IirDev& a, int block, int nblocks) {
     if (a.fp64) {
-        iir_body64(a, block, nblocks);
+        iir_body64<(U > 4 ? 4 : U)>(a, block, nblocks);   // double state: at most 4 in registers
         return;
     }
     const long long pu = a.p.uoff[a.p.levels];
@@ -151,11 +157,11 @@ __device__ __forceinline__ void iir_body(const IirDev& a, int block, int nblocks
     const float* __restrict__ coef = a.coef;
     float4* __restrict__ state = static_cast<float4*>(a.state);
     float* __restrict__ dout = a.delta_out;
-    for (long long u0 = block * (long long)IIR_THREADS + threadIdx.x; u0 < pu; u0 += IIR_U * B) {
-        float x[IIR_U];
-        float4 st[IIR_U];
+    for (long long u0 = block * (long long)IIR_THREADS + threadIdx.x; u0 < pu; u0 += U * B) {
+        float x[U];
+        float4 st[U];
 #pragma unroll
-        for (int j = 0; j < IIR_U; j++) {
+        for (int j = 0; j < U; j++) {
             const long long u = u0 + j * B;
             if (u < pu) {
                 x[j] = __ldg(coef + u);
@@ -163,7 +169,7 @@ __device__ __forceinline__ void iir_body(const IirDev& a, int block, int nblocks
             }
         }
 #pragma unroll
-        for (int j = 0; j < IIR_U; j++) {
+        for (int j = 0; j < U; j++) {
             const long long u = u0 + j * B;
             if (u < pu) {
                 bool tail;
@@ -178,15 +184,45 @@ __device__ __forceinline__ void iir_body(const IirDev& a, int block, int nblocks
 __global__ void __launch_bounds__(IIR_THREADS) k_iir_preseed(IirDev a) {
     iir_preseed_body(a, blockIdx.x, gridDim.x);
 }
-// (4 CTAs per SM: 64 registers, 32 warps to keep the loads in flight)
-__global__ void __launch_bounds__(IIR_THREADS, 4) k_iir(IirDev a) { iir_body(a, blockIdx.x, gridDim.x); }
+// (U <= 4: 4 CTAs per SM, 64 registers, 32 warps keep the loads in flight;
+// U = 8: 2 CTAs per SM, 16 warps with twice the loads each)
+template <int U>
+__global__ void __launch_bounds__(IIR_THREADS, U <= 4 ? 4 : 2) k_iir(IirDev a) {
+    iir_body<U>(a, blockIdx.x, gridDim.x);
+}
 // batched: task = one (stream, channel); the task's grid x is its block count
-__global__ void __launch_bounds__(IIR_THREADS, 4)
+template <int U>
+__global__ void __launch_bounds__(IIR_THREADS, U <= 4 ? 4 : 2)
     k_iir_multi(const IirDev* __restrict__ as, const int* __restrict__ map, int preseed) {
     const TaskBlock t = task_block(map, blockIdx.x);
     const int nb = map[map[0] + 2 + t.task];
     if (preseed) iir_preseed_body(as[t.task], t.x, nb);
-    else iir_body(as[t.task], t.x, nb);
+    else iir_body<U>(as[t.task], t.x, nb);
+}
+
+// ---- positions per thread, per device
+static std::atomic<int> g_positions[64];
+
+static int device_now() {
+    int d = 0;
+    cudaGetDevice(&d);
+    return d;
+}
+
+int iir_positions(int dev) {
+    const int u = (dev >= 0 && dev < 64) ? g_positions[dev].load() : 0;
+    return u ? u : IIR_U;
+}
+
+bool iir_set_positions(int dev, int u) {
+    if (dev < 0 || dev >= 64 || (u != 2 && u != 4 && u != 8)) return false;
+    g_positions[dev].store(u);
+    return true;
+}
+
+template <int U>
+static void launch_k_iir(int blocks, const IirDev& a, cudaStream_t st) {
+    k_iir<U><<<blocks, IIR_THREADS, 0, st>>>(a);
 }
 
 __global__ void __launch_bounds__(IIR_THREADS) k_amplify(IirDev a) {
@@ -202,10 +238,11 @@ __global__ void __launch_bounds__(IIR_THREADS) k_amplify(IirDev a) {
     }
 }
 
-static int grid_for(long long n) {
-    long long b = (n + IIR_THREADS * IIR_U - 1) / (IIR_THREADS * IIR_U);
+static int grid_for_u(long long n, int u) {
+    long long b = (n + (long long)IIR_THREADS * u - 1) / ((long long)IIR_THREADS * u);
     return (int)(b < 148 * 16 ? (b > 0 ? b : 1) : 148 * 16);
 }
+static int grid_for(long long n) { return grid_for_u(n, iir_positions(device_now())); }
 
 cudaError_t launch_iir_preseed(const IirParams& p, const float* coef, void* state, int fp64, int warmup,
                                cudaStream_t st) {
@@ -227,7 +264,11 @@ cudaError_t launch_iir(const IirParams& p, const float* coef, void* state, int f
     a.state = state;
     a.fp64 = fp64;
     a.delta_out = delta;
-    k_iir<<<grid_for(p.uoff[p.levels]), IIR_THREADS, 0, st>>>(a);
+    const int u = iir_positions(device_now());
+    const int g = grid_for_u(p.uoff[p.levels], u);
+    if (u == 2) launch_k_iir<2>(g, a, st);
+    else if (u == 8) launch_k_iir<8>(g, a, st);
+    else launch_k_iir<4>(g, a, st);
     return cudaGetLastError();
 }
 
@@ -263,8 +304,80 @@ unsigned iir_args_fill(void* dst, const IirParams& p, const float* coef, void* s
 cudaError_t launch_iir_multi(const void* d_args, const int* d_map, unsigned blocks, int preseed,
                              cudaStream_t st) {
     if (blocks == 0) return cudaSuccess;
-    k_iir_multi<<<blocks, IIR_THREADS, 0, st>>>(static_cast<const IirDev*>(d_args), d_map, preseed);
+    const IirDev* as = static_cast<const IirDev*>(d_args);
+    const int u = iir_positions(device_now());
+    if (u == 2) k_iir_multi<2><<<blocks, IIR_THREADS, 0, st>>>(as, d_map, preseed);
+    else if (u == 8) k_iir_multi<8><<<blocks, IIR_THREADS, 0, st>>>(as, d_map, preseed);
+    else k_iir_multi<4><<<blocks, IIR_THREADS, 0, st>>>(as, d_map, preseed);
     return cudaGetLastError();
+}
+
+// ---- the autotuner: times the filter step at 2, 4 and 8 positions per thread
+// on a synthetic 2^23-position plane (a 3840x2160 frame's detail count) and
+// keeps the fastest for this device - the default 4 unless another is faster
+// by more than 3% (the trial runs alone; in a tick the filter shares the GPU
+// with the threshold, so small margins are not worth a change).  The
+// arithmetic per position does not depend on the choice, so results are
+// bit-identical whatever it picks.
+cudaError_t iir_autotune(int dev, float ms[3], int* chosen) {
+    cudaError_t e = cudaSetDevice(dev);
+    if (e != cudaSuccess) return e;
+    const long long n = 1LL << 23;
+    float *coef = nullptr, *delta = nullptr;
+    float4* state = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaStream_t st = nullptr;
+    auto done = [&](cudaError_t r) {
+        if (coef) cudaFree(coef);
+        if (delta) cudaFree(delta);
+        if (state) cudaFree(state);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (st) cudaStreamDestroy(st);
+        return r;
+    };
+    if ((e = cudaMalloc(&coef, n * sizeof(float))) != cudaSuccess) return done(e);
+    if ((e = cudaMalloc(&delta, n * sizeof(float))) != cudaSuccess) return done(e);
+    if ((e = cudaMalloc(&state, n * sizeof(float4))) != cudaSuccess) return done(e);
+    if ((e = cudaMemset(coef, 0, n * sizeof(float))) != cudaSuccess) return done(e);
+    if ((e = cudaMemset(state, 0, n * sizeof(float4))) != cudaSuccess) return done(e);
+    if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) return done(e);
+    if ((e = cudaEventCreate(&e0)) != cudaSuccess || (e = cudaEventCreate(&e1)) != cudaSuccess) return done(e);
+    IirDev a{};
+    a.p.levels = 1;
+    a.p.uoff[1] = n;
+    a.p.n[0] = n / 3;
+    a.p.off6[1] = 2 * n;
+    a.p.simd_end = (2 * n) & ~15LL;
+    a.coef = coef;
+    a.state = state;
+    a.delta_out = delta;
+    const int us[3] = {2, 4, 8};
+    for (int k = 0; k < 3; k++) {
+        const int u = us[k], g = grid_for_u(n, u);
+        for (int rep = 0; rep < 6; rep++) {          // one warm-up, five timed
+            if (rep == 1 && (e = cudaEventRecord(e0, st)) != cudaSuccess) return done(e);
+            if (u == 2) launch_k_iir<2>(g, a, st);
+            else if (u == 8) launch_k_iir<8>(g, a, st);
+            else launch_k_iir<4>(g, a, st);
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return done(e);
+        if ((e = cudaEventRecord(e1, st)) != cudaSuccess) return done(e);
+        if ((e = cudaEventSynchronize(e1)) != cudaSuccess) return done(e);
+        float t = 0.f;
+        if ((e = cudaEventElapsedTime(&t, e0, e1)) != cudaSuccess) return done(e);
+        ms[k] = t / 5.f;
+    }
+    int best = IIR_U;
+    float best_ms = ms[1];
+    for (int k = 0; k < 3; k++)
+        if (ms[k] < 0.97f * best_ms) {
+            best = us[k];
+            best_ms = ms[k];
+        }
+    iir_set_positions(dev, best);
+    *chosen = best;
+    return done(cudaSuccess);
 }
 
 }  // namespace wema

@@ -142,6 +142,11 @@ cudaError_t launch_threshold_multi(int stage, const void* d_args, const int* d_m
 size_t iir_args_bytes();
 unsigned iir_args_fill(void* dst, const IirParams& p, const float* coef, void* state, int fp64, float* delta,
                        int warmup);   // returns the task's block count
+// positions per thread of the filter step on a device (2, 4 or 8; 4 until tuned)
+int iir_positions(int dev);
+bool iir_set_positions(int dev, int positions);
+// times the filter at 2 / 4 / 8 positions per thread (ms[3]) and keeps the fastest
+cudaError_t iir_autotune(int dev, float ms[3], int* chosen);
 cudaError_t launch_iir_multi(const void* d_args, const int* d_map, unsigned blocks, int preseed,
                              cudaStream_t st);
 unsigned transfer_grid(const TransferParams& p, unsigned& gx, unsigned& gy);

@@ -667,6 +667,29 @@ WEMA_API int wema_cuda_session_sync(wema_cuda_session* s) {
     return s->s.sync_all() ? 0 : -1;
 }
 
+WEMA_API int wema_cuda_autotune(int device, char* report, size_t cap) {
+    clear_error();
+    if (!ensure_device(device)) return -1;
+    float ms[3] = {0.f, 0.f, 0.f};
+    int chosen = 0;
+    if (!cuda_ok(iir_autotune(device, ms, &chosen), "autotune")) return -1;
+    if (report && cap)
+        snprintf(report, cap, "iir positions per thread: 2 %.4f ms, 4 %.4f ms, 8 %.4f ms -> %d", ms[0], ms[1],
+                 ms[2], chosen);
+    return chosen;
+}
+
+WEMA_API int wema_cuda_set_iir_positions(int device, int positions) {
+    clear_error();
+    if (!iir_set_positions(device, positions)) { set_error("positions per thread must be 2, 4 or 8"); return -1; }
+    return 0;
+}
+
+WEMA_API int wema_cuda_get_iir_positions(int device) {
+    clear_error();
+    return iir_positions(device);
+}
+
 WEMA_API size_t wema_cuda_session_snapshot_bytes(wema_cuda_session* s) {
     clear_error();
     if (!s) { set_error("null session"); return 0; }

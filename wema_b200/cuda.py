@@ -91,6 +91,9 @@ def lib() -> C.CDLL:
         L.wema_cuda_batch_remove.argtypes = [vp, i]
         L.wema_cuda_batch_tick.argtypes = [vp, C.POINTER(i), C.POINTER(vp), C.POINTER(vp), i, vp, vp]
         L.wema_cuda_batch_sync.argtypes = [vp]
+        L.wema_cuda_autotune.argtypes = [i, C.c_char_p, sz]
+        L.wema_cuda_set_iir_positions.argtypes = [i, i]
+        L.wema_cuda_get_iir_positions.argtypes = [i]
         L.wema_cuda_batch_tick_host.argtypes = [vp, C.POINTER(i), C.POINTER(vp), C.POINTER(vp), i, vp, vp]
         L.wema_cuda_session_snapshot_bytes.argtypes = [vp]
         L.wema_cuda_session_snapshot_bytes.restype = sz
@@ -424,3 +427,21 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def autotune(device=0):
+    """Times the filter step at 2 / 4 / 8 positions per thread and keeps the
+    fastest for the device -> (positions, report)."""
+    buf = C.create_string_buffer(256)
+    u = lib().wema_cuda_autotune(int(device), buf, 256)
+    if u < 0:
+        raise RuntimeError(f"autotune failed: {last_error()}")
+    return u, buf.value.decode()
+
+
+def set_iir_positions(device, positions):
+    _check(lib().wema_cuda_set_iir_positions(int(device), int(positions)), "set_iir_positions")
+
+
+def iir_positions(device=0) -> int:
+    return lib().wema_cuda_get_iir_positions(int(device))
