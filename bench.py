@@ -72,14 +72,17 @@ METRIC = "Mpix-frames/s"
 # capture each, keyed by (workload, stage); stages not captured report null.
 # profiles/k_thr_monoids_plain_fullhd_color.txt, k_thr_walk_..., k_dwt_inv_level0_...
 # and k_dwt_fwd_level0_... hold the captures and the commands that made them.
+# DRAM bytes (read + written) per launch from ncu captures (profiles/).  The
+# batched kernels were captured on a tick of 16 streams (8 x 640x480 +
+# 8 x 1920x1080, 19.05 Mpix) and are scaled by pixels to the 77.72 Mpix of the
+# 48-stream tick; the threshold of the plain workload is monoids + walk.
+_MIX = 77.722 / 19.046
 TRAFFIC_NCU = {
-    # k_guided_transfer_multi: 133.39 MB read + 37.21 MB written for a tick of
-    # 16 streams (8 x 640x480 + 8 x 1920x1080, 19.05 Mpix), scaled by pixels
-    # to the 77.72 Mpix of the 48-stream tick
-    ("mixed_streams_48", "luma_transfer"): int((133387008 + 37206784) * 77.722 / 19.046),
+    ("mixed_streams_48", "luma_transfer"): int((133387008 + 37206784) * _MIX),
+    ("mixed_streams_48", "fwd_dwt_level0"): int((57178624 + 28476672) * _MIX),
+    ("mixed_streams_48", "inv_dwt_level0"): int((133352960 + 47001344) * _MIX),
+    ("mixed_streams_48", "temporal_amplify"): int((379583232 + 321814528) * _MIX),
     ("plain_fullhd_color", "threshold"): 25081088 + 2323456,
-    ("plain_fullhd_color", "inv_dwt_level0"): 43630080 + 278784,
-    ("plain_fullhd_color", "fwd_dwt_level0"): 6266624 + 7168,
 }
 
 
