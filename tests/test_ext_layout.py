@@ -1,5 +1,7 @@
 """The extension structs of include/wema_cuda.h (config, session status,
-serve stats) have the same layout in C and in the Python binding."""
+serve stats) have the same layout in C and in the Python binding, and a C11
+caller of the extension API (tests/c/serve_client.c) compiles with -Wall
+-Werror and links against libwema_cuda."""
 import ctypes as C
 import subprocess
 
@@ -43,3 +45,18 @@ def test_layout_matches(c_layout, name):
     assert c_layout[(name, "size")] == C.sizeof(py)
     for f, _ in py._fields_:
         assert c_layout[(name, f)] == getattr(py, f).offset, f
+
+
+def _client(tmp_path):
+    from wema_b200 import _build
+    lib = _build.build_cuda()
+    exe = tmp_path / "serve_client"
+    subprocess.run(["gcc", "-std=c11", "-Wall", "-Werror", "-I", INCLUDE,
+                    __import__("os").path.join(__import__("os").path.dirname(__file__), "c", "serve_client.c"),
+                    "-o", str(exe), "-L", __import__("os").path.dirname(lib), "-lwema_cuda",
+                    "-Wl,-rpath," + __import__("os").path.dirname(lib)], check=True)
+    return exe
+
+
+def test_c_client_builds(tmp_path):
+    assert _client(tmp_path).exists()
