@@ -1,7 +1,7 @@
 """The extension structs of include/wema_cuda.h (config, session status,
 serve stats) have the same layout in C and in the Python binding, and a C11
 caller of the extension API (tests/c/serve_client.c) compiles with -Wall
--Werror and links against libwema_cuda."""
+-Werror and links against libwema_cuda; on a GPU it runs and checks its frames."""
 import ctypes as C
 import subprocess
 
@@ -60,3 +60,9 @@ def _client(tmp_path):
 
 def test_c_client_builds(tmp_path):
     assert _client(tmp_path).exists()
+
+
+@pytest.mark.gpu
+def test_c_client_runs(tmp_path):
+    r = subprocess.run([str(_client(tmp_path))], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "OK" in r.stdout, r.stdout + r.stderr
