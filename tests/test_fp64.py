@@ -63,3 +63,19 @@ def test_stream_fp64_against_fp32(oracle):
         # to the delta itself
         assert np.linalg.norm(d32 - d64) <= 1e-5 * np.linalg.norm(s64.last["coef"]), f"frame {t} delta"
         assert np.abs(out32.astype(np.float64) - out64).max() * 255.0 < 0.05, f"frame {t} output"
+
+
+@pytest.mark.parametrize("w,h", [(64, 48), (37, 29), (9, 9)])
+def test_box_and_guided_fp64_against_fp32(oracle, w, h):
+    """The clipped-window box mean and the guided filter (r 4, eps 0.01) agree
+    with the FP32 restatement to FP32 rounding (its running prefix sums lose a
+    few ulp of the row total)."""
+    rng = np.random.default_rng(w * h)
+    I = rng.random((h, w))
+    p = 0.05 * rng.standard_normal((h, w))
+    b64 = fp64.box(I)
+    b32 = oracle.box(I.astype(np.float32)).astype(np.float64)
+    assert np.abs(b64 - b32).max() < 1e-5
+    q64 = fp64.guided(I, p)
+    q32 = oracle.guided(I.astype(np.float32), p.astype(np.float32)).astype(np.float64)
+    assert np.abs(q64 - q32).max() < 1e-4
