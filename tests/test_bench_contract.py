@@ -1,0 +1,37 @@
+"""bench.py's reference arm (the reference's own CPU path, host only) prints
+one JSON line with the contract's keys, on the default workload's config."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def run(*args, timeout=600):
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), *args], capture_output=True,
+                       text=True, timeout=timeout, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    return json.loads(lines[0])
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref_harness.so")),
+                    reason="the reference library is built where its sources are (oracle/_ref)")
+def test_reference_arm_line():
+    line = run("--impl", "reference", "--steps", "3", "--warmup", "3")
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "higher_is_better", "scaling",
+              "vs_baseline", "dtype", "data", "config", "impl", "cpu_baseline", "e2e"):
+        assert k in line, k
+    assert line["impl"] == "reference" and line["config"]["workload"] == "mixed_streams_48"
+    assert line["metric"] == "Mpix-frames/s" and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] == "reference" and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]
+
+
+def test_served_reference_arm_is_unavailable():
+    line = run("--impl", "reference", "--workload", "served_poisson")
+    assert line["impl"] == "reference" and "unavailable" in line
