@@ -181,3 +181,44 @@ def test_ref_gray_to_rgb(oracle, reference):
         a = oracle.gray_to_rgb(g, rgb, edge)
         b = reference.gray_to_rgb(g, rgb, edge)
         assert np.abs(a - b).max() <= 4e-7
+
+
+@pytest.mark.parametrize("bilateral", [False, True])
+def test_ref_stream_window(oracle, reference, bilateral):
+    """Window mode (--haar, optionally --bilateral-filter): passthrough until the
+    ring is full, then deltas within relative L2 1e-5 (the reference's vector
+    reductions and expf order the sums differently) and output within 1 LSB."""
+    w, h, F, ws = 96, 80, 12, 8
+    u8 = SynthVideo(SynthSpec(w, h, 30.0, 14, [1.2], [0.4], 14.0, 2.0)).frames(0, F)
+    rgb = oracle.u8_to_float(u8)
+    cfg = dict(width=w, height=h, fps=30.0, amp=60.0, f_low=0.5, f_high=3.0, window=ws,
+               use_iir=False, bilateral=bilateral)
+    so, sr = oracle.stream(**cfg), reference.stream(**cfg)
+    N = oracle.positions(w, h)
+    for t in range(F):
+        a, b = so.process(rgb[t]), sr.process(rgb[t])
+        if t < ws - 1:
+            assert np.array_equal(a, rgb[t]) and np.array_equal(b, rgb[t])
+            continue
+        do, dr = so.get(3, N).astype(np.float64), sr.get(3, N).astype(np.float64)
+        assert np.linalg.norm(do - dr) <= 1e-5 * np.linalg.norm(dr) + 1e-12, f"frame {t}"
+        q = np.abs(oracle.float_to_u8(a).astype(int) - oracle.float_to_u8(b).astype(int))
+        assert q.max() <= 1, f"frame {t}"
+
+
+def test_ref_stream_fullhd_colour(oracle, reference):
+    """1920x1080 colour (the level-4 input is 240x135, odd): every 6-slot
+    coefficient plane (stale entries included), the deltas, the amplified
+    planes and the float output bit-exact for two frames."""
+    w, h, F = 1920, 1080, 2
+    from wema_b200.synth import plain_fullhd
+    u8 = SynthVideo(plain_fullhd(seed=2)).frames(0, F)
+    rgb = oracle.u8_to_float(u8)
+    cfg = dict(width=w, height=h, fps=30.0, amp=120.0, f_low=0.5, f_high=3.0, color=True)
+    so, sr = oracle.stream(**cfg), reference.stream(**cfg)
+    N = oracle.positions(w, h)
+    for t in range(F):
+        a, b = so.process(rgb[t]), sr.process(rgb[t])
+        for k in (2, 3, 4, 7, 8, 9, 10):
+            assert np.array_equal(so.get(k, N).view(np.uint32), sr.get(k, N).view(np.uint32)), (t, k)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), f"frame {t}"
