@@ -222,3 +222,19 @@ def test_ref_stream_fullhd_colour(oracle, reference):
         for k in (2, 3, 4, 7, 8, 9, 10):
             assert np.array_equal(so.get(k, N).view(np.uint32), sr.get(k, N).view(np.uint32)), (t, k)
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), f"frame {t}"
+
+
+@pytest.mark.parametrize("w,h", [(160, 128), (100, 64)])
+def test_ref_batch_route(oracle, reference, w, h):
+    """wema_batch_process (the CLI's default IIR luma route: batch threshold
+    form, always the guided filter) against the restatement's batch route,
+    16 frames in batches of 8: u8 within 1 LSB."""
+    F = 16
+    u8 = SynthVideo(SynthSpec(w, h, 30.0, 15, [1.1], [0.4], 14.0, 2.0)).frames(0, F)
+    rgb = oracle.u8_to_float(u8)
+    cfg = dict(width=w, height=h, fps=30.0, amp=80.0, f_low=0.5, f_high=3.0)
+    a = oracle.float_to_u8(oracle.stream(**cfg).batch(rgb))
+    sr = reference.stream(batch_size=8, threads=1, **cfg)
+    b = np.concatenate([oracle.float_to_u8(sr.batch(rgb[i:i + 8])) for i in range(0, F, 8)])
+    d = np.abs(a.astype(int) - b.astype(int))
+    assert d.max() <= 1
