@@ -70,8 +70,8 @@ METRIC = "Mpix-frames/s"
 
 # DRAM bytes (read + write) per frame of a stage's kernels from one ncu
 # capture each, keyed by (workload, stage); stages not captured report null.
-# profiles/k_thr_monoids_plain_fullhd_color.txt, k_thr_walk_..., k_dwt_inv_level0_...
-# and k_dwt_fwd_level0_... hold the captures and the commands that made them.
+# profiles/k_thr_monoids_plain_fullhd_color.txt, k_thr_walk_plain_fullhd_color.txt
+# and batched_kernels_16streams.md hold the captures and the commands that made them.
 # DRAM bytes (read + written) per launch from ncu captures (profiles/).  The
 # batched kernels were captured on a tick of 16 streams (8 x 640x480 +
 # 8 x 1920x1080, 19.05 Mpix) and are scaled by pixels to the 77.72 Mpix of the

@@ -188,16 +188,32 @@ static void lift_inv(float *v, int n, float *t) {
     if (ne > no) v[2 * no] = e[no];
 }
 
-static void lift_rows(float *img, int w, int h, float *t, int inverse) {
-    for (int y = 0; y < h; y++)
-        (inverse ? lift_inv : lift_fwd)(img + (long)y * w, w, t);
+/* Rows and columns are independent lines, so they are split over OpenMP
+ * threads; every line's arithmetic is the same whatever the thread count. */
+static void lift_rows(float *img, int w, int h, int inverse) {
+    #pragma omp parallel if ((long)w * h > 65536)
+    {
+        float *t = malloc((w + 1) * sizeof(float));
+        #pragma omp for schedule(static)
+        for (int y = 0; y < h; y++)
+            (inverse ? lift_inv : lift_fwd)(img + (long)y * w, w, t);
+        free(t);
+    }
 }
 
-static void lift_cols(float *img, int w, int h, float *t, float *col, int inverse) {
-    for (int x = 0; x < w; x++) {
-        for (int y = 0; y < h; y++) col[y] = img[(long)y * w + x];
-        (inverse ? lift_inv : lift_fwd)(col, h, t);
-        for (int y = 0; y < h; y++) img[(long)y * w + x] = col[y];
+static void lift_cols(float *img, int w, int h, int inverse) {
+    #pragma omp parallel if ((long)w * h > 65536)
+    {
+        float *t = malloc((h + 1) * sizeof(float));
+        float *col = malloc((h + 1) * sizeof(float));
+        #pragma omp for schedule(static)
+        for (int x = 0; x < w; x++) {
+            for (int y = 0; y < h; y++) col[y] = img[(long)y * w + x];
+            (inverse ? lift_inv : lift_fwd)(col, h, t);
+            for (int y = 0; y < h; y++) img[(long)y * w + x] = col[y];
+        }
+        free(t);
+        free(col);
     }
 }
 
@@ -212,16 +228,13 @@ static void lift_cols(float *img, int w, int h, float *t, float *col, int invers
 int orc_dwt_forward(const float *img, int w, int h, float *flat6, float *lowpass) {
     long P = (long)w * h;
     int L = orc_levels(w, h);
-    int md = w > h ? w : h;
     float *work = malloc(P * sizeof(float));
     float *ll = malloc(P * sizeof(float));
     float *lh = calloc(P, sizeof(float));
     float *hl = calloc(P, sizeof(float));
     float *hh = calloc(P, sizeof(float));
-    float *t = malloc((md + 1) * sizeof(float));
-    float *col = malloc((md + 1) * sizeof(float));
-    if (!work || !ll || !lh || !hl || !hh || !t || !col) {
-        free(work); free(ll); free(lh); free(hl); free(hh); free(t); free(col);
+    if (!work || !ll || !lh || !hl || !hh) {
+        free(work); free(ll); free(lh); free(hl); free(hh);
         return -1;
     }
     memcpy(work, img, P * sizeof(float));
@@ -230,8 +243,8 @@ int orc_dwt_forward(const float *img, int w, int h, float *flat6, float *lowpass
     for (int l = 0; l < L; l++) {
         int sw = (cw + 1) / 2, sh = (ch + 1) / 2;
         int nhx = cw - sw, nhy = ch - sh;
-        lift_rows(work, cw, ch, t, 0);
-        lift_cols(work, cw, ch, t, col, 0);
+        lift_rows(work, cw, ch, 0);
+        lift_cols(work, cw, ch, 0);
         for (int y = 0; y < sh; y++)
             for (int x = 0; x < sw; x++) {
                 long k = (long)y * sw + x;
@@ -253,7 +266,7 @@ int orc_dwt_forward(const float *img, int w, int h, float *flat6, float *lowpass
         ch = sh;
     }
     memcpy(lowpass, work, (long)cw * ch * sizeof(float));
-    free(work); free(ll); free(lh); free(hl); free(hh); free(t); free(col);
+    free(work); free(ll); free(lh); free(hl); free(hh);
     return 0;
 }
 
@@ -269,12 +282,9 @@ int orc_dwt_inverse(const float *flat6, const float *lowpass, int w, int h, floa
     long pos = 0;
     for (int l = 0; l < L; l++) { off[l] = pos; pos += 6L * lw[l + 1] * lh[l + 1]; }
     long P = (long)w * h;
-    int md = w > h ? w : h;
     float *work = malloc(P * sizeof(float));
     float *out = malloc(P * sizeof(float));
-    float *t = malloc((md + 1) * sizeof(float));
-    float *col = malloc((md + 1) * sizeof(float));
-    if (!work || !out || !t || !col) { free(work); free(out); free(t); free(col); return -1; }
+    if (!work || !out) { free(work); free(out); return -1; }
     memcpy(work, lowpass, (long)lw[L] * lh[L] * sizeof(float));
     for (int l = L - 1; l >= 0; l--) {
         int ow = lw[l], oh = lh[l], sw = lw[l + 1], sh = lh[l + 1];
@@ -290,12 +300,12 @@ int orc_dwt_inverse(const float *flat6, const float *lowpass, int w, int h, floa
                 if (y < nhy) out[(long)(sh + y) * ow + x] = LH[k];
                 if (x < nhx && y < nhy) out[(long)(sh + y) * ow + sw + x] = HH[k];
             }
-        lift_cols(out, ow, oh, t, col, 1);
-        lift_rows(out, ow, oh, t, 1);
+        lift_cols(out, ow, oh, 1);
+        lift_rows(out, ow, oh, 1);
         memcpy(work, out, (long)ow * oh * sizeof(float));
     }
     memcpy(img, work, P * sizeof(float));
-    free(work); free(out); free(t); free(col);
+    free(work); free(out);
     return 0;
 }
 
@@ -350,12 +360,14 @@ static inline float biquad2(const float *c, float *st, float x, int tail) {
 
 void orc_iir_preseed(const float *c, int warmup, const float *x, long n, float *state4) {
     long simd = n & ~15L;                       /* iir_filter.c:376-471 */
+    #pragma omp parallel for schedule(static) if (n > 65536)
     for (long i = 0; i < n; i++)
         for (int it = 0; it < warmup; it++) biquad2(c, state4 + 4 * i, x[i], i >= simd);
 }
 
 void orc_iir_step(const float *c, const float *x, long n, float *state4, float *out) {
     long simd = n & ~15L;
+    #pragma omp parallel for schedule(static) if (n > 65536)
     for (long i = 0; i < n; i++) out[i] = biquad2(c, state4 + 4 * i, x[i], i >= simd);
 }
 
@@ -432,26 +444,31 @@ void orc_box(const float *in, float *out, int w, int h, int r) {
     long P = (long)w * h;
     int md = w > h ? w : h;
     float *tmp = malloc(P * sizeof(float));
-    float *pre = malloc((md + 1) * sizeof(float));
-    for (int y = 0; y < h; y++) {
-        const float *row = in + (long)y * w;
-        pre[0] = 0.0f;
-        for (int x = 0; x < w; x++) pre[x + 1] = pre[x] + row[x];
-        for (int x = 0; x < w; x++) {
-            int a = x - r > 0 ? x - r : 0, b = x + r + 1 < w ? x + r + 1 : w;
-            tmp[(long)y * w + x] = (pre[b] - pre[a]) / (float)(b - a);
-        }
-    }
-    for (int x = 0; x < w; x++) {
-        pre[0] = 0.0f;
-        for (int y = 0; y < h; y++) pre[y + 1] = pre[y] + tmp[(long)y * w + x];
+    #pragma omp parallel if (P > 65536)
+    {
+        float *pre = malloc((md + 1) * sizeof(float));
+        #pragma omp for schedule(static)
         for (int y = 0; y < h; y++) {
-            int a = y - r > 0 ? y - r : 0, b = y + r + 1 < h ? y + r + 1 : h;
-            out[(long)y * w + x] = (pre[b] - pre[a]) / (float)(b - a);
+            const float *row = in + (long)y * w;
+            pre[0] = 0.0f;
+            for (int x = 0; x < w; x++) pre[x + 1] = pre[x] + row[x];
+            for (int x = 0; x < w; x++) {
+                int a = x - r > 0 ? x - r : 0, b = x + r + 1 < w ? x + r + 1 : w;
+                tmp[(long)y * w + x] = (pre[b] - pre[a]) / (float)(b - a);
+            }
         }
+        #pragma omp for schedule(static)
+        for (int x = 0; x < w; x++) {
+            pre[0] = 0.0f;
+            for (int y = 0; y < h; y++) pre[y + 1] = pre[y] + tmp[(long)y * w + x];
+            for (int y = 0; y < h; y++) {
+                int a = y - r > 0 ? y - r : 0, b = y + r + 1 < h ? y + r + 1 : h;
+                out[(long)y * w + x] = (pre[b] - pre[a]) / (float)(b - a);
+            }
+        }
+        free(pre);
     }
     free(tmp);
-    free(pre);
 }
 
 /* guided filter, output = mean_a*I + mean_b (wema.c:173-230) with GCC's
@@ -546,8 +563,9 @@ void orc_window_apply(const float *ring, long n, int ws, int head, int bilateral
             tw[t] = expf(-(d * d) * inv2);
         }
     }
-    float raw[256], tmp[256];
+    #pragma omp parallel for schedule(static) if (n > 16384)
     for (long pos = 0; pos < n; pos++) {
+        float raw[256], tmp[256];
         const float *b = ring + pos * ws;
         float mean = 0.0f;
         for (int t = 0; t < ws; t++) {

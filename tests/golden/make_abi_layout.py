@@ -1,7 +1,10 @@
 """Records the reference headers' struct layouts (sizeof / offsetof) into
 tests/golden/abi_layout.json; tests/test_abi.py checks include/ against it.
 
-    python tests/golden/make_abi_layout.py   # needs the reference checkout
+    WEMA_REF_DIR=<reference checkout> python tests/golden/make_abi_layout.py
+
+The reference checkout defaults to a directory named `reference` beside this
+repository.
 """
 import json
 import os
@@ -10,7 +13,9 @@ import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(os.path.dirname(HERE), "c", "abi_layout.c")
-REF_INC = "/root/reference/src"
+REPO = os.path.dirname(os.path.dirname(HERE))
+REF_INC = os.path.join(os.environ.get("WEMA_REF_DIR",
+                                      os.path.join(os.path.dirname(REPO), "reference")), "src")
 
 with tempfile.TemporaryDirectory() as d:
     exe = os.path.join(d, "layout")

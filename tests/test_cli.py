@@ -62,7 +62,7 @@ def test_nyquist_clamp_rejects_empty_band(tmp_path):
     (["--batch", "1", "--no-edge-aware"], dict(edge_aware=False)),  # single-frame route, Gaussian
     (["--color"], dict(color=True)),
 ])
-def test_cli_equals_session(tmp_path, extra, cfg):
+def test_cli_equals_session(oracle, tmp_path, extra, cfg):
     import torch
     from wema_b200 import cuda as wc
     from wema_b200.synth import SynthSpec, SynthVideo
@@ -82,6 +82,10 @@ def test_cli_equals_session(tmp_path, extra, cfg):
         torch.cuda.synchronize()
         assert np.array_equal(o.cpu().numpy(), got[t]), f"frame {t}"
     s.close()
+    from oracle_frames import assert_close, oracle_u8
+    want = oracle_u8(oracle, u8, fps=30.0, amp=80.0, f_low=0.5, f_high=3.0, **cfg)
+    for t in range(F):
+        assert_close(got[t], want[t], cfg.get("color", False), f"CLI frame {t}")
 
 
 @pytest.mark.gpu

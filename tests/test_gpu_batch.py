@@ -6,6 +6,7 @@ also checked against the oracle (u8 within 1 LSB, colour bit-exact)."""
 import numpy as np
 import pytest
 
+from oracle_frames import assert_close, oracle_u8
 from wema_b200 import cuda as wc
 from wema_b200.synth import SynthSpec, SynthVideo
 
@@ -200,9 +201,9 @@ def test_batch_stage_timing(torch_cuda):
         assert np.array_equal(outs[False][t], outs[True][t])
 
 
-def test_batch_tick_host_equals_device(torch_cuda):
+def test_batch_tick_host_equals_device(oracle, torch_cuda):
     """Host-frame ticks (pinned and pageable buffers, double-buffered staging)
-    give the device ticks' frames."""
+    give the device ticks' frames, and the oracle's."""
     torch = torch_cuda
     F = 5
     sel = [STREAMS[0], STREAMS[2], STREAMS[4]]
@@ -223,9 +224,11 @@ def test_batch_tick_host_equals_device(torch_cuda):
         hst.tick_host(ids_h, [x[t] for x in h_in], [x[t] for x in h_out])
     dev.sync()
     hst.sync()
-    for k in range(len(sel)):
+    for k, (w, h, cfg) in enumerate(sel):
+        want = oracle_u8(oracle, data[k], **cfg)
         for t in range(F):
             got = h_out[k][t].numpy() if hasattr(h_out[k][t], "numpy") else h_out[k][t]
             assert np.array_equal(got, ref[k][t].cpu().numpy()), f"stream {k} frame {t}"
+            assert_close(got, want[t], cfg.get("color", False), f"stream {k} frame {t}")
     dev.close()
     hst.close()

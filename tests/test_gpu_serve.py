@@ -7,6 +7,7 @@ import time
 import numpy as np
 import pytest
 
+from oracle_frames import assert_close, oracle_u8
 from wema_b200 import cuda as wc
 from wema_b200.synth import SynthSpec, SynthVideo
 
@@ -55,7 +56,7 @@ SESS = [
 ]
 
 
-def test_served_sessions_equal_alone(torch_cuda):
+def test_served_sessions_equal_alone(oracle, torch_cuda):
     """Sessions open at different times and submit at different rates (some
     several frames at once); the dispatcher is held on alternate rounds so
     frames collect and ticks mix the sessions in changing combinations."""
@@ -92,8 +93,11 @@ def test_served_sessions_equal_alone(torch_cuda):
     for k, (w, h, cfg) in enumerate(SESS):
         assert srv.poll(sids[k])["completed"] == F
         ref = alone(torch, w, h, cfg, data[k])
+        want = oracle_u8(oracle, data[k], **cfg)
         for t in range(F):
-            assert np.array_equal(outs[k][t].cpu().numpy(), ref[t]), f"session {k} frame {t}"
+            got = outs[k][t].cpu().numpy()
+            assert np.array_equal(got, ref[t]), f"session {k} frame {t}"
+            assert_close(got, want[t], cfg.get("color", False), f"session {k} frame {t}")
     srv.close()
 
 

@@ -5,6 +5,7 @@ colour and window (bilateral) modes; a snapshot of another config is refused."""
 import numpy as np
 import pytest
 
+from oracle_frames import assert_close, oracle_u8
 from wema_b200 import cuda as wc
 from wema_b200.synth import SynthSpec, SynthVideo
 
@@ -31,7 +32,7 @@ def run(torch, s, d, frames):
 
 @pytest.mark.parametrize("cfg", [dict(amp=60.0), dict(amp=60.0, color=True),
                                  dict(amp=40.0, use_iir=False, window=8, bilateral=True)])
-def test_session_snapshot_continues_exactly(torch_cuda, cfg):
+def test_session_snapshot_continues_exactly(oracle, torch_cuda, cfg):
     torch = torch_cuda
     w, h, F, K = 120, 88, 14, 9
     u8 = SynthVideo(SynthSpec(w, h, 30.0, 13, [1.4], [0.4], 14.0, 2.0)).frames(0, F)
@@ -43,8 +44,10 @@ def test_session_snapshot_continues_exactly(torch_cuda, cfg):
     b = wc.Session(width=w, height=h, fps=30.0, **cfg)
     b.restore(snap)
     got = run(torch, b, d, range(K, F))
+    want = oracle_u8(oracle, u8, fps=30.0, **cfg)
     for t in range(F - K):
         assert np.array_equal(got[t], ref[t]), f"frame {K + t}"
+        assert_close(got[t], want[K + t], cfg.get("color", False), f"restored frame {K + t}")
     c = wc.Session(width=w + 8, height=h, fps=30.0, **cfg)
     with pytest.raises(RuntimeError):
         c.restore(snap)
@@ -52,7 +55,7 @@ def test_session_snapshot_continues_exactly(torch_cuda, cfg):
         s.close()
 
 
-def test_batched_stream_snapshot(torch_cuda):
+def test_batched_stream_snapshot(oracle, torch_cuda):
     torch = torch_cuda
     w, h, F, K = 128, 96, 10, 6
     u8 = SynthVideo(SynthSpec(w, h, 30.0, 21, [1.0], [0.4], 14.0, 2.0)).frames(0, F)
@@ -76,7 +79,9 @@ def test_batched_stream_snapshot(torch_cuda):
     for t in range(K, F):
         b2.tick([other, y], [dn[0], d[t]], [on, o[t]])
     b2.sync()
+    want = oracle_u8(oracle, u8, amp=70.0)
     for t in range(K, F):
         assert np.array_equal(o[t].cpu().numpy(), ref[t - K]), f"frame {t}"
+        assert_close(o[t].cpu().numpy(), want[t], False, f"restored frame {t}")
     b1.close()
     b2.close()

@@ -290,10 +290,17 @@ public:
             if (!h_in[k] || !h_out[k]) { set_error("stream %d: null frame", id); return false; }
             if ((int)hstage.size() <= id) hstage.resize(id + 1, {nullptr, nullptr, nullptr, nullptr});
             const size_t fb = 3 * (size_t)streams[id]->g.pixels;
-            if (!hstage[id][0])
-                for (uint8_t*& p : hstage[id])
-                    if (!cuda_ok(cudaMallocAsync((void**)&p, fb, st_h2d), "cudaMallocAsync(host staging)"))
+            if (!hstage[id][0]) {
+                // all four staging buffers or none: a partial set is freed
+                std::array<uint8_t*, 4> got{nullptr, nullptr, nullptr, nullptr};
+                for (uint8_t*& p : got)
+                    if (!cuda_ok(cudaMallocAsync((void**)&p, fb, st_h2d), "cudaMallocAsync(host staging)")) {
+                        for (uint8_t* q : got)
+                            if (q) cudaFreeAsync(q, st_h2d);
                         return false;
+                    }
+                hstage[id] = got;
+            }
             din[k] = hstage[id][2 * hcur];
             dout[k] = hstage[id][2 * hcur + 1];
         }

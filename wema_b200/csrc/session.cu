@@ -548,8 +548,12 @@ bool Session::restore(const void* host, size_t bytes) {
         set_error("snapshot is of another stream configuration");
         return false;
     }
+    // from pageable memory cudaMemcpy may return before its DMA lands, and the
+    // session's streams are non-blocking (not ordered after the legacy
+    // stream): wait for the legacy stream before the next frame can read
     if (!cuda_ok(cudaMemcpy(arena, (const char*)host + sizeof h, arena_bytes, cudaMemcpyHostToDevice),
-                 "restore copy"))
+                 "restore copy") ||
+        !cuda_ok(cudaStreamSynchronize(cudaStreamLegacy), "restore copy sync"))
         return false;
     frames_run = h.frames_run;
     frames_processed = h.frames_processed;
