@@ -272,26 +272,127 @@ def cpu_reference_rate(name, frames_u8, kw, nframes):
             "sample": f"{nframes} frames of {name} ({w}x{h}), first-frame preseed included"}
 
 
-def mixed_cpu_sample():
-    """The reference's CPU path on a bounded sample of the mix: 3 frames of
-    one stream of each size, one after another (Mpix-frames/s)."""
+def _mix_sizes():
+    """The mix's sizes: (first stream of the size, its settings, streams of
+    that size in the mix)."""
     from wema_b200 import synth as S
-    picks, seen = [], set()
+    picks, count = {}, {}
     for spec, cfg in S.mixed_streams(seed=7):
-        if (spec.width, spec.height) not in seen:
-            seen.add((spec.width, spec.height))
-            picks.append((spec, cfg))
-    tot_pix, tot_s, cores, r = 0, 0.0, 1, {}
-    for spec, cfg in picks:
-        fr = S.SynthVideo(spec).frames(0, 3)
-        r = cpu_reference_rate("mixed_streams_48", fr, cfg, 3)
-        tot_pix += spec.width * spec.height * 3
-        tot_s += spec.width * spec.height * 3 / (r["value"] * 1e6)
-        cores = r["cores"]
-    return {"value": round(tot_pix / tot_s / 1e6, 4), "unit": METRIC, "cores": cores,
-            "kind": r.get("kind"),
-            "sample": "3 frames each of one 640x480, 1280x720, 1920x1080 and 3840x2160 stream "
-                      "of the mix, first-frame preseed included"}
+        key = (spec.width, spec.height)
+        count[key] = count.get(key, 0) + 1
+        picks.setdefault(key, (spec, cfg))
+    return [(spec, cfg, count[k]) for k, (spec, cfg) in picks.items()]
+
+
+def mixed_cpu_sample(log=None):
+    """The reference's CPU path on a bounded sample of the mix (about 20 s):
+    for one stream of each size, wema_batch_process on all host cores
+    (batches of 16 frames, 8 at 3840x2160), an untimed 1-frame first batch
+    (the preseed, timed on its own), then 16 steady frames.  The sizes' rates
+    are combined in the mix's proportions."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_timing as RT
+    from oracle import Oracle, Reference
+    from wema_b200 import synth as S
+    O = Oracle()
+    cores = RT.host_cores()
+    per, rates = {}, []
+    kind = "reference" if RT.reference_available() else "port"
+    R = Reference() if kind == "reference" else None
+    for spec, cfg, n in _mix_sizes():
+        w, h = spec.width, spec.height
+        b = 8 if w * h > 4_000_000 else 16
+        fr = S.SynthVideo(spec).frames(0, b + 1)
+        if R is not None:
+            pre = RT.preseed_ms(R, O, O.u8_to_float(fr[:1])[0], cfg)
+            st = RT.RefStream(R, w, h, cfg, b, cores)
+            st.run(O.u8_to_float(fr[:1]))
+            rgb = O.u8_to_float(fr[1:])
+            secs = sum(st.run(rgb) for _ in range(-(-16 // b)))
+            st.close()
+            r = w * h * b * (-(-16 // b)) / secs / 1e6
+            per[f"{w}x{h}"] = {"batch": b, "threads": cores, "mpix_frames_s": round(r, 3),
+                               "preseed_ms": round(pre, 1)}
+        else:
+            r = RT.port_rate(O, fr, cfg, 4)
+            per[f"{w}x{h}"] = {"threads": 1, "mpix_frames_s": round(r, 3)}
+        rates.append((n, w * h, r))
+    return {"value": round(RT.mix_rate(rates), 4), "unit": METRIC,
+            "cores": cores if kind == "reference" else 1, "kind": kind,
+            "sample": "one stream of each size of the mix: wema_batch_process, all cores, "
+                      "batch 16 (8 at 3840x2160), 16 steady frames after an untimed first "
+                      "batch; preseed timed separately; sizes combined in the mix's proportions",
+            "per_size": per}
+
+
+def reference_mixed(a):
+    """The reference arm on the mixed workload: the reference's own C path
+    (oracle/_ref) on this host's cores, like for like with the device's steady
+    ticks.  Per size of the mix (one stream of each): the sweep of batch
+    8 / 16 / 64 x threads 1 / all cores (each candidate an untimed 1-frame
+    batch with the preseed, then >= 16 steady frames), the best candidate
+    kept; its preseed time is reported on its own.  Then the timed steps:
+    step i is one batch of size (i mod 4) through its best candidate, after
+    `warmup` untimed steps; value = the sizes' steady rates combined in the
+    mix's proportions (16 / 16 / 12 / 4 streams)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_timing as RT
+    from oracle import Oracle, Reference
+    from wema_b200 import synth as S
+    O = Oracle()
+    cores = RT.host_cores()
+    sizes = _mix_sizes()
+    K = max(1, min(a.steps, 40))
+    W = a.warmup
+    if not RT.reference_available():
+        rates, per = [], {}
+        for spec, cfg, n in sizes:
+            fr = S.SynthVideo(spec).frames(0, 5)
+            r = RT.port_rate(O, fr, cfg, 4)
+            rates.append((n, spec.width * spec.height, r))
+            per[f"{spec.width}x{spec.height}"] = {"threads": 1, "mpix_frames_s": round(r, 3)}
+        v = RT.mix_rate(rates)
+        return v, None, {"value": round(v, 4), "unit": METRIC, "cores": 1, "kind": "port",
+                         "sample": "the oracle restatement, 4 frames per size", "per_size": per}
+    R = Reference()
+    log = (lambda m: print(m, file=sys.stderr, flush=True))
+    per, rates, total_s, steps_done = {}, [], 0.0, 0
+    for si, (spec, cfg, n) in enumerate(sizes):
+        w, h = spec.width, spec.height
+        bmax = max(b for b, _ in RT.batch_candidates(w * h, cores))
+        fr = S.SynthVideo(spec).frames(0, bmax + 1)
+        pre = RT.preseed_ms(R, O, O.u8_to_float(fr[:1])[0], cfg)
+        sweep, best = RT.sweep_size(R, O, fr, cfg, cores, log=log)
+        b, t = best["batch"], best["threads"]
+        mine = [i for i in range(W + K) if i % len(sizes) == si]
+        st = RT.RefStream(R, w, h, cfg, b, t)
+        rgb = O.u8_to_float(fr)
+        st.run(rgb[:1])
+        secs, frames = 0.0, 0
+        for i in mine:
+            dt = st.run(np.ascontiguousarray(rgb[1:b + 1]))
+            if i >= W:
+                secs += dt
+                frames += b
+                steps_done += 1
+        if frames == 0:                              # too few steps to reach this size
+            secs = st.run(np.ascontiguousarray(rgb[1:b + 1]))
+            frames = b
+        st.close()
+        total_s += secs
+        r = w * h * frames / secs / 1e6
+        rates.append((n, w * h, r))
+        per[f"{w}x{h}"] = {"streams_in_mix": n, "batch": b, "threads": t,
+                           "mpix_frames_s": round(r, 3), "frames_timed": frames,
+                           "preseed_ms": round(pre, 1), "sweep": sweep}
+    v = RT.mix_rate(rates)
+    cb = {"value": round(v, 4), "unit": METRIC, "cores": cores, "kind": "reference",
+          "sample": "one stream of each size of the mix through wema_batch_process; per size "
+                    "the best of batch 8/16/64 x threads 1/all, steady frames after an "
+                    "untimed first batch (preseed timed separately); sizes combined in the "
+                    "mix's proportions",
+          "per_size": per}
+    return v, (total_s * 1e3 / max(steps_done, 1), steps_done), cb
 
 
 def mixed_config(world):
@@ -827,15 +928,17 @@ def main():
             return bench_mixed(a, rank, world, local)
         if rank != 0:
             return
-        cb = mixed_cpu_sample()
-        v = cb["value"]
-        print(json.dumps({"metric": METRIC, "value": v, "unit": METRIC, "n_gpus": a.gpus,
-                          "steps": 3, "warmup": 0, "higher_is_better": True, "scaling": "weak",
-                          "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                          "impl": "reference", "config": mixed_config(a.gpus),
-                          "cpu_baseline": cb,
-                          "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0,
-                                  "d2h_bytes_per_step": 0}}), flush=True)
+        v, timing, cb = reference_mixed(a)
+        line = {"metric": METRIC, "value": round(v, 4), "unit": METRIC, "n_gpus": a.gpus,
+                "steps": timing[1] if timing else 0, "warmup": a.warmup,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic", "impl": "reference",
+                "config": mixed_config(a.gpus), "cpu_baseline": cb,
+                "e2e": {"value": round(v, 4), "unit": METRIC, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        if timing:
+            line["ms_per_step"] = round(timing[0], 3)
+        print(json.dumps(line), flush=True)
         return
 
     from wema_b200 import synth as S
