@@ -60,6 +60,8 @@ WORKLOADS = {
     "mixed_streams_48": ("mixed_streams", None),
     # Poisson stream sessions through the served request loop (wema_cuda_server_*)
     "served_poisson": ("served_sessions", None),
+    # the 48 streams of the mix on the served loop, clients keeping their queues full
+    "served_saturated": ("mixed_streams", None),
     # error report of the precision variants against the FP64 re-evaluation
     "precision_report": ("precision_720p", None),
     # a small batched case for full ncu captures: 8 x 640x480 + 8 x 1920x1080
@@ -97,6 +99,9 @@ def parse():
     ap.add_argument("--served-seconds", type=float, default=20.0, help="served_poisson measured window")
     ap.add_argument("--precision-frames", type=int, default=480, help="precision_report frames")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-sweep", default="full", choices=["full", "none"],
+                    help="reference arm: sweep batch x threads per size (full), or batch 16 / 8 on "
+                         "all cores only (none)")
     return ap.parse_args()
 
 
@@ -362,8 +367,11 @@ def reference_mixed(a):
         bmax = max(b for b, _ in RT.batch_candidates(w * h, cores))
         fr = S.SynthVideo(spec).frames(0, bmax + 1)
         pre = RT.preseed_ms(R, O, O.u8_to_float(fr[:1])[0], cfg)
-        sweep, best = RT.sweep_size(R, O, fr, cfg, cores, log=log)
-        b, t = best["batch"], best["threads"]
+        if a.ref_sweep == "full":
+            sweep, best = RT.sweep_size(R, O, fr, cfg, cores, log=log)
+            b, t = best["batch"], best["threads"]
+        else:
+            sweep, b, t = [], (8 if w * h > 4_000_000 else 16), cores
         mine = [i for i in range(W + K) if i % len(sizes) == si]
         st = RT.RefStream(R, w, h, cfg, b, t)
         rgb = O.u8_to_float(fr)
@@ -403,6 +411,31 @@ def mixed_config(world):
             "mode": "IIR 0.5-5 Hz, luma, edge-aware guided filter",
             "mpix_per_tick": round(pix / 1e6, 3), "step": "one tick = one frame of every stream",
             "parallelism": f"replicas x{world}", "l2": "per-tick working set > 126 MB L2 (no flush)"}
+
+
+def plain_path_seconds(mix, d_in, d_out, local, t_stream, rounds, barrier):
+    """The plain one-stream-at-a-time GPU path: each stream's frame alone
+    through its own session, one after another, each waited for; seconds for
+    `rounds` frames of every stream (first frames, with the preseed, untimed)."""
+    import torch
+    from wema_b200 import cuda as wc
+    torch.cuda.synchronize()
+    sess = [wc.Session(width=spec.width, height=spec.height, device=local, inspect=False, **cfg)
+            for spec, cfg in mix]
+    K = d_in[0].shape[0]
+    for k in range(len(mix)):
+        sess[k].process_u8(d_in[k][0], d_out[k], stream=t_stream)
+    torch.cuda.synchronize()
+    barrier()
+    tp0 = time.perf_counter()
+    for i in range(rounds):
+        for k in range(len(mix)):
+            sess[k].process_u8(d_in[k][(i + 1) % K], d_out[k], stream=t_stream)
+            t_stream.synchronize()
+    plain_s = time.perf_counter() - tp0
+    for s in sess:
+        s.close()
+    return plain_s
 
 
 def bench_mixed(a, rank, world, local):
@@ -543,25 +576,10 @@ def bench_mixed(a, rank, world, local):
                                       for k in per_tick if per_tick[k] > 0 and sb[k] > 0},
                 "frac_of_hbm_roofline": round(total_bytes / (ms / a.steps * 1e-3) / 1e9 / peak, 4)}
 
-    # ---- the plain one-stream-at-a-time GPU path: each stream's frame alone
-    # through its own session, one after another, each waited for
+    # ---- the plain one-stream-at-a-time GPU path
     b.close()
-    torch.cuda.synchronize(dev)
-    sess = [wc.Session(width=spec.width, height=spec.height, device=local, inspect=False, **cfg)
-            for spec, cfg in mix]
-    for k in range(n):                                # first frames (preseed) untimed
-        sess[k].process_u8(d_in[k][0], d_out[k], stream=t_stream)
-    torch.cuda.synchronize(dev)
     P = max(2, a.steps // 8)
-    barrier()
-    tp0 = time.perf_counter()
-    for i in range(P):
-        for k in range(n):
-            sess[k].process_u8(d_in[k][(i + 1) % K], d_out[k], stream=t_stream)
-            t_stream.synchronize()
-    plain_s = time.perf_counter() - tp0
-    for s in sess:
-        s.close()
+    plain_s = plain_path_seconds(mix, d_in, d_out, local, t_stream, P, barrier)
 
     if dist:
         t = torch.tensor([ms, e2e_ms, plain_s, p99], device=dev, dtype=torch.float64)
@@ -706,6 +724,108 @@ def bench_served(a, rank, world, local):
         "gpu_launches": int(st["launches"]), "clocks": clocks,
     }
     srv.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def bench_served_saturated(a, rank, world, local):
+    """The 48 streams of the mix opened on the served loop at once, every
+    client keeping its queue full (it submits again whenever the server
+    accepts), so frames arrive faster than ticks complete and each tick takes
+    a frame of every live session: the served loop's saturated throughput
+    against the plain one-stream-at-a-time GPU path, with per-frame latency
+    (queueing included) and admission wait."""
+    import torch
+    from wema_b200 import cuda as wc
+    from wema_b200 import synth as S
+
+    from wema_b200 import replicas
+    torch.cuda.set_device(local)
+    dist = replicas.init("nccl")
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    mix = S.mixed_streams(seed=7 + rank)
+    n, K, R = len(mix), 4, 16                  # unique inputs per stream; output ring (> 8 pending + 3 ticks)
+    d_in, d_out, outs = [], [], []
+    for spec, cfg in mix:
+        h = torch.empty((K, spec.height, spec.width, 3), dtype=torch.uint8)
+        S.SynthVideo(spec).frames(0, K, out=h.numpy())
+        d_in.append(h.to(dev))
+        d_out.append(torch.empty((spec.height, spec.width, 3), dtype=torch.uint8, device=dev))
+        outs.append([torch.empty((spec.height, spec.width, 3), dtype=torch.uint8, device=dev)
+                     for _ in range(R)])
+    pix = [spec.width * spec.height for spec, _ in mix]
+    budget = 150 * 10**9
+    torch.cuda.synchronize(dev)
+    srv = wc.Server(device=local, budget_bytes=budget, max_streams=64)
+    sids = [srv.open(spec.width, spec.height, **cfg) for spec, cfg in mix]
+    t_open = time.perf_counter()
+    while any(srv.poll(x)["state"] != wc.SESSION_LIVE for x in sids):
+        if time.perf_counter() - t_open > 60:
+            raise RuntimeError("sessions not admitted within 60 s")
+        time.sleep(0.001)
+    admit_all_ms = (time.perf_counter() - t_open) * 1e3
+    nfr = [0] * n
+    warm, window = 1.0, min(float(a.served_seconds), 8.0)
+
+    def pump(until):
+        while time.perf_counter() < until:
+            for k in range(n):
+                # at most 8 pending + 3 ticks in flight per session: the ring of R outputs
+                # is never overwritten while in use
+                while srv.submit(sids[k], d_in[k][nfr[k] % K], outs[k][nfr[k] % R]) == 0:
+                    nfr[k] += 1
+            time.sleep(0.0002)
+
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        pump(t0 + warm)
+        srv.stats(reset=True)
+        pump(time.perf_counter() + window)
+        st = srv.stats()
+    srv.drain(120000)
+    clocks = clk.summary()
+    srv.close()
+    # the plain path on the same streams
+    t_stream = torch.cuda.Stream(device=dev)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+    P = 4
+    plain_s = plain_path_seconds(mix, d_in, d_out, local, t_stream, P, barrier)
+    _, _, value = replicas.aggregate(st["mpix_frames"] * 1e6, st["seconds"] * 1e3, dist, device=dev)
+    plain = P * sum(pix) * world / plain_s / 1e6
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": METRIC,
+        "n_gpus": world, "steps": int(st["ticks"]), "warmup": 0,
+        "ms_per_step": round(st["seconds"] * 1e3 / max(st["ticks"], 1), 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "served_saturated", "streams": n,
+                   "mix": "16x640x480@30, 16x1280x720@30, 12x1920x1080@60, 4x3840x2160@30",
+                   "mode": "IIR 0.5-5 Hz, luma, edge-aware guided filter",
+                   "arrivals": "every client resubmits as soon as the server accepts (saturating)",
+                   "window_s": window, "warmup_s": warm, "budget_bytes": budget,
+                   "step": "one tick of the dispatcher", "parallelism": f"replicas x{world}"},
+        "plain_gpu": {"value": round(plain, 2), "unit": METRIC,
+                      "how": "each stream's frame through its own session, one at a time, waited for"},
+        "served_over_plain": round(value / plain, 3),
+        "frames": int(st["frames"]), "frames_per_tick": round(st["frames"] / max(st["ticks"], 1), 2),
+        "latency_ms": {"p50": round(st["latency_p50_ms"], 3), "p99": round(st["latency_p99_ms"], 3),
+                       "max": round(st["latency_max_ms"], 3),
+                       "note": "submission to completion, queueing behind up to 8 pending frames included"},
+        "admission": {"all_48_live_ms": round(admit_all_ms, 2),
+                      "wait_p50_ms": round(st["admission_wait_p50_ms"], 3),
+                      "wait_max_ms": round(st["admission_wait_max_ms"], 3)},
+        "dispatcher_ms": {k: round(st[k], 3) for k in ("tick_host_ms_mean", "tick_host_ms_max",
+                                                       "tick_span_ms_mean", "tick_span_ms_max",
+                                                       "admit_ms_max")},
+        "gpu_launches": int(st["launches"]), "clocks": clocks,
+    }
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -916,6 +1036,13 @@ def main():
         return profile_batch16(a, rank, local)
     if a.workload == "precision_report":
         return bench_precision(a, rank, world, local)
+    if a.workload == "served_saturated":
+        if a.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference has no served "
+                                  "form; its CPU path is timed on the mixed_streams_48 sample"}))
+            return
+        return bench_served_saturated(a, rank, world, local)
     if a.workload == "served_poisson":
         if a.impl == "reference":
             if rank == 0:

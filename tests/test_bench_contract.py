@@ -22,7 +22,7 @@ def run(*args, timeout=600):
 @pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref_harness.so")),
                     reason="the reference library is built where its sources are (oracle/_ref)")
 def test_reference_arm_line():
-    line = run("--impl", "reference", "--steps", "3", "--warmup", "3")
+    line = run("--impl", "reference", "--steps", "4", "--warmup", "0", "--ref-sweep", "none")
     for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "higher_is_better", "scaling",
               "vs_baseline", "dtype", "data", "config", "impl", "cpu_baseline", "e2e"):
         assert k in line, k
@@ -30,8 +30,14 @@ def test_reference_arm_line():
     assert line["metric"] == "Mpix-frames/s" and line["value"] > 0
     assert line["cpu_baseline"]["kind"] == "reference" and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]
+    assert line["steps"] == 4 and line["warmup"] == 0
+    per = line["cpu_baseline"]["per_size"]
+    assert sorted(per) == ["1280x720", "1920x1080", "3840x2160", "640x480"]
+    for v in per.values():
+        assert v["mpix_frames_s"] > 0 and v["preseed_ms"] > 0 and v["frames_timed"] >= 8
 
 
-def test_served_reference_arm_is_unavailable():
-    line = run("--impl", "reference", "--workload", "served_poisson")
+@pytest.mark.parametrize("workload", ["served_poisson", "served_saturated"])
+def test_served_reference_arm_is_unavailable(workload):
+    line = run("--impl", "reference", "--workload", workload)
     assert line["impl"] == "reference" and "unavailable" in line

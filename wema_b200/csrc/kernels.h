@@ -105,6 +105,7 @@ struct TransferParams {
     uint8_t* out_u8;            // output RGB24 (optional)
     float* out_f32;             // output float RGB (optional)
     int edge_aware;             // 1: guided filter r=4 eps=0.01; 0: 5-tap Gaussian
+    int seg_rows;               // guided filter: output rows per sweep segment (0: the device's)
 };
 cudaError_t launch_transfer(const TransferParams& p, cudaStream_t st);
 cudaError_t spatial_prepare_device();
@@ -149,7 +150,10 @@ bool iir_set_positions(int dev, int positions);
 cudaError_t iir_autotune(int dev, float ms[3], int* chosen);
 cudaError_t launch_iir_multi(const void* d_args, const int* d_map, unsigned blocks, int preseed,
                              cudaStream_t st);
-unsigned transfer_grid(const TransferParams& p, unsigned& gx, unsigned& gy);
+unsigned transfer_grid(TransferParams& p, unsigned& gx, unsigned& gy);
+// guided filter rows per sweep segment on a device (default 128)
+int guided_rows(int dev);
+bool guided_set_rows(int dev, int rows);
 cudaError_t launch_transfer_multi(int edge_aware, const TransferParams* d_params, const int* d_map,
                                   unsigned blocks, cudaStream_t st);
 

@@ -114,10 +114,29 @@ public:
         budget = budget_bytes;
         max_streams = max_n;
         if (!batch.init(device, max_n)) return false;
+        if (!reserve()) return false;
         t_stats = now_ms();
         th = std::thread([this] { run(); });
         th_alloc = std::thread([this] { run_alloc(); });
         return true;
+    }
+
+    // The budget (at most the device's free memory less 2 GiB) is reserved in
+    // the device's stream-ordered pool before serving starts: one allocation,
+    // freed back to the pool, which keeps it (its release threshold is
+    // raised).  Sessions' state is then carved from reserved memory, so an
+    // admission does not grow the pool - growing it maps new physical memory,
+    // which blocked the dispatcher's launches for tens of milliseconds.
+    bool reserve() {
+        size_t free_b = 0, total_b = 0;
+        if (!cuda_ok(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo")) return false;
+        const size_t margin = (size_t)2 << 30;
+        const size_t want = std::min(budget, free_b > margin ? free_b - margin : (size_t)0);
+        if (want == 0) return true;
+        void* p = nullptr;
+        if (!cuda_ok(cudaMallocAsync(&p, want, batch.st_main), "cudaMallocAsync(reserve)")) return false;
+        if (!cuda_ok(cudaFreeAsync(p, batch.st_main), "cudaFreeAsync(reserve)")) return false;
+        return cuda_ok(cudaStreamSynchronize(batch.st_main), "reserve sync");
     }
 
     // allocation thread: Batch::make touches no batch state
@@ -133,6 +152,12 @@ public:
             lk.unlock();
             const double t0 = now_ms();
             Session* s = batch.make(cfg);
+            if (!s) {                  // the pool may hold reserved memory it cannot split: release it, retry
+                cudaMemPool_t pool;
+                if (cudaDeviceGetDefaultMemPool(&pool, batch.device) == cudaSuccess &&
+                    cudaMemPoolTrimTo(pool, 0) == cudaSuccess)
+                    s = batch.make(cfg);
+            }
             const double dt = now_ms() - t0;
             const std::string why = s ? "" : last_error();
             lk.lock();

@@ -7,25 +7,22 @@
 // with border renormalisation (wema.c:236-283); then
 // out = clamp01(RGB + smooth) and u8 = (uint8)(v*255 + 0.5).
 //
-// One CTA produces a TS x TS output tile.  The guided filter's two rounds of
-// radius-4 box means need an 8-pixel halo; every box mean is the clipped
-// window's sum divided by the clipped count, rows first then columns (the
-// reference's definition), computed here by window sums sliding along short
-// segments in shared memory rather than by the reference's FP32 running
-// prefix sums - the two differ in the last bits only, which the u8 output
-// absorbs (<= 1 LSB).
+// Guided filter: one warp sweeps a strip of the frame from top to bottom
+// (see guided_sweep).  Every box mean is the clipped window's sum divided by
+// the clipped count (the reference's definition); the sums here are
+// vertical running sums over a 9-row ring and horizontal window sums across
+// the warp's lanes, not the reference's FP32 running prefix sums - the two
+// differ in the last bits only, which the u8 output absorbs (<= 1 LSB).
 #include "common.cuh"
 #include "kernels.h"
 #include "multi.cuh"
 
+#include <atomic>
+
 namespace wema {
 
-constexpr int TS = 32;
-constexpr int GR = 4;                   // guided-filter radius
-constexpr int H0 = 2 * GR;              // input halo
-constexpr int R0 = TS + 2 * H0;         // 48: I, p region
-constexpr int R1 = TS + 2 * GR;         // 40: first-round means, a, b
-constexpr int SP_THREADS = 256;
+constexpr int TS = 32;                  // Gaussian fallback: output tile
+constexpr int SP_THREADS = 256;         // Gaussian fallback: threads per tile
 
 struct SpArgs { TransferParams p; };
 
@@ -55,354 +52,343 @@ __device__ __forceinline__ void store_rgb(const TransferParams& p, int pi, float
     }
 }
 
-// Shared-memory rows are padded to 16-byte strides that keep 128-bit accesses
-// by 8 consecutive rows on distinct banks; arrays dead after one phase share
-// space with the next phase's.
-constexpr int IS = 52;                  // row stride of I, p
-constexpr int HS = 44;                  // row stride of the first-round row means and a, b
-constexpr int QS = 36;                  // row stride of the second-round row means and dy
-constexpr int NG = R0 * R0 / 4;         // 4-pixel groups of the 48x48 region (12 per row)
+// ---- guided filter: a vertical sweep per warp --------------------------------
+//
+// A warp owns a strip of 128 input columns, 4 consecutive columns per lane,
+// and sweeps a segment of `seg_rows` output rows from top to bottom.  The
+// strip's first and last 8 columns are the halo of the two radius-4 rounds,
+// so a strip produces 112 output columns (lanes 2..29); strips overlap by 16
+// columns and segments by 16 rows (the vertical halo), about 1.14 x 1.13
+// the output area loaded, against 2.25 for a 32x32 tile with its 8-pixel
+// border.  Per input row r entering the sweep:
+//   I, p of row r (0 outside the image) go into a 9-row ring in shared
+//   memory; vertical running sums of I, p, I*I, I*p over rows r-8..r add
+//   row r and drop row r-9 (read back from the ring);
+//   the first round at row r-4: horizontal 9-column window sums of those
+//   vertical sums, exchanged with the neighbouring lanes by shuffles, times
+//   1/(clipped column count x clipped row count) give mean_I, mean_p,
+//   corr_II, corr_Ip and then a, b (0 outside the image, wema.c:206-217);
+//   the horizontal window sums of a and b go into a second 9-row ring, whose
+//   vertical running sums over rows r-12..r-4 give the second round at row
+//   r-8: dy = mean_a * I + mean_b (wema.c:218-229, I read back from the
+//   first ring), added to the row's RGB, clamped and quantised.
+// Running sums restart at every segment, so rounding drift spans at most
+// seg_rows + 16 updates.
+constexpr int GR = 4;                   // guided-filter radius (wema.c:314)
+constexpr int GS_IN = 128;              // input columns per strip (4 per lane)
+constexpr int GS_OUT = GS_IN - 4 * GR;  // output columns per strip
+constexpr int GS_RING = 2 * GR + 1;     // rows in each ring
+constexpr int GS_WARPS = 2;             // strips per CTA (one per warp)
+constexpr int GS_THREADS = 32 * GS_WARPS;
+constexpr int GS_ROWS_DEFAULT = 128;
+constexpr float kEps = 0.01f;           // wema.c:315
+constexpr unsigned kFull = 0xffffffffu;
 
-struct GuidedSmem {
-    float I[R0][IS];                    // guide over the 48x48 region, 0 outside the image
-    union {
-        float P[R0][IS];                // p over the region (load, first-round rows)
-        struct {
-            float A[R1][HS];            // a, b over the 40x40 first-round region (0 outside)
-            float B[R1][HS];
-        } ab;
-    } x;
-    union {
-        float hm[4][R0][HS];            // row means of I, p, I*I, I*p (0 outside the image)
-        struct {
-            float ha[2][R1][QS];        // row means of a, b
-            float dy[TS][QS];           // the smoothed luma delta of the tile
-        } sec;
-    } y;
-    uint32_t rgbw[TS][TS * 3 / 4];      // the tile's input RGB24 as words (word-aligned frames)
-    float rcp[16];                      // 1/k for the clipped window counts k = 1 .. 2 GR + 1
-    float lut[256];                     // u8 -> float, i / 255 correctly rounded
+struct SweepRing {                      // one warp's rings
+    float4 ip[GS_RING][2][32];          // I, p of rows r-8..r; lane l holds columns 4l..4l+3
+    float4 ab[GS_RING][2][32];          // horizontal window sums of a, b
 };
 
-// 1 / (clipped count of a radius-4 window at coordinate c of a line of n)
-__device__ __forceinline__ float inv_count(const float* rcp, int c, int n) {
-    return rcp[min(c + GR, n - 1) - max(c - GR, 0) + 1];
+// u8 -> float: fl(i / 255), as the reference's frame reader converts
+// (ffmpeg_io.c:293).  With x = i / 256 (exact), fma(x, fl(1/255), x) =
+// x * (1 + fl(1/255)) rounded once equals the correctly rounded i / 255 for
+// every i in 0..255 (checked exhaustively in tests/test_u8_exact.py).
+__device__ __forceinline__ float u8f(uint32_t i) {
+    const float x = __fmul_rn(__uint2float_rn(i), 0.00390625f);
+    return __fmaf_rn(x, 1.0f / 255.0f, x);
+}
+__device__ __forceinline__ float byte_of(uint32_t w, int k) { return u8f((w >> (8 * k)) & 0xffu); }
+
+// 1 / (clipped count of a radius-4 window at coordinate c of a line of n);
+// 0 for c outside the line
+__device__ __forceinline__ float inv_count(int c, int n) {
+    if (c < 0 || c >= n) return 0.f;
+    return __frcp_rn((float)(min(c + GR, n - 1) - max(c - GR, 0) + 1));
 }
 
-__device__ __forceinline__ float byte_f(const float* lut, uint32_t w, int k) {
-    return lut[(w >> (8 * k)) & 0xffu];
-}
-
-// guide luma of 4 pixels from their 12 RGB24 bytes (words a0 a1 a2); pi = first pixel
-__device__ __forceinline__ void luma4(const float* lut, uint32_t a0, uint32_t a1, uint32_t a2,
-                                      long long pi, long long vec_end, float v[4]) {
-    float r[4], g[4], b[4];
-    r[0] = byte_f(lut, a0, 0); g[0] = byte_f(lut, a0, 1); b[0] = byte_f(lut, a0, 2);
-    r[1] = byte_f(lut, a0, 3); g[1] = byte_f(lut, a1, 0); b[1] = byte_f(lut, a1, 1);
-    r[2] = byte_f(lut, a1, 2); g[2] = byte_f(lut, a1, 3); b[2] = byte_f(lut, a2, 0);
-    r[3] = byte_f(lut, a2, 1); g[3] = byte_f(lut, a2, 2); b[3] = byte_f(lut, a2, 3);
-    if (pi + 3 < vec_end) {
+// The 9-column window sums centred on a lane's 4 columns: its own 4 values
+// and its neighbours' 4 each, by shuffles (lanes 0 and 31 get garbage, which
+// only halo columns use).
+__device__ __forceinline__ void hwin(const float v[4], float o[4]) {
+    float L[4], R[4];
 #pragma unroll
-        for (int j = 0; j < 4; j++) v[j] = luma_vec(r[j], g[j], b[j]);
-    } else {
+    for (int j = 0; j < 4; j++) {
+        L[j] = __shfl_up_sync(kFull, v[j], 1);
+        R[j] = __shfl_down_sync(kFull, v[j], 1);
+    }
+    float s = __fadd_rn(__fadd_rn(__fadd_rn(L[0], L[1]), __fadd_rn(L[2], L[3])),
+                        __fadd_rn(__fadd_rn(v[0], v[1]), __fadd_rn(v[2], v[3])));
+    s = __fadd_rn(s, R[0]);
+    o[0] = s;
 #pragma unroll
-        for (int j = 0; j < 4; j++)
-            v[j] = pi + j < vec_end ? luma_vec(r[j], g[j], b[j]) : luma_tail(r[j], g[j], b[j]);
+    for (int j = 1; j < 4; j++) {
+        s = __fadd_rn(__fsub_rn(s, L[j - 1]), R[j]);
+        o[j] = s;
     }
 }
 
-// Box means with the image's edges: every array holds 0 outside the image,
-// so a radius-4 window's sum is its clipped sum, and the mean is that sum
-// times 1/(clipped count).  Sums slide along segments of 8 (the last round 4)
-// outputs.  Frames whose RGB24 rows are word-aligned (width a multiple of 4)
-// move 4 pixels = 3 words per thread and access.  IN: the 48x48 region lies
-// inside the image, so no test is needed and every count is 9.
-template <bool IN>
-__device__ __forceinline__ void guided_tile(const TransferParams& p, GuidedSmem& S, int bx, int by) {
-    const int W = p.w, H = p.h;
-    const int x0 = bx * TS, y0 = by * TS;
-    const int gx0 = x0 - H0, gy0 = y0 - H0;      // region origin (may be negative)
-    const int tid = threadIdx.x;
-    const bool fast = p.src_u8 && !(W & 3) && !(reinterpret_cast<uintptr_t>(p.src_u8) & 3) &&
-                      !(reinterpret_cast<uintptr_t>(p.gray_out) & 15);
+// One row of 4 pixels of a lane: the loads of row r (issued a row ahead) and
+// their decoding.  FAST: RGB24 rows word-aligned (width a multiple of 4 and
+// aligned buffers): the 4 pixels are 3 words, all in or all out of the image.
+template <bool FAST>
+struct RowLoad {
+    uint32_t w[3];
+    float4 g;
+    float rgb[12];                      // generic path: decoded RGB
+    float gv[4];
+    bool any;
 
-    // region loads first (a thread's groups tid, tid + 256, tid + 512), tables meanwhile
-    uint32_t wv[3][3];
-    float4 gv[3];
-    bool ok[3];
-    if (fast) {
-#pragma unroll
-        for (int i = 0; i < 3; i++) {
-            const int k = tid + i * SP_THREADS;
-            const int ly = k / 12, g = k - ly * 12;
-            const int gx = gx0 + 4 * g, gy = gy0 + ly;
-            ok[i] = k < NG && (IN || (gx >= 0 && gx < W && gy >= 0 && gy < H));
-            if (ok[i]) {
-                const int pi = gy * W + gx;
+    __device__ __forceinline__ void issue(const TransferParams& p, int r, int cx) {
+        any = r >= 0 && r < p.h && cx + 3 >= 0 && cx < p.w;
+        if (FAST) {
+            if (any) {
+                const long long pi = (long long)r * p.w + cx;
                 const uint32_t* q = reinterpret_cast<const uint32_t*>(p.src_u8) + 3 * (pi >> 2);
-                wv[i][0] = __ldg(q);
-                wv[i][1] = __ldg(q + 1);
-                wv[i][2] = __ldg(q + 2);
-                gv[i] = __ldg(reinterpret_cast<const float4*>(p.gray_out + pi));
+                w[0] = __ldg(q);
+                w[1] = __ldg(q + 1);
+                w[2] = __ldg(q + 2);
+                g = __ldg(reinterpret_cast<const float4*>(p.gray_out + pi));
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int x = cx + j;
+                const bool in = any && x >= 0 && x < p.w;
+                const long long pi = (long long)r * p.w + x;
+                gv[j] = in ? __ldg(p.gray_out + pi) : 0.f;
+#pragma unroll
+                for (int c = 0; c < 3; c++)
+                    rgb[3 * j + c] = !in ? 0.f
+                                         : (p.src_u8 ? u8f(__ldg(p.src_u8 + 3 * pi + c))
+                                                     : __ldg(p.src_f32 + 3 * pi + c));
             }
         }
     }
-    S.lut[tid] = __fdiv_rn((float)tid, 255.0f);
-    if (tid < 16) S.rcp[tid] = tid ? __frcp_rn((float)tid) : 0.f;
-    __syncthreads();
 
-    // I and p over the 48x48 region
-    if (fast) {
+    // guide I and p = gray_out - I of the 4 pixels (0 outside the image)
+    __device__ __forceinline__ void decode(const TransferParams& p, int r, int cx, float I[4],
+                                           float P[4]) const {
+        const long long pi0 = (long long)r * p.w + cx;
+        float rr[4], gg[4], bb[4], gy[4];
+        if (FAST) {
+            rr[0] = byte_of(w[0], 0); gg[0] = byte_of(w[0], 1); bb[0] = byte_of(w[0], 2);
+            rr[1] = byte_of(w[0], 3); gg[1] = byte_of(w[1], 0); bb[1] = byte_of(w[1], 1);
+            rr[2] = byte_of(w[1], 2); gg[2] = byte_of(w[1], 3); bb[2] = byte_of(w[2], 0);
+            rr[3] = byte_of(w[2], 1); gg[3] = byte_of(w[2], 2); bb[3] = byte_of(w[2], 3);
+            gy[0] = g.x; gy[1] = g.y; gy[2] = g.z; gy[3] = g.w;
+        } else {
 #pragma unroll
-        for (int i = 0; i < 3; i++) {
-            const int k = tid + i * SP_THREADS;
-            if (k >= NG) break;
-            const int ly = k / 12, g = k - ly * 12;
-            float4 Iv = make_float4(0.f, 0.f, 0.f, 0.f), Pv = Iv;
-            if (ok[i]) {
-                const uint32_t a0 = wv[i][0], a1 = wv[i][1], a2 = wv[i][2];
-                float v[4];
-                luma4(S.lut, a0, a1, a2, (long long)(gy0 + ly) * W + gx0 + 4 * g, p.vec_end, v);
-                Iv = make_float4(v[0], v[1], v[2], v[3]);
-                Pv = make_float4(__fadd_rn(gv[i].x, -v[0]), __fadd_rn(gv[i].y, -v[1]),
-                                 __fadd_rn(gv[i].z, -v[2]), __fadd_rn(gv[i].w, -v[3]));
-                const int ty = ly - H0, tg = g - H0 / 4;
-                if (ty >= 0 && ty < TS && tg >= 0 && tg < TS / 4) {
-                    S.rgbw[ty][3 * tg] = a0;
-                    S.rgbw[ty][3 * tg + 1] = a1;
-                    S.rgbw[ty][3 * tg + 2] = a2;
-                }
+            for (int j = 0; j < 4; j++) {
+                rr[j] = rgb[3 * j]; gg[j] = rgb[3 * j + 1]; bb[j] = rgb[3 * j + 2];
+                gy[j] = gv[j];
             }
-            *reinterpret_cast<float4*>(&S.I[ly][4 * g]) = Iv;
-            *reinterpret_cast<float4*>(&S.x.P[ly][4 * g]) = Pv;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const bool in = any && (FAST || (cx + j >= 0 && cx + j < p.w));
+            const float Iv = pi0 + j < p.vec_end ? luma_vec(rr[j], gg[j], bb[j])
+                                                 : luma_tail(rr[j], gg[j], bb[j]);
+            I[j] = in ? Iv : 0.f;
+            P[j] = in ? __fadd_rn(gy[j], -Iv) : 0.f;
+        }
+    }
+};
+
+// out = clamp01(RGB + dy) of a lane's 4 output pixels of row y
+template <bool FAST>
+__device__ __forceinline__ void put_row(const TransferParams& p, int y, int cx, const float dy[4]) {
+    const long long pi0 = (long long)y * p.w + cx;
+    if (FAST) {
+        if (cx < 0 || cx >= p.w) return;
+        const uint32_t* q = reinterpret_cast<const uint32_t*>(p.src_u8) + 3 * (pi0 >> 2);
+        const uint32_t w[3] = {__ldg(q), __ldg(q + 1), __ldg(q + 2)};
+        float v[12];
+        uint32_t ow[3] = {0u, 0u, 0u};
+#pragma unroll
+        for (int c = 0; c < 12; c++) {
+            v[c] = clamp01(__fadd_rn(byte_of(w[c >> 2], c & 3), dy[c / 3]));
+            ow[c >> 2] |= (uint32_t)quant_u8(v[c]) << (8 * (c & 3));
+        }
+        if (p.out_u8) {
+            uint32_t* d = reinterpret_cast<uint32_t*>(p.out_u8) + 3 * (pi0 >> 2);
+            d[0] = ow[0];
+            d[1] = ow[1];
+            d[2] = ow[2];
+        }
+        if (p.out_f32) {
+            float4* d = reinterpret_cast<float4*>(p.out_f32 + 3 * pi0);
+            d[0] = make_float4(v[0], v[1], v[2], v[3]);
+            d[1] = make_float4(v[4], v[5], v[6], v[7]);
+            d[2] = make_float4(v[8], v[9], v[10], v[11]);
         }
     } else {
-        for (int k = tid; k < R0 * R0; k += SP_THREADS) {
-            const int ly = k / R0, lx = k - ly * R0;
-            const int gx = gx0 + lx, gy = gy0 + ly;
-            float I = 0.f, P = 0.f;
-            if (gx >= 0 && gx < W && gy >= 0 && gy < H) {
-                const int pi = gy * W + gx;
-                float r, g, b;
-                load_rgb(p, S.lut, pi, r, g, b);
-                I = pi < p.vec_end ? luma_vec(r, g, b) : luma_tail(r, g, b);
-                P = __fadd_rn(p.gray_out[pi], -I);
-            }
-            S.I[ly][lx] = I;
-            S.x.P[ly][lx] = P;
-        }
-    }
-    __syncthreads();
-
-    // first round, rows: 48 rows x 5 segments of 8 of the 40 columns
-    if (tid < R0 * (R1 / 8)) {
-        const int ly = tid % R0, c0 = (tid / R0) * 8;
-        const int gy = gy0 + ly;
-        const bool rowin = IN || (gy >= 0 && gy < H);
-        const float r9 = S.rcp[2 * GR + 1];
-        float Iv[16], Pv[16];
 #pragma unroll
         for (int j = 0; j < 4; j++) {
-            const float4 a = *reinterpret_cast<const float4*>(&S.I[ly][c0 + 4 * j]);
-            const float4 b = *reinterpret_cast<const float4*>(&S.x.P[ly][c0 + 4 * j]);
-            Iv[4 * j] = a.x; Iv[4 * j + 1] = a.y; Iv[4 * j + 2] = a.z; Iv[4 * j + 3] = a.w;
-            Pv[4 * j] = b.x; Pv[4 * j + 1] = b.y; Pv[4 * j + 2] = b.z; Pv[4 * j + 3] = b.w;
-        }
-        float sI = 0.f, sP = 0.f, sII = 0.f, sIP = 0.f;
-        // output column cx sits at region column cx + GR; its window is cx .. cx + 2 GR
+            const int x = cx + j;
+            if (x < 0 || x >= p.w) continue;
+            const long long pi = pi0 + j;
+            float c3[3];
 #pragma unroll
-        for (int x = 0; x < 2 * GR; x++) {
-            sI = __fadd_rn(sI, Iv[x]);
-            sP = __fadd_rn(sP, Pv[x]);
-            sII = __fmaf_rn(Iv[x], Iv[x], sII);
-            sIP = __fmaf_rn(Iv[x], Pv[x], sIP);
-        }
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            float o[4][4];
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const int x = 4 * h + j;
-                const float In = Iv[x + 2 * GR], Pn = Pv[x + 2 * GR];
-                sI = __fadd_rn(sI, In);
-                sP = __fadd_rn(sP, Pn);
-                sII = __fmaf_rn(In, In, sII);
-                sIP = __fmaf_rn(In, Pn, sIP);
-                const int gx = x0 - GR + c0 + x;
-                const bool in = IN || (rowin && gx >= 0 && gx < W);
-                const float inv = IN ? r9 : inv_count(S.rcp, gx, W);
-                o[0][j] = in ? __fmul_rn(sI, inv) : 0.f;
-                o[1][j] = in ? __fmul_rn(sP, inv) : 0.f;
-                o[2][j] = in ? __fmul_rn(sII, inv) : 0.f;
-                o[3][j] = in ? __fmul_rn(sIP, inv) : 0.f;
-                sI = __fsub_rn(sI, Iv[x]);
-                sP = __fsub_rn(sP, Pv[x]);
-                sII = __fmaf_rn(-Iv[x], Iv[x], sII);
-                sIP = __fmaf_rn(-Iv[x], Pv[x], sIP);
-            }
-#pragma unroll
-            for (int q = 0; q < 4; q++)
-                *reinterpret_cast<float4*>(&S.y.hm[q][ly][c0 + 4 * h]) =
-                    make_float4(o[q][0], o[q][1], o[q][2], o[q][3]);
-        }
-    }
-    __syncthreads();
-
-    // first round, columns -> a, b: 40 columns x 5 segments of 8 of the 40 rows
-    if (tid < R1 * (R1 / 8)) {
-        const int cx = tid % R1, r0 = (tid / R1) * 8;
-        const int gx = x0 - GR + cx;
-        const bool colin = IN || (gx >= 0 && gx < W);
-        const float r9 = S.rcp[2 * GR + 1];
-        float m[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-        for (int y = r0; y < r0 + 2 * GR; y++)
-#pragma unroll
-            for (int q = 0; q < 4; q++) m[q] = __fadd_rn(m[q], S.y.hm[q][y][cx]);
-        float av[8], bv[8];
-#pragma unroll
-        for (int j = 0; j < 8; j++) {
-            const int cy = r0 + j;
-#pragma unroll
-            for (int q = 0; q < 4; q++) m[q] = __fadd_rn(m[q], S.y.hm[q][cy + 2 * GR][cx]);
-            const int gy = y0 - GR + cy;
-            av[j] = 0.f;
-            bv[j] = 0.f;
-            if (IN || (colin && gy >= 0 && gy < H)) {
-                const float inv = IN ? r9 : inv_count(S.rcp, gy, H);
-                const float mI = __fmul_rn(m[0], inv), mP = __fmul_rn(m[1], inv);
-                const float cII = __fmul_rn(m[2], inv), cIP = __fmul_rn(m[3], inv);
-                // the denominator is >= 0.01 - mI^2 + E[I^2] > 0; a within 2 ulp
-                av[j] = __fdividef(__fmaf_rn(-mI, mP, cIP), __fmaf_rn(-mI, mI, __fadd_rn(cII, 0.01f)));
-                bv[j] = __fmaf_rn(-av[j], mI, mP);
-            }
-#pragma unroll
-            for (int q = 0; q < 4; q++) m[q] = __fsub_rn(m[q], S.y.hm[q][cy][cx]);
-        }
-#pragma unroll
-        for (int j = 0; j < 8; j++) {
-            S.x.ab.A[r0 + j][cx] = av[j];
-            S.x.ab.B[r0 + j][cx] = bv[j];
-        }
-    }
-    __syncthreads();
-
-    // second round, rows: 40 rows x 4 segments of 8 of the tile's 32 columns
-    if (tid < R1 * (TS / 8)) {
-        const int cy = tid % R1, t0 = (tid / R1) * 8;
-        const float r9 = S.rcp[2 * GR + 1];
-        float Av[16], Bv[16];
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const float4 a = *reinterpret_cast<const float4*>(&S.x.ab.A[cy][t0 + 4 * j]);
-            const float4 b = *reinterpret_cast<const float4*>(&S.x.ab.B[cy][t0 + 4 * j]);
-            Av[4 * j] = a.x; Av[4 * j + 1] = a.y; Av[4 * j + 2] = a.z; Av[4 * j + 3] = a.w;
-            Bv[4 * j] = b.x; Bv[4 * j + 1] = b.y; Bv[4 * j + 2] = b.z; Bv[4 * j + 3] = b.w;
-        }
-        float sa = 0.f, sb = 0.f;
-        // tile column tx sits at first-round column tx + GR; window tx .. tx + 2 GR
-#pragma unroll
-        for (int x = 0; x < 2 * GR; x++) {
-            sa = __fadd_rn(sa, Av[x]);
-            sb = __fadd_rn(sb, Bv[x]);
-        }
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            float oa[4], ob[4];
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const int x = 4 * h + j;
-                sa = __fadd_rn(sa, Av[x + 2 * GR]);
-                sb = __fadd_rn(sb, Bv[x + 2 * GR]);
-                const float inv = IN ? r9 : inv_count(S.rcp, min(x0 + t0 + x, W - 1), W);
-                oa[j] = __fmul_rn(sa, inv);
-                ob[j] = __fmul_rn(sb, inv);
-                sa = __fsub_rn(sa, Av[x]);
-                sb = __fsub_rn(sb, Bv[x]);
-            }
-            *reinterpret_cast<float4*>(&S.y.sec.ha[0][cy][t0 + 4 * h]) = make_float4(oa[0], oa[1], oa[2], oa[3]);
-            *reinterpret_cast<float4*>(&S.y.sec.ha[1][cy][t0 + 4 * h]) = make_float4(ob[0], ob[1], ob[2], ob[3]);
-        }
-    }
-    __syncthreads();
-
-    // second round, columns -> dy: 32 columns x 8 segments of 4 rows
-    {
-        const int tx = tid % TS, t0 = (tid / TS) * 4;
-        const float r9 = S.rcp[2 * GR + 1];
-        float sa = 0.f, sb = 0.f;
-#pragma unroll
-        for (int y = t0; y < t0 + 2 * GR; y++) {
-            sa = __fadd_rn(sa, S.y.sec.ha[0][y][tx]);
-            sb = __fadd_rn(sb, S.y.sec.ha[1][y][tx]);
-        }
-        float d[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int ty = t0 + j;
-            sa = __fadd_rn(sa, S.y.sec.ha[0][ty + 2 * GR][tx]);
-            sb = __fadd_rn(sb, S.y.sec.ha[1][ty + 2 * GR][tx]);
-            const float inv = IN ? r9 : inv_count(S.rcp, min(y0 + ty, H - 1), H);
-            d[j] = __fmaf_rn(__fmul_rn(sa, inv), S.I[ty + H0][tx + H0], __fmul_rn(sb, inv));
-            sa = __fsub_rn(sa, S.y.sec.ha[0][ty][tx]);
-            sb = __fsub_rn(sb, S.y.sec.ha[1][ty][tx]);
-        }
-#pragma unroll
-        for (int j = 0; j < 4; j++) S.y.sec.dy[t0 + j][tx] = d[j];
-    }
-    __syncthreads();
-
-    // out = clamp01(RGB + dy): a thread per 4-pixel group of the tile where the
-    // frame layout allows, else per pixel
-    const bool fast_out = fast && !(reinterpret_cast<uintptr_t>(p.out_u8) & 3) &&
-                          !(reinterpret_cast<uintptr_t>(p.out_f32) & 15);
-    if (fast_out) {
-        const int ty = tid >> 3, g = tid & 7;
-        const int gx = x0 + 4 * g, gy = y0 + ty;
-        if (IN || (gx < W && gy < H)) {
-            const int pi = gy * W + gx;
-            const float4 dv = *reinterpret_cast<const float4*>(&S.y.sec.dy[ty][4 * g]);
-            const float dyv[4] = {dv.x, dv.y, dv.z, dv.w};
-            const uint32_t w[3] = {S.rgbw[ty][3 * g], S.rgbw[ty][3 * g + 1], S.rgbw[ty][3 * g + 2]};
-            float v[12];
-            uint32_t ow[3] = {0u, 0u, 0u};
-#pragma unroll
-            for (int c = 0; c < 12; c++) {
-                v[c] = clamp01(__fadd_rn(byte_f(S.lut, w[c >> 2], c & 3), dyv[c / 3]));
-                ow[c >> 2] |= (uint32_t)quant_u8(v[c]) << (8 * (c & 3));
+            for (int c = 0; c < 3; c++) {
+                const float in = p.src_u8 ? u8f(__ldg(p.src_u8 + 3 * pi + c)) : __ldg(p.src_f32 + 3 * pi + c);
+                c3[c] = clamp01(__fadd_rn(in, dy[j]));
             }
             if (p.out_u8) {
-                uint32_t* d = reinterpret_cast<uint32_t*>(p.out_u8) + 3 * (pi >> 2);
-                d[0] = ow[0];
-                d[1] = ow[1];
-                d[2] = ow[2];
+#pragma unroll
+                for (int c = 0; c < 3; c++) p.out_u8[3 * pi + c] = quant_u8(c3[c]);
             }
             if (p.out_f32) {
-                float4* d = reinterpret_cast<float4*>(p.out_f32 + 3 * (long long)pi);
-                d[0] = make_float4(v[0], v[1], v[2], v[3]);
-                d[1] = make_float4(v[4], v[5], v[6], v[7]);
-                d[2] = make_float4(v[8], v[9], v[10], v[11]);
+#pragma unroll
+                for (int c = 0; c < 3; c++) p.out_f32[3 * pi + c] = c3[c];
             }
-        }
-    } else {
-        for (int k = tid; k < TS * TS; k += SP_THREADS) {
-            const int ty = k / TS, tx = k - ty * TS;
-            const int gx = x0 + tx, gy = y0 + ty;
-            if (gx >= W || gy >= H) continue;
-            const int pi = gy * W + gx;
-            float r, g, b;
-            load_rgb(p, S.lut, pi, r, g, b);
-            store_rgb(p, pi, r, g, b, S.y.sec.dy[ty][tx]);
         }
     }
 }
 
+template <bool FAST>
+__device__ __forceinline__ void guided_sweep(const TransferParams& p, SweepRing& R, int strip, int seg) {
+    const int W = p.w, H = p.h;
+    const int lane = threadIdx.x & 31;
+    const int x0 = strip * GS_OUT;
+    const int cx = x0 - 2 * GR + 4 * lane;          // this lane's first column
+    const int ys = seg * p.seg_rows;
+    const int ye = min(ys + p.seg_rows, H);
+    if (x0 >= W || ys >= H) return;
+
+    float icx[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) icx[j] = inv_count(cx + j, W);
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < GS_RING; k++) {
+        R.ip[k][0][lane] = z4; R.ip[k][1][lane] = z4;
+        R.ab[k][0][lane] = z4; R.ab[k][1][lane] = z4;
+    }
+    float vI[4] = {0.f, 0.f, 0.f, 0.f}, vP[4] = {0.f, 0.f, 0.f, 0.f};
+    float vII[4] = {0.f, 0.f, 0.f, 0.f}, vIP[4] = {0.f, 0.f, 0.f, 0.f};
+    float uA[4] = {0.f, 0.f, 0.f, 0.f}, uB[4] = {0.f, 0.f, 0.f, 0.f};
+    int s1 = 0, s2 = 0;                             // ring slots of the row entering
+
+    // one input row through the sweep (the row's loads were issued a row ahead)
+    auto step = [&](const RowLoad<FAST>& in, int r) {
+        float I[4], P[4];
+        in.decode(p, r, cx, I, P);
+        // ring of I, p; vertical sums over rows r-8..r
+        {
+            const float4 oI = R.ip[s1][0][lane], oP = R.ip[s1][1][lane];
+            R.ip[s1][0][lane] = make_float4(I[0], I[1], I[2], I[3]);
+            R.ip[s1][1][lane] = make_float4(P[0], P[1], P[2], P[3]);
+            const float ofI[4] = {oI.x, oI.y, oI.z, oI.w}, ofP[4] = {oP.x, oP.y, oP.z, oP.w};
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                vI[j] = __fsub_rn(__fadd_rn(vI[j], I[j]), ofI[j]);
+                vP[j] = __fsub_rn(__fadd_rn(vP[j], P[j]), ofP[j]);
+                vII[j] = __fmaf_rn(-ofI[j], ofI[j], __fmaf_rn(I[j], I[j], vII[j]));
+                vIP[j] = __fmaf_rn(-ofI[j], ofP[j], __fmaf_rn(I[j], P[j], vIP[j]));
+            }
+            s1 = s1 == GS_RING - 1 ? 0 : s1 + 1;
+        }
+        if (r < ys) return;                         // rows r-8..r not all in yet
+        // first round at row c1 = r - 4: a, b
+        float a[4], b[4];
+        {
+            float sI[4], sP[4], sII[4], sIP[4];
+            hwin(vI, sI);
+            hwin(vP, sP);
+            hwin(vII, sII);
+            hwin(vIP, sIP);
+            const float icy = inv_count(r - GR, H);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const float inv = __fmul_rn(icx[j], icy);
+                const float mI = __fmul_rn(sI[j], inv), mP = __fmul_rn(sP[j], inv);
+                const float cII = __fmul_rn(sII[j], inv), cIP = __fmul_rn(sIP[j], inv);
+                // the denominator is >= eps + E[I^2] - E[I]^2 > 0; a within 2 ulp
+                const float av = __fdividef(__fmaf_rn(-mI, mP, cIP),
+                                            __fmaf_rn(-mI, mI, __fadd_rn(cII, kEps)));
+                const bool inside = inv != 0.f;
+                a[j] = inside ? av : 0.f;
+                b[j] = inside ? __fmaf_rn(-av, mI, mP) : 0.f;
+            }
+        }
+        // second round: horizontal sums of a, b into the ring; vertical sums over rows c1-8..c1
+        {
+            float hA[4], hB[4];
+            hwin(a, hA);
+            hwin(b, hB);
+            const float4 oA = R.ab[s2][0][lane], oB = R.ab[s2][1][lane];
+            R.ab[s2][0][lane] = make_float4(hA[0], hA[1], hA[2], hA[3]);
+            R.ab[s2][1][lane] = make_float4(hB[0], hB[1], hB[2], hB[3]);
+            const float ofA[4] = {oA.x, oA.y, oA.z, oA.w}, ofB[4] = {oB.x, oB.y, oB.z, oB.w};
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                uA[j] = __fsub_rn(__fadd_rn(uA[j], hA[j]), ofA[j]);
+                uB[j] = __fsub_rn(__fadd_rn(uB[j], hB[j]), ofB[j]);
+            }
+            s2 = s2 == GS_RING - 1 ? 0 : s2 + 1;
+        }
+        if (r < ys + 2 * GR) return;                // first-round rows c1-8..c1 not all in yet
+        if (lane < 2 || lane >= 30) return;         // halo lanes
+        // output row y = r - 8; its I is the oldest row of the first ring (slot s1)
+        const int y = r - 2 * GR;
+        const float icy = inv_count(y, H);
+        const float4 Iy = R.ip[s1][0][lane];
+        const float Iv[4] = {Iy.x, Iy.y, Iy.z, Iy.w};
+        float dy[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const float inv = __fmul_rn(icx[j], icy);
+            dy[j] = __fmaf_rn(__fmul_rn(uA[j], inv), Iv[j], __fmul_rn(uB[j], inv));
+        }
+        put_row<FAST>(p, y, cx, dy);
+    };
+
+    // two load buffers in turn, so a row's loads are in flight while the
+    // previous row is computed (no register copy that would wait on them)
+    const int r0 = ys - 2 * GR, r1 = ye + 2 * GR;
+    RowLoad<FAST> A, B;
+    A.issue(p, r0, cx);
+    for (int r = r0; r < r1; r += 2) {
+        if (r + 1 < r1) B.issue(p, r + 1, cx);
+        step(A, r);
+        if (r + 1 >= r1) break;
+        if (r + 2 < r1) A.issue(p, r + 2, cx);
+        step(B, r + 1);
+    }
+}
+
+__device__ __forceinline__ bool sweep_fast(const TransferParams& p) {
+    return p.src_u8 && !(p.w & 3) && !(reinterpret_cast<uintptr_t>(p.src_u8) & 3) &&
+           !(reinterpret_cast<uintptr_t>(p.gray_out) & 15) &&
+           !(reinterpret_cast<uintptr_t>(p.out_u8) & 3) && !(reinterpret_cast<uintptr_t>(p.out_f32) & 15);
+}
+
+// block (bx, by): strips GS_WARPS*bx .. +GS_WARPS-1 of segment by
 __device__ __forceinline__ void guided_body(const TransferParams& p, int bx, int by) {
-    extern __shared__ __align__(16) unsigned char raw[];
-    GuidedSmem& S = *reinterpret_cast<GuidedSmem*>(raw);
-    const int gx0 = bx * TS - H0, gy0 = by * TS - H0;
-    if (gx0 >= 0 && gy0 >= 0 && gx0 + R0 <= p.w && gy0 + R0 <= p.h) guided_tile<true>(p, S, bx, by);
-    else guided_tile<false>(p, S, bx, by);
+    __shared__ SweepRing rings[GS_WARPS];
+    const int w = threadIdx.x >> 5;
+    if (sweep_fast(p)) guided_sweep<true>(p, rings[w], bx * GS_WARPS + w, by);
+    else guided_sweep<false>(p, rings[w], bx * GS_WARPS + w, by);
+}
+
+// ---- rows per segment, per device (the autotuner may change it)
+static std::atomic<int> g_seg_rows[64];
+
+int guided_rows(int dev) {
+    const int v = (dev >= 0 && dev < 64) ? g_seg_rows[dev].load() : 0;
+    return v > 0 ? v : GS_ROWS_DEFAULT;
+}
+
+bool guided_set_rows(int dev, int rows) {
+    if (dev < 0 || dev >= 64 || rows < 16 || rows > 4096) return false;
+    g_seg_rows[dev].store(rows);
+    return true;
+}
+
+static int current_device() {
+    int d = 0;
+    cudaGetDevice(&d);
+    return d;
 }
 
 // 5-tap Gaussian fallback: halo 2
@@ -470,14 +456,14 @@ __device__ __forceinline__ void gauss_body(const TransferParams& p, int bx, int 
     }
 }
 
-__global__ void __launch_bounds__(SP_THREADS) k_guided_transfer(SpArgs args) {
+__global__ void __launch_bounds__(GS_THREADS) k_guided_transfer(SpArgs args) {
     guided_body(args.p, blockIdx.x, blockIdx.y);
 }
 __global__ void __launch_bounds__(SP_THREADS) k_gauss_transfer(SpArgs args) {
     gauss_body(args.p, blockIdx.x, blockIdx.y);
 }
 // batched: task = one stream (edge-aware and Gaussian streams in separate launches)
-__global__ void __launch_bounds__(SP_THREADS)
+__global__ void __launch_bounds__(GS_THREADS)
     k_guided_transfer_multi(const TransferParams* __restrict__ ps, const int* __restrict__ map) {
     const TaskBlock t = task_block(map, blockIdx.x);
     guided_body(ps[t.task], t.x, t.y);
@@ -500,17 +486,27 @@ __global__ void k_passthrough(SpArgs args) {
 }
 
 cudaError_t spatial_prepare_device() {
-    cudaError_t e = cudaFuncSetAttribute(k_guided_transfer, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sizeof(GuidedSmem));
+    // the sweep's rings are static shared memory; prefer shared memory over L1
+    cudaError_t e = cudaFuncSetAttribute(k_guided_transfer, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         cudaSharedmemCarveoutMaxShared);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_guided_transfer_multi, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sizeof(GuidedSmem));
+        e = cudaFuncSetAttribute(k_guided_transfer_multi, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
     return e;
 }
 
-unsigned transfer_grid(const TransferParams& p, unsigned& gx, unsigned& gy) {
-    gx = (unsigned)((p.w + TS - 1) / TS);
-    gy = (unsigned)((p.h + TS - 1) / TS);
+// guided filter: blocks of GS_WARPS strips x one segment of seg_rows rows
+// (seg_rows filled from the device's setting when 0); Gaussian: 32x32 tiles
+unsigned transfer_grid(TransferParams& p, unsigned& gx, unsigned& gy) {
+    if (p.edge_aware) {
+        if (p.seg_rows <= 0) p.seg_rows = guided_rows(current_device());
+        const int strips = (p.w + GS_OUT - 1) / GS_OUT;
+        gx = (unsigned)((strips + GS_WARPS - 1) / GS_WARPS);
+        gy = (unsigned)((p.h + p.seg_rows - 1) / p.seg_rows);
+    } else {
+        gx = (unsigned)((p.w + TS - 1) / TS);
+        gy = (unsigned)((p.h + TS - 1) / TS);
+    }
     return gx * gy;
 }
 
@@ -518,16 +514,18 @@ cudaError_t launch_transfer_multi(int edge_aware, const TransferParams* d_params
                                   unsigned blocks, cudaStream_t st) {
     if (blocks == 0) return cudaSuccess;
     if (edge_aware)
-        k_guided_transfer_multi<<<blocks, SP_THREADS, sizeof(GuidedSmem), st>>>(d_params, d_map);
+        k_guided_transfer_multi<<<blocks, GS_THREADS, 0, st>>>(d_params, d_map);
     else
         k_gauss_transfer_multi<<<blocks, SP_THREADS, 0, st>>>(d_params, d_map);
     return cudaGetLastError();
 }
 
-cudaError_t launch_transfer(const TransferParams& p, cudaStream_t st) {
-    SpArgs a{p};
-    dim3 grid((p.w + TS - 1) / TS, (p.h + TS - 1) / TS);
-    if (p.edge_aware) k_guided_transfer<<<grid, SP_THREADS, sizeof(GuidedSmem), st>>>(a);
+cudaError_t launch_transfer(const TransferParams& p0, cudaStream_t st) {
+    SpArgs a{p0};
+    unsigned gx, gy;
+    transfer_grid(a.p, gx, gy);
+    dim3 grid(gx, gy);
+    if (a.p.edge_aware) k_guided_transfer<<<grid, GS_THREADS, 0, st>>>(a);
     else k_gauss_transfer<<<grid, SP_THREADS, 0, st>>>(a);
     return cudaGetLastError();
 }
