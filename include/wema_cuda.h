@@ -181,19 +181,25 @@ int wema_cuda_batch_tick(wema_cuda_batch *b, const int *ids, const void *const *
                          void *const *d_out_u8, int n, void *wait_event, void *done_event);
 int wema_cuda_batch_sync(wema_cuda_batch *b);
 /* The same tick with HOST frames (RGB24; pin them, e.g. with cudaHostAlloc,
- * for the copies to overlap): each stream's frame is copied into one of two
- * device staging sets the batch keeps per stream, the tick runs, the output
- * is copied back - so tick i's outputs go out while tick i+1's inputs come in
- * and it runs (the reference's async_io.c double buffering, on copy
- * engines; a tick's copies in start once the previous tick has finished).  Asynchronous: the copies in wait for
- * wait_event (may be NULL); a host buffer may be reused once done_event (may
- * be NULL) has completed, or after wema_cuda_batch_sync. */
+ * for the copies to overlap): the tick's frames are copied into one of two
+ * device staging sets the batch keeps (each a pair of arenas holding the
+ * tick's frames back to back), the tick runs, the outputs are copied back -
+ * so tick i's outputs go out while tick i+1's inputs come in and tick i runs
+ * (the reference's async_io.c double buffering, on copy engines).  Frames
+ * that lie back to back in host memory (in `ids` order) move in one copy;
+ * many small copies in both directions at once run well below the host
+ * link's rate.  Asynchronous: the copies in wait for wait_event (may be NULL)
+ * and for the staging set's previous tick; a host buffer may be reused once
+ * done_event (may be NULL) has completed, or after wema_cuda_batch_sync. */
 int wema_cuda_batch_tick_host(wema_cuda_batch *b, const int *ids, const void *const *h_in_u8,
                               void *const *h_out_u8, int n, void *wait_event, void *done_event);
 /* Per-stage device timing of the batched ticks (CUDA events on each stage's
  * stream, the WEMA_CUDA_STAGES order of wema_cuda_stage_times): times_ms[7]
  * receives the milliseconds summed over every timed tick, *ticks their
  * count.  Both wait for the batch. */
+/* enable = 0: a host tick's copies in also wait for the previous tick to
+ * finish (no overlap of copies in with kernels); default 1. */
+int wema_cuda_batch_set_host_overlap(wema_cuda_batch *b, int enable);
 int wema_cuda_batch_set_timing(wema_cuda_batch *b, int enable);
 int wema_cuda_batch_stage_times(wema_cuda_batch *b, double *times_ms, long long *ticks);
 /* Snapshot / restore of one batched stream (as the session calls; a batched
@@ -268,17 +274,23 @@ int wema_cuda_server_drain(wema_cuda_server *srv, int timeout_ms);
 /* reset != 0 starts a new measurement window after filling *out. */
 int wema_cuda_server_stats(wema_cuda_server *srv, int reset, wema_cuda_serve_stats *out);
 
-/* Autotuner (no counterpart in the reference): times the temporal filter's
- * step at 2, 4 and 8 coefficient positions per thread on this device
- * (allocating ~200 MB for the trial and freeing it) and keeps the fastest for
- * every later launch on the device (4, the default, unless another is more
- * than 3% faster); returns it (or -1), and writes the timings
- * to `report` (may be NULL).  Results do not depend on the choice - each
- * position's arithmetic is the same - only speed does.  Until a call, 4.
- * set / get fix or read the choice directly (2, 4 or 8). */
+/* Autotuner (no counterpart in the reference).  On this device it times
+ *   - the temporal filter's step at 2, 4 and 8 coefficient positions per
+ *     thread (a 2^23-position trial plane) and keeps the fastest (4, the
+ *     default, unless another is more than 3% faster);
+ *   - the batched guided filter's sweep at 64, 128 and 256 output rows per
+ *     segment (a 3840x8640 trial frame) and keeps the fastest (128 until then);
+ * allocating ~550 MB for the trials and freeing it.  Every later launch on the
+ * device uses the choices.  Returns the positions per thread (or -1) and
+ * writes the timings to `report` (may be NULL).  Results do not depend on
+ * either choice - each position's and each pixel's arithmetic is the same -
+ * only speed does.  set / get fix or read a choice directly (positions 2, 4
+ * or 8; rows a multiple of 16 in 16..4096). */
 int wema_cuda_autotune(int device, char *report, size_t cap);
 int wema_cuda_set_iir_positions(int device, int positions);
 int wema_cuda_get_iir_positions(int device);
+int wema_cuda_set_guided_rows(int device, int rows);
+int wema_cuda_get_guided_rows(int device);
 
 /* Message of the last failure on this thread ("" if none). */
 const char *wema_cuda_last_error(void);

@@ -51,3 +51,44 @@ def test_autotune_and_choice_independence(torch_cuda):
     with pytest.raises(RuntimeError):
         wc.set_iir_positions(0, 3)
     wc.set_iir_positions(0, before)
+
+
+def test_guided_rows_choice_independence(torch_cuda):
+    """The guided filter's sweep gives the same frames for every segment
+    height (its running sums restart at rows fixed in the frame), batched and
+    per stream, on word-aligned and ragged frames."""
+    torch = torch_cuda
+    assert "guided sweep rows" in wc.autotune(0)[1]
+    before = wc.guided_rows(0)
+    F = 4
+    cfgs = [(640, 480, dict(amp=90.0)), (137, 91, dict(amp=60.0)), (1920, 1080, dict(amp=40.0))]
+    data = [torch.from_numpy(SynthVideo(SynthSpec(w, h, 30.0, 3 + k, [1.1], [0.4], 14.0, 2.0))
+                             .frames(0, F)).cuda() for k, (w, h, _) in enumerate(cfgs)]
+    outs = {}
+    for rows in (16, 48, 128, 256):
+        wc.set_guided_rows(0, rows)
+        b = wc.Batch(device=0, max_streams=len(cfgs))
+        ids = [b.add(w, h, **c) for (w, h, c) in cfgs]
+        got = [[torch.empty((h, w, 3), dtype=torch.uint8, device="cuda") for _ in range(F)]
+               for (w, h, _) in cfgs]
+        for t in range(F):
+            b.tick(ids, [d[t] for d in data], [g[t] for g in got])
+        b.sync()
+        outs[rows] = [[x.cpu().numpy() for x in g] for g in got]
+        b.close()
+    for rows in (16, 48, 256):
+        for k in range(len(cfgs)):
+            for t in range(F):
+                assert np.array_equal(outs[rows][k][t], outs[128][k][t]), f"{rows} rows, stream {k}, frame {t}"
+    # the per-stream path (shorter segments for latency) gives the batched frames
+    for k, (w, h, c) in enumerate(cfgs):
+        s = wc.Session(width=w, height=h, **c)
+        for t in range(F):
+            o = torch.empty((h, w, 3), dtype=torch.uint8, device="cuda")
+            s.process_u8(data[k][t], o)
+            s.sync()
+            assert np.array_equal(o.cpu().numpy(), outs[128][k][t]), f"session, stream {k}, frame {t}"
+        s.close()
+    with pytest.raises(RuntimeError):
+        wc.set_guided_rows(0, 40)
+    wc.set_guided_rows(0, before)

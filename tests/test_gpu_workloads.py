@@ -180,8 +180,9 @@ def test_fullhd_colour_configuration(oracle, torch_cuda):
         ref = oracle.float_to_u8(so.process(oracle.u8_to_float(u8[t])))
         sg.process_u8(d_in[t], d_out)
         sg.sync()
+        thrs = sg.read(wc.READ_THRESHOLD)          # one per channel
         for ch, code in enumerate((2, 7, 8)):
-            thr = sg.read(wc.READ_THRESHOLD, channel=ch)[0]
+            thr = thrs[ch]
             assert bits(thr) == bits(oracle.threshold(so.get(code, N))), f"frame {t} channel {ch}"
         assert np.array_equal(d_out.cpu().numpy(), ref), f"frame {t}: colour output"
     sg.close()

@@ -103,17 +103,24 @@ public:
     double stage_ms[T_COUNT] = {};
     long long ticks_timed = 0;
 
-    // host-frame ticks: two device staging sets (frames in and out) per stream,
+    // host-frame ticks: two device staging sets, each one arena for a tick's
+    // frames in and one for its frames out (the tick's streams back to back),
     // copies on their own streams, so tick i's outputs go out while tick i+1's
-    // inputs come in and it runs (async_io.c's double buffering, on copy
-    // engines instead of threads)
+    // inputs come in (async_io.c's double buffering, on copy engines instead
+    // of threads).  Host frames that lie back to back move in one copy.
     struct HostSet {
         cudaEvent_t h2d = nullptr, tick = nullptr, d2h = nullptr;
         bool used = false;
+        uint8_t* din = nullptr;
+        uint8_t* dout = nullptr;
+        size_t cap = 0;                 // bytes of each arena
     } hs[2];
     cudaStream_t st_h2d = nullptr, st_d2h = nullptr;
     int hcur = 0;
-    std::vector<std::array<uint8_t*, 4>> hstage;   // by stream id: in0, out0, in1, out1
+    // copies in wait only for their staging set's previous tick (two ticks
+    // back), so they overlap the previous tick's kernels; off: they also wait
+    // for the previous tick to finish
+    bool host_overlap = true;
     int cur = 0;
     long long launches = 0;
     long long ticks = 0;
@@ -123,7 +130,10 @@ public:
     ~Batch() {
         for (cudaStream_t st : {st_main, st_iir, st_xfer, st_h2d, st_d2h})
             if (st) cudaStreamSynchronize(st);
-        for (size_t i = 0; i < hstage.size(); i++) free_stage((int)i);
+        for (HostSet& h : hs) {
+            if (h.din) cudaFree(h.din);
+            if (h.dout) cudaFree(h.dout);
+        }
         for (Session* s : streams) delete s;
         for (Table& t : tb) {
             if (t.host) cudaFreeHost(t.host);
@@ -155,9 +165,12 @@ public:
             return false;
         int lo = 0, hi = 0;
         if (!cuda_ok(cudaDeviceGetStreamPriorityRange(&lo, &hi), "stream priorities")) return false;
-        for (cudaStream_t* st : {&st_main, &st_iir})
-            if (!cuda_ok(cudaStreamCreateWithPriority(st, cudaStreamNonBlocking, hi), "cudaStreamCreate"))
-                return false;
+        // the threshold (main stream) before the filter: its latency-bound
+        // blocks take SMs first and the HBM-bound filter fills the rest
+        const int mid = hi < lo ? hi + 1 : hi;
+        if (!cuda_ok(cudaStreamCreateWithPriority(&st_main, cudaStreamNonBlocking, hi), "cudaStreamCreate") ||
+            !cuda_ok(cudaStreamCreateWithPriority(&st_iir, cudaStreamNonBlocking, mid), "cudaStreamCreate"))
+            return false;
         if (!cuda_ok(cudaStreamCreateWithPriority(&st_xfer, cudaStreamNonBlocking, lo), "cudaStreamCreate"))
             return false;
         for (cudaStream_t* st : {&st_h2d, &st_d2h})
@@ -216,25 +229,10 @@ public:
         return (int)streams.size() - 1;
     }
 
-    // a stream's host-tick staging back to the pool (its copies have completed)
-    void free_stage(int id) {
-        if (id >= (int)hstage.size()) return;
-        for (uint8_t*& p : hstage[id])
-            if (p) {
-                cudaFreeAsync(p, st_main);
-                p = nullptr;
-            }
-    }
-
     // wait = false: the caller knows the stream's last tick has completed
     bool remove(int id, bool wait = true) {
         if (id < 0 || id >= (int)streams.size() || !streams[id]) { set_error("no stream %d", id); return false; }
         if (wait && !sync()) return false;
-        if (id < (int)hstage.size() && hstage[id][0]) {
-            if (!cuda_ok(cudaStreamSynchronize(st_h2d), "sync") || !cuda_ok(cudaStreamSynchronize(st_d2h), "sync"))
-                return false;
-            free_stage(id);
-        }
         delete streams[id];
         streams[id] = nullptr;
         return true;
@@ -282,50 +280,69 @@ public:
     bool tick_host(const int* ids, const uint8_t* const* h_in, uint8_t* const* h_out, int n,
                    cudaEvent_t wait, cudaEvent_t done) {
         HostSet& S = hs[hcur];
-        std::vector<const uint8_t*> din(n);
-        std::vector<uint8_t*> dout(n);
+        std::vector<size_t> off(n + 1, 0);
         for (int k = 0; k < n; k++) {
             const int id = ids[k];
             if (id < 0 || id >= (int)streams.size() || !streams[id]) { set_error("no stream %d", id); return false; }
             if (!h_in[k] || !h_out[k]) { set_error("stream %d: null frame", id); return false; }
-            if ((int)hstage.size() <= id) hstage.resize(id + 1, {nullptr, nullptr, nullptr, nullptr});
             const size_t fb = 3 * (size_t)streams[id]->g.pixels;
-            if (!hstage[id][0]) {
-                // all four staging buffers or none: a partial set is freed
-                std::array<uint8_t*, 4> got{nullptr, nullptr, nullptr, nullptr};
-                for (uint8_t*& p : got)
-                    if (!cuda_ok(cudaMallocAsync((void**)&p, fb, st_h2d), "cudaMallocAsync(host staging)")) {
-                        for (uint8_t* q : got)
-                            if (q) cudaFreeAsync(q, st_h2d);
-                        return false;
-                    }
-                hstage[id] = got;
-            }
-            din[k] = hstage[id][2 * hcur];
-            dout[k] = hstage[id][2 * hcur + 1];
+            off[k + 1] = off[k] + ((fb + 255) & ~(size_t)255);   // 256-byte aligned frames
         }
-        // this set was last used two ticks ago: its tick read the inputs and
-        // its outputs went out before they are overwritten.  The copies in also
-        // wait for the previous tick to finish: overlapping them with that
-        // tick's kernels measured slower here (the two copy directions then
-        // contend on the host link while the kernels run)
+        // this set was last used two ticks ago: its tick has read the inputs and
+        // its outputs have gone out before they are overwritten
         if (S.used && (!cuda_ok(cudaStreamWaitEvent(st_h2d, S.tick, 0), "stream wait") ||
                        !cuda_ok(cudaStreamWaitEvent(st_h2d, S.d2h, 0), "stream wait")))
             return false;
         const HostSet& P = hs[hcur ^ 1];
-        if (P.used && !cuda_ok(cudaStreamWaitEvent(st_h2d, P.tick, 0), "stream wait")) return false;
+        if (!host_overlap && P.used && !cuda_ok(cudaStreamWaitEvent(st_h2d, P.tick, 0), "stream wait"))
+            return false;
         if (wait && !cuda_ok(cudaStreamWaitEvent(st_h2d, wait, 0), "stream wait")) return false;
-        for (int k = 0; k < n; k++)
-            if (!cuda_ok(cudaMemcpyAsync((void*)din[k], h_in[k], 3 * (size_t)streams[ids[k]]->g.pixels,
-                                         cudaMemcpyHostToDevice, st_h2d), "copy in"))
+        if (off[n] > S.cap) {                  // grow the set's arenas, in stream order after its last use
+            if (S.din) cudaFreeAsync(S.din, st_h2d);
+            if (S.dout) cudaFreeAsync(S.dout, st_h2d);
+            S.din = S.dout = nullptr;
+            S.cap = 0;
+            if (!cuda_ok(cudaMallocAsync((void**)&S.din, off[n], st_h2d), "cudaMallocAsync(host staging)"))
                 return false;
+            if (!cuda_ok(cudaMallocAsync((void**)&S.dout, off[n], st_h2d), "cudaMallocAsync(host staging)")) {
+                cudaFreeAsync(S.din, st_h2d);
+                S.din = nullptr;
+                return false;
+            }
+            S.cap = off[n];
+        }
+        std::vector<const uint8_t*> din(n);
+        std::vector<uint8_t*> dout(n);
+        for (int k = 0; k < n; k++) {
+            din[k] = S.din + off[k];
+            dout[k] = S.dout + off[k];
+        }
+        // runs of frames contiguous on both sides move as one copy
+        auto copies = [&](bool in, cudaStream_t st) {
+            for (int k = 0; k < n;) {
+                const int k0 = k;
+                size_t len = 3 * (size_t)streams[ids[k]]->g.pixels;
+                // frame k+1 joins while it follows the run directly in the arena (no
+                // alignment gap) and in host memory
+                while (k + 1 < n && off[k + 1] - off[k0] == len &&
+                       (in ? h_in[k + 1] == h_in[k0] + len : h_out[k + 1] == h_out[k0] + len)) {
+                    k++;
+                    len += 3 * (size_t)streams[ids[k]]->g.pixels;
+                }
+                const bool ok = in ? cuda_ok(cudaMemcpyAsync((void*)din[k0], h_in[k0], len, cudaMemcpyHostToDevice, st),
+                                             "copy in")
+                                   : cuda_ok(cudaMemcpyAsync(h_out[k0], dout[k0], len, cudaMemcpyDeviceToHost, st),
+                                             "copy out");
+                if (!ok) return false;
+                k++;
+            }
+            return true;
+        };
+        if (!copies(true, st_h2d)) return false;
         if (!cuda_ok(cudaEventRecord(S.h2d, st_h2d), "event record")) return false;
         if (!tick(ids, din.data(), dout.data(), n, S.h2d, S.tick)) return false;
         if (!cuda_ok(cudaStreamWaitEvent(st_d2h, S.tick, 0), "stream wait")) return false;
-        for (int k = 0; k < n; k++)
-            if (!cuda_ok(cudaMemcpyAsync(h_out[k], dout[k], 3 * (size_t)streams[ids[k]]->g.pixels,
-                                         cudaMemcpyDeviceToHost, st_d2h), "copy out"))
-                return false;
+        if (!copies(false, st_d2h)) return false;
         if (!cuda_ok(cudaEventRecord(S.d2h, st_d2h), "event record")) return false;
         if (done && !cuda_ok(cudaEventRecord(done, st_d2h), "event record")) return false;
         S.used = true;
@@ -528,6 +545,11 @@ public:
                 return false;
         if (!mark(T_FWD, 1, st_main)) return false;
         if (!cuda_ok(cudaEventRecord(ev_fwd, st_main), "event record")) return false;
+        if (!mark(T_THR, 0, st_main)) return false;
+        for (int k = L_THR_PART; k <= L_THR_WALK; k++)
+            if (!go(k, [&] { return launch_threshold_multi(k - L_THR_PART, P(k), M(k), L[k].total, st_main); }, "threshold"))
+                return false;
+        if (!mark(T_THR, 1, st_main)) return false;
         if (!cuda_ok(cudaStreamWaitEvent(st_iir, ev_fwd, 0), "stream wait")) return false;
         if (!mark(T_IIR, 0, st_iir)) return false;
         if (!go(L_IIR_PRESEED, [&] { return launch_iir_multi(P(L_IIR_PRESEED), M(L_IIR_PRESEED), L[L_IIR_PRESEED].total, 1, st_iir); }, "IIR preseed"))
@@ -536,11 +558,6 @@ public:
             return false;
         if (!mark(T_IIR, 1, st_iir)) return false;
         if (!cuda_ok(cudaEventRecord(ev_iir, st_iir), "event record")) return false;
-        if (!mark(T_THR, 0, st_main)) return false;
-        for (int k = L_THR_PART; k <= L_THR_WALK; k++)
-            if (!go(k, [&] { return launch_threshold_multi(k - L_THR_PART, P(k), M(k), L[k].total, st_main); }, "threshold"))
-                return false;
-        if (!mark(T_THR, 1, st_main)) return false;
         if (!cuda_ok(cudaStreamWaitEvent(st_main, ev_iir, 0), "stream wait")) return false;
         // the previous tick's transfer still reads its reconstructed luma
         if (xfer_pending && !cuda_ok(cudaStreamWaitEvent(st_main, ev_xfer, 0), "stream wait")) return false;

@@ -154,6 +154,8 @@ unsigned transfer_grid(TransferParams& p, unsigned& gx, unsigned& gy);
 // guided filter rows per sweep segment on a device (default 128)
 int guided_rows(int dev);
 bool guided_set_rows(int dev, int rows);
+// times the sweep at each candidate segment height, keeps the fastest
+cudaError_t guided_autotune(int dev, const int* cand, int nc, float* ms, int* chosen);
 cudaError_t launch_transfer_multi(int edge_aware, const TransferParams* d_params, const int* d_map,
                                   unsigned blocks, cudaStream_t st);
 

@@ -674,13 +674,31 @@ WEMA_API int wema_cuda_session_sync(wema_cuda_session* s) {
 WEMA_API int wema_cuda_autotune(int device, char* report, size_t cap) {
     clear_error();
     if (!ensure_device(device)) return -1;
-    float ms[3] = {0.f, 0.f, 0.f};
-    int chosen = 0;
+    float ms[3] = {0.f, 0.f, 0.f}, gms[3] = {0.f, 0.f, 0.f};
+    const int rows[3] = {64, 128, 256};
+    int chosen = 0, grows = 0;
     if (!cuda_ok(iir_autotune(device, ms, &chosen), "autotune")) return -1;
+    if (!cuda_ok(guided_autotune(device, rows, 3, gms, &grows), "autotune")) return -1;
     if (report && cap)
-        snprintf(report, cap, "iir positions per thread: 2 %.4f ms, 4 %.4f ms, 8 %.4f ms -> %d", ms[0], ms[1],
-                 ms[2], chosen);
+        snprintf(report, cap,
+                 "iir positions per thread: 2 %.4f ms, 4 %.4f ms, 8 %.4f ms -> %d; "
+                 "guided sweep rows per segment: 64 %.4f ms, 128 %.4f ms, 256 %.4f ms -> %d",
+                 ms[0], ms[1], ms[2], chosen, gms[0], gms[1], gms[2], grows);
     return chosen;
+}
+
+WEMA_API int wema_cuda_set_guided_rows(int device, int rows) {
+    clear_error();
+    if (!guided_set_rows(device, rows)) {
+        set_error("rows per segment must be a multiple of 16 in 16..4096");
+        return -1;
+    }
+    return 0;
+}
+
+WEMA_API int wema_cuda_get_guided_rows(int device) {
+    clear_error();
+    return guided_rows(device);
 }
 
 WEMA_API int wema_cuda_set_iir_positions(int device, int positions) {

@@ -17,6 +17,7 @@
 #include "kernels.h"
 #include "multi.cuh"
 
+#include <algorithm>
 #include <atomic>
 
 namespace wema {
@@ -72,8 +73,11 @@ __device__ __forceinline__ void store_rgb(const TransferParams& p, int pi, float
 //   vertical running sums over rows r-12..r-4 give the second round at row
 //   r-8: dy = mean_a * I + mean_b (wema.c:218-229, I read back from the
 //   first ring), added to the row's RGB, clamped and quantised.
-// Running sums restart at every segment, so rounding drift spans at most
-// seg_rows + 16 updates.
+// Every running sum is recomputed from its ring, oldest row first, at rows
+// fixed in the frame (first round: window ends r = 0 mod 16; second round:
+// c1 = 4 mod 16) and slides from there, so a row's sums do not depend on
+// where its segment starts: any seg_rows that is a multiple of 16 gives
+// bit-identical output, and rounding drift spans at most 15 slides.
 constexpr int GR = 4;                   // guided-filter radius (wema.c:314)
 constexpr int GS_IN = 128;              // input columns per strip (4 per lane)
 constexpr int GS_OUT = GS_IN - 4 * GR;  // output columns per strip
@@ -286,6 +290,23 @@ __device__ __forceinline__ void guided_sweep(const TransferParams& p, SweepRing&
                 vII[j] = __fmaf_rn(-ofI[j], ofI[j], __fmaf_rn(I[j], I[j], vII[j]));
                 vIP[j] = __fmaf_rn(-ofI[j], ofP[j], __fmaf_rn(I[j], P[j], vIP[j]));
             }
+            if ((r & 15) == 0) {                    // anchor: the window's sums afresh
+#pragma unroll
+                for (int j = 0; j < 4; j++) vI[j] = vP[j] = vII[j] = vIP[j] = 0.f;
+#pragma unroll
+                for (int k = 1; k <= GS_RING; k++) {   // slots s1+1 .. s1+9: rows r-8 .. r
+                    const int sl = s1 + k < GS_RING ? s1 + k : s1 + k - GS_RING;
+                    const float4 a4 = R.ip[sl][0][lane], b4 = R.ip[sl][1][lane];
+                    const float ai[4] = {a4.x, a4.y, a4.z, a4.w}, bi[4] = {b4.x, b4.y, b4.z, b4.w};
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        vI[j] = __fadd_rn(vI[j], ai[j]);
+                        vP[j] = __fadd_rn(vP[j], bi[j]);
+                        vII[j] = __fmaf_rn(ai[j], ai[j], vII[j]);
+                        vIP[j] = __fmaf_rn(ai[j], bi[j], vIP[j]);
+                    }
+                }
+            }
             s1 = s1 == GS_RING - 1 ? 0 : s1 + 1;
         }
         if (r < ys) return;                         // rows r-8..r not all in yet
@@ -324,6 +345,21 @@ __device__ __forceinline__ void guided_sweep(const TransferParams& p, SweepRing&
             for (int j = 0; j < 4; j++) {
                 uA[j] = __fsub_rn(__fadd_rn(uA[j], hA[j]), ofA[j]);
                 uB[j] = __fsub_rn(__fadd_rn(uB[j], hB[j]), ofB[j]);
+            }
+            if (((r - GR) & 15) == 4) {             // anchor: first-round rows c1-8..c1 afresh
+#pragma unroll
+                for (int j = 0; j < 4; j++) uA[j] = uB[j] = 0.f;
+#pragma unroll
+                for (int k = 1; k <= GS_RING; k++) {
+                    const int sl = s2 + k < GS_RING ? s2 + k : s2 + k - GS_RING;
+                    const float4 a4 = R.ab[sl][0][lane], b4 = R.ab[sl][1][lane];
+                    const float ai[4] = {a4.x, a4.y, a4.z, a4.w}, bi[4] = {b4.x, b4.y, b4.z, b4.w};
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        uA[j] = __fadd_rn(uA[j], ai[j]);
+                        uB[j] = __fadd_rn(uB[j], bi[j]);
+                    }
+                }
             }
             s2 = s2 == GS_RING - 1 ? 0 : s2 + 1;
         }
@@ -380,7 +416,7 @@ int guided_rows(int dev) {
 }
 
 bool guided_set_rows(int dev, int rows) {
-    if (dev < 0 || dev >= 64 || rows < 16 || rows > 4096) return false;
+    if (dev < 0 || dev >= 64 || rows < 16 || rows > 4096 || (rows & 15)) return false;
     g_seg_rows[dev].store(rows);
     return true;
 }
@@ -520,8 +556,19 @@ cudaError_t launch_transfer_multi(int edge_aware, const TransferParams* d_params
     return cudaGetLastError();
 }
 
+// One stream's frame, waited for by the per-stream path, so latency counts:
+// segments short enough that the frame's strips x segments give about eight
+// warps per SM (multiples of 16 rows, at most the batched setting).  The
+// output is the same whatever the segment height.
 cudaError_t launch_transfer(const TransferParams& p0, cudaStream_t st) {
     SpArgs a{p0};
+    if (a.p.edge_aware && a.p.seg_rows <= 0) {
+        const long long strips = (a.p.w + GS_OUT - 1) / GS_OUT;
+        const long long want = 148LL * 8;
+        long long rows = (strips * a.p.h + want - 1) / want;
+        rows = (rows + 15) / 16 * 16;
+        a.p.seg_rows = (int)std::min<long long>(std::max<long long>(rows, 16), guided_rows(current_device()));
+    }
     unsigned gx, gy;
     transfer_grid(a.p, gx, gy);
     dim3 grid(gx, gy);
@@ -537,6 +584,71 @@ cudaError_t launch_passthrough(const TransferParams& p, cudaStream_t st) {
     if (blocks > 148 * 8) blocks = 148 * 8;
     k_passthrough<<<blocks, 256, 0, st>>>(a);
     return cudaGetLastError();
+}
+
+// ---- the autotuner's trial of the segment height: one launch of the sweep
+// over a 3840 x 8640 RGB24 frame (four 2160-row frames' worth of strips and
+// segments, about the batched tick's warp count at 128 rows), each candidate
+// timed over five launches after one warm-up; the fastest is kept.  Outputs
+// do not depend on the choice.
+cudaError_t guided_autotune(int dev, const int* cand, int nc, float* ms, int* chosen) {
+    cudaError_t e = cudaSetDevice(dev);
+    if (e != cudaSuccess) return e;
+    const int W = 3840, H = 4 * 2160;
+    const size_t P = (size_t)W * H;
+    uint8_t *in = nullptr, *out = nullptr;
+    float* gray = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaStream_t st = nullptr;
+    auto done = [&](cudaError_t r) {
+        if (in) cudaFree(in);
+        if (out) cudaFree(out);
+        if (gray) cudaFree(gray);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (st) cudaStreamDestroy(st);
+        return r;
+    };
+    if ((e = cudaMalloc(&in, 3 * P)) != cudaSuccess) return done(e);
+    if ((e = cudaMalloc(&out, 3 * P)) != cudaSuccess) return done(e);
+    if ((e = cudaMalloc(&gray, P * sizeof(float))) != cudaSuccess) return done(e);
+    if ((e = cudaMemset(in, 0x5a, 3 * P)) != cudaSuccess) return done(e);
+    if ((e = cudaMemset(gray, 0, P * sizeof(float))) != cudaSuccess) return done(e);
+    if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) return done(e);
+    if ((e = cudaEventCreate(&e0)) != cudaSuccess || (e = cudaEventCreate(&e1)) != cudaSuccess) return done(e);
+    if ((e = spatial_prepare_device()) != cudaSuccess) return done(e);
+    int best = guided_rows(dev);
+    float best_ms = 1e30f;
+    for (int k = 0; k < nc; k++) {
+        SpArgs a{};
+        a.p.w = W;
+        a.p.h = H;
+        a.p.vec_end = (long long)P;
+        a.p.src_u8 = in;
+        a.p.gray_out = gray;
+        a.p.out_u8 = out;
+        a.p.edge_aware = 1;
+        a.p.seg_rows = cand[k];
+        unsigned gx, gy;
+        transfer_grid(a.p, gx, gy);
+        for (int rep = 0; rep < 6; rep++) {
+            if (rep == 1 && (e = cudaEventRecord(e0, st)) != cudaSuccess) return done(e);
+            k_guided_transfer<<<dim3(gx, gy), GS_THREADS, 0, st>>>(a);
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return done(e);
+        if ((e = cudaEventRecord(e1, st)) != cudaSuccess) return done(e);
+        if ((e = cudaEventSynchronize(e1)) != cudaSuccess) return done(e);
+        float t = 0.f;
+        if ((e = cudaEventElapsedTime(&t, e0, e1)) != cudaSuccess) return done(e);
+        ms[k] = t / 5.f;
+        if (ms[k] < best_ms) {
+            best_ms = ms[k];
+            best = cand[k];
+        }
+    }
+    guided_set_rows(dev, best);
+    *chosen = best;
+    return done(cudaSuccess);
 }
 
 }  // namespace wema

@@ -305,7 +305,10 @@ __device__ __forceinline__ void thr_prefix_body(const ThrArgs& a, int bx, int by
 // order of summation is free: thread ln reads float4s 32k + ln (coalesced),
 // which always hold lanes 4(ln & 1) .. 4(ln & 1) + 3, and the sums meet by
 // shuffles.  A warp that meets an exact half takes lane_monoids.
-constexpr int MON_WARPS = 8;   // sub-chunks per CTA
+// Sub-chunks per CTA.  A warp that meets an exact half takes the much slower
+// lane_monoids; small CTAs free their slot as soon as their own warps finish
+// instead of holding it for the slowest of eight.
+constexpr int MON_WARPS = 2;
 
 __device__ __forceinline__ void sub_candidates(const ThrArgs& a, const ThrScratch& sc,
                                                const ThrGeom& g, long long row, int sub,
@@ -1052,7 +1055,7 @@ __global__ void __launch_bounds__(THR_THREADS) k_thr_partials(ThrArgs a) {
 __global__ void __launch_bounds__(THR_THREADS) k_thr_prefix(ThrArgs a) {
     thr_prefix_body(a, blockIdx.x, blockIdx.y);
 }
-__global__ void __launch_bounds__(32 * MON_WARPS, 2) k_thr_monoids(ThrArgs a) {
+__global__ void __launch_bounds__(32 * MON_WARPS, 16 / MON_WARPS) k_thr_monoids(ThrArgs a) {
     thr_monoids_body(a, blockIdx.x, blockIdx.y);
 }
 __global__ void __launch_bounds__(THR_THREADS, 1) k_thr_walk(ThrArgs a) {
@@ -1069,7 +1072,7 @@ __global__ void __launch_bounds__(THR_THREADS)
     const TaskBlock t = task_block(map, blockIdx.x);
     thr_prefix_body(as[t.task], t.x, t.y);
 }
-__global__ void __launch_bounds__(32 * MON_WARPS, 2)
+__global__ void __launch_bounds__(32 * MON_WARPS, 16 / MON_WARPS)
     k_thr_monoids_multi(const ThrArgs* __restrict__ as, const int* __restrict__ map) {
     const TaskBlock t = task_block(map, blockIdx.x);
     thr_monoids_body(as[t.task], t.x, t.y);

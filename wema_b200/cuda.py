@@ -94,6 +94,8 @@ def lib() -> C.CDLL:
         L.wema_cuda_autotune.argtypes = [i, C.c_char_p, sz]
         L.wema_cuda_set_iir_positions.argtypes = [i, i]
         L.wema_cuda_get_iir_positions.argtypes = [i]
+        L.wema_cuda_set_guided_rows.argtypes = [i, i]
+        L.wema_cuda_get_guided_rows.argtypes = [i]
         L.wema_cuda_batch_tick_host.argtypes = [vp, C.POINTER(i), C.POINTER(vp), C.POINTER(vp), i, vp, vp]
         L.wema_cuda_session_snapshot_bytes.argtypes = [vp]
         L.wema_cuda_session_snapshot_bytes.restype = sz
@@ -104,6 +106,7 @@ def lib() -> C.CDLL:
         L.wema_cuda_batch_snapshot.argtypes = [vp, i, vp, sz]
         L.wema_cuda_batch_restore.argtypes = [vp, i, vp, sz]
         L.wema_cuda_batch_set_timing.argtypes = [vp, i]
+        L.wema_cuda_batch_set_host_overlap.argtypes = [vp, i]
         L.wema_cuda_batch_stage_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
         L.wema_cuda_batch_stats.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                                             C.POINTER(i)]
@@ -339,6 +342,9 @@ class Batch:
         d = C.c_void_p(done_event.cuda_event) if done_event is not None else None
         _check(lib().wema_cuda_batch_tick_host(self.h, ia, pin, pout, n, w, d), "batch_tick_host")
 
+    def set_host_overlap(self, enable: bool):
+        _check(lib().wema_cuda_batch_set_host_overlap(self.h, int(bool(enable))), "set_host_overlap")
+
     def set_timing(self, enable: bool):
         _check(lib().wema_cuda_batch_set_timing(self.h, int(bool(enable))), "batch_set_timing")
 
@@ -432,8 +438,8 @@ class Server:
 def autotune(device=0):
     """Times the filter step at 2 / 4 / 8 positions per thread and keeps the
     fastest for the device -> (positions, report)."""
-    buf = C.create_string_buffer(256)
-    u = lib().wema_cuda_autotune(int(device), buf, 256)
+    buf = C.create_string_buffer(512)
+    u = lib().wema_cuda_autotune(int(device), buf, 512)
     if u < 0:
         raise RuntimeError(f"autotune failed: {last_error()}")
     return u, buf.value.decode()
@@ -445,3 +451,11 @@ def set_iir_positions(device, positions):
 
 def iir_positions(device=0) -> int:
     return lib().wema_cuda_get_iir_positions(int(device))
+
+
+def set_guided_rows(device, rows):
+    _check(lib().wema_cuda_set_guided_rows(int(device), int(rows)), "set_guided_rows")
+
+
+def guided_rows(device=0) -> int:
+    return lib().wema_cuda_get_guided_rows(int(device))
