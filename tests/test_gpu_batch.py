@@ -232,3 +232,42 @@ def test_batch_tick_host_equals_device(oracle, torch_cuda):
             assert_close(got, want[t], cfg.get("color", False), f"stream {k} frame {t}")
     dev.close()
     hst.close()
+
+
+@pytest.mark.parametrize("overlap", [True, False])
+def test_batch_tick_host_contiguous_frames(torch_cuda, overlap):
+    """Host frames back to back in one pinned arena (the copies coalesce into
+    one per direction, across sizes whose frames are 256-byte multiples and
+    not) give the device ticks' frames, with and without the copies in
+    overlapping the previous tick."""
+    torch = torch_cuda
+    F = 5
+    sel = [(160, 128, dict(amp=50.0)), (320, 240, dict(amp=30.0, f_high=5.0)),
+           (137, 91, dict(amp=60.0, fps=60.0, f_high=8.0)), (96, 80, dict(amp=120.0, color=True))]
+    data = [frames(w, h, F, seed=k + 81, fps=cfg.get("fps", 30.0)) for k, (w, h, cfg) in enumerate(sel)]
+    fb = [3 * w * h for (w, h, _) in sel]
+    offs = np.concatenate([[0], np.cumsum(fb)])
+    arena_in = [torch.empty(int(offs[-1]), dtype=torch.uint8).pin_memory() for _ in range(F)]
+    arena_out = [torch.empty(int(offs[-1]), dtype=torch.uint8).pin_memory() for _ in range(F)]
+    for t in range(F):
+        for k in range(len(sel)):
+            arena_in[t][offs[k]:offs[k + 1]].copy_(torch.from_numpy(data[k][t].reshape(-1)))
+    dev = wc.Batch(device=0, max_streams=4)
+    hst = wc.Batch(device=0, max_streams=4)
+    hst.set_host_overlap(overlap)
+    ids_d = [dev.add(w, h, **cfg) for (w, h, cfg) in sel]
+    ids_h = [hst.add(w, h, **cfg) for (w, h, cfg) in sel]
+    d_in = [torch.from_numpy(u).cuda() for u in data]
+    ref = [[torch.empty((h, w, 3), dtype=torch.uint8, device="cuda") for _ in range(F)] for (w, h, _) in sel]
+    for t in range(F):
+        dev.tick(ids_d, [d[t] for d in d_in], [r[t] for r in ref])
+        hst.tick_host(ids_h, [arena_in[t][offs[k]:offs[k + 1]] for k in range(len(sel))],
+                      [arena_out[t][offs[k]:offs[k + 1]] for k in range(len(sel))])
+    dev.sync()
+    hst.sync()
+    for k, (w, h, _) in enumerate(sel):
+        for t in range(F):
+            got = arena_out[t][offs[k]:offs[k + 1]].numpy().reshape(h, w, 3)
+            assert np.array_equal(got, ref[k][t].cpu().numpy()), f"stream {k} frame {t}"
+    dev.close()
+    hst.close()

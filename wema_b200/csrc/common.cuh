@@ -104,12 +104,30 @@ __device__ __forceinline__ float clamp01(float v) {
     return v > 0.0f ? v : 0.0f;
 }
 
-// float in [0,1] -> u8 the way the reference's frame writer quantises
-// (ffmpeg_io.c:305-310): clamp, v*255, +0.5, truncate; each op rounded alone.
-__device__ __forceinline__ uint8_t quant_u8(float v) {
-    v = clamp01(v);
-    return (uint8_t)__float2uint_rz(__fadd_rn(__fmul_rn(v, 255.0f), 0.5f));
+// u8 -> float: fl(i / 255), as the reference's frame reader converts
+// (ffmpeg_io.c:293).  With x = i / 256 (exact), fma(x, fl(1/255), x) =
+// x * (1 + fl(1/255)) rounded once equals the correctly rounded i / 255 for
+// every i in 0..255 (checked exhaustively in tests/test_u8_exact.py).  x is
+// made without a conversion instruction (those share the narrow XU pipe):
+// the float with bits 0x47000000 | i is 32768 + i/256 exactly (exponent 15,
+// mantissa step 2^-8), and subtracting 32768 is exact.
+__device__ __forceinline__ float byte_of(uint32_t w, int k) {   // byte k of w
+    const float x = __fsub_rn(__uint_as_float(__byte_perm(w, 0x47000000u, 0x7540u | (unsigned)k)), 32768.0f);
+    return __fmaf_rn(x, 1.0f / 255.0f, x);
 }
+__device__ __forceinline__ float u8f(uint32_t i) { return byte_of(i, 0); }
+
+// float in [0,1] -> u8 the way the reference's frame writer quantises
+// (ffmpeg_io.c:305-310): v*255, +0.5, truncate; each op rounded alone.  The
+// truncation without a conversion instruction: y = v*255 + 0.5 lies in
+// [0.5, 255.5], so y + 2^23 rounded down is 2^23 + floor(y), whose low
+// mantissa byte is the result.
+__device__ __forceinline__ uint32_t quant_bits(float v) {
+    const float y = __fadd_rn(__fmul_rn(v, 255.0f), 0.5f);
+    return __float_as_uint(__fadd_rd(y, 8388608.0f));
+}
+// the same after the clamp to [0, 1]
+__device__ __forceinline__ uint8_t quant_u8(float v) { return (uint8_t)(quant_bits(clamp01(v)) & 0xffu); }
 
 // YCbCr -> RGB with clamp (wema.c:80-102)
 __device__ __forceinline__ void ycbcr_to_rgb(float y, float cb, float cr, float& r, float& g, float& b) {

@@ -93,21 +93,16 @@ struct SweepRing {                      // one warp's rings
     float4 ab[GS_RING][2][32];          // horizontal window sums of a, b
 };
 
-// u8 -> float: fl(i / 255), as the reference's frame reader converts
-// (ffmpeg_io.c:293).  With x = i / 256 (exact), fma(x, fl(1/255), x) =
-// x * (1 + fl(1/255)) rounded once equals the correctly rounded i / 255 for
-// every i in 0..255 (checked exhaustively in tests/test_u8_exact.py).
-__device__ __forceinline__ float u8f(uint32_t i) {
-    const float x = __fmul_rn(__uint2float_rn(i), 0.00390625f);
-    return __fmaf_rn(x, 1.0f / 255.0f, x);
-}
-__device__ __forceinline__ float byte_of(uint32_t w, int k) { return u8f((w >> (8 * k)) & 0xffu); }
+// 1/k for the clipped window counts k = 1 .. 2 GR + 1 (index 0 unused),
+// correctly rounded (the compiler's IEEE division)
+__constant__ float c_rcp[2 * GR + 2] = {0.f, 1.f / 1, 1.f / 2, 1.f / 3, 1.f / 4, 1.f / 5,
+                                         1.f / 6, 1.f / 7, 1.f / 8, 1.f / 9};
 
 // 1 / (clipped count of a radius-4 window at coordinate c of a line of n);
 // 0 for c outside the line
 __device__ __forceinline__ float inv_count(int c, int n) {
     if (c < 0 || c >= n) return 0.f;
-    return __frcp_rn((float)(min(c + GR, n - 1) - max(c - GR, 0) + 1));
+    return c_rcp[min(c + GR, n - 1) - max(c - GR, 0) + 1];
 }
 
 // The 9-column window sums centred on a lane's 4 columns: its own 4 values
@@ -207,12 +202,18 @@ __device__ __forceinline__ void put_row(const TransferParams& p, int y, int cx, 
         const uint32_t* q = reinterpret_cast<const uint32_t*>(p.src_u8) + 3 * (pi0 >> 2);
         const uint32_t w[3] = {__ldg(q), __ldg(q + 1), __ldg(q + 2)};
         float v[12];
-        uint32_t ow[3] = {0u, 0u, 0u};
+        uint32_t qb[12];
 #pragma unroll
         for (int c = 0; c < 12; c++) {
-            v[c] = clamp01(__fadd_rn(byte_of(w[c >> 2], c & 3), dy[c / 3]));
-            ow[c >> 2] |= (uint32_t)quant_u8(v[c]) << (8 * (c & 3));
+            // clamp01 of a finite sum: the saturating add
+            v[c] = __saturatef(__fadd_rn(byte_of(w[c >> 2], c & 3), dy[c / 3]));
+            qb[c] = quant_bits(v[c]);
         }
+        uint32_t ow[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++)   // low bytes of four quantised values into one word
+            ow[k] = __byte_perm(__byte_perm(qb[4 * k], qb[4 * k + 1], 0x0040u),
+                                __byte_perm(qb[4 * k + 2], qb[4 * k + 3], 0x0040u), 0x5410u);
         if (p.out_u8) {
             uint32_t* d = reinterpret_cast<uint32_t*>(p.out_u8) + 3 * (pi0 >> 2);
             d[0] = ow[0];
