@@ -891,10 +891,12 @@ def bench_precision(a, rank, world, local):
     t0 = time.perf_counter()
 
     # ---- IIR: FP32 vs FP64 state
+    # keys: False FP32 state, True FP64 state, "h16" FP16 planes (FP32 state)
     sess = {v: wc.Session(width=w, height=h, device=local, state_fp64=v, **band) for v in (False, True)}
+    sess["h16"] = wc.Session(width=w, height=h, device=local, planes_fp16=True, **band)
     ref64 = fp64.Stream64(w, h, coef=c32, **band)
-    rel = {False: [], True: []}
-    absmax = {False: 0.0, True: 0.0}
+    rel = {False: [], True: [], "h16": []}
+    absmax = {False: 0.0, True: 0.0, "h16": 0.0}
     outs = {}
     o = torch.empty((h, w, 3), dtype=torch.uint8, device=dev)
     coef = None
@@ -938,11 +940,13 @@ def bench_precision(a, rank, world, local):
         return {"max_lsb": int(d.max()), "rms_lsb": round(float(np.sqrt((d.astype(float) ** 2).mean())), 5),
                 "frac_gt1": float((d > 1).mean())}
     iir = {}
-    for v, name in ((False, "fp32_state"), (True, "fp64_state")):
-        iir[name] = {"state_bytes_per_position": 32 if v else 16,
+    for v, name in ((False, "fp32_state"), (True, "fp64_state"), ("h16", "fp16_planes")):
+        iir[name] = {"state_bytes_per_position": 32 if v is True else 16,
                      "delta_rel_l2_vs_fp64": {"max": float(max(rel[v])), "last": rel[v][-1]},
                      "delta_max_abs_vs_fp64": absmax[v],
                      "output_vs_fp64": cmp(outs[v], out64), "output_vs_reference": cmp(outs[v], out_ref)}
+    iir["fp16_planes"]["plane_bytes"] = "coefficient, delta, LL and reconstructed planes in FP16 (half the FP32 bytes)"
+    iir["fp16_planes"]["output_vs_fp32_state"] = cmp(outs["h16"], outs[False].astype(int))
     for s in sess.values():
         s.close()
 

@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define WEMA_CUDA_ABI_VERSION 1
+#define WEMA_CUDA_ABI_VERSION 2
 
 typedef struct wema_cuda_session wema_cuda_session;
 
@@ -49,6 +49,15 @@ typedef struct {
     int   ring_fp16;         /* precision variant, window mode: the temporal ring stored
                                 in FP16 (round to nearest), arithmetic in FP32; halves
                                 the ring's bytes (read ws times per position per frame) */
+    int   planes_fp16;       /* precision variant: the pyramid's planes - detail
+                                coefficients, band-passed deltas, LL and reconstructed
+                                planes up to the reconstructed frame - stored in FP16
+                                (round to nearest), arithmetic in FP32; the IIR state
+                                stays FP32.  The threshold is then the FP64 sum of the
+                                FP16 coefficients rounded once, not the reference's
+                                bit-exact FP32 sum: outputs are NOT within the bit-exact /
+                                1-LSB parity bars of the FP32 path (their error against an
+                                FP64 re-evaluation is reported instead).  0: FP32 */
 } wema_cuda_config;
 
 /* Fills *cfg with the reference CLI's defaults for a stream of the given

@@ -68,7 +68,7 @@ struct Launch {
 
 enum {
     L_FWD0_LUMA, L_FWD0_COLOR, L_FWD1, L_FWD2, L_FWD3,
-    L_THR_PART, L_THR_PREFIX, L_THR_MON, L_THR_WALK,
+    L_THR_PART, L_THR_PREFIX, L_THR_MON, L_THR_WALK, L_THR16,
     L_IIR_PRESEED, L_IIR,
     L_INV3, L_INV2, L_INV1, L_INV0_LUMA, L_INV0_COLOR,
     L_XFER_GUIDED, L_XFER_GAUSS,
@@ -390,7 +390,7 @@ public:
         L[L_FWD0_LUMA].reset(sizeof(FwdLevelParams));
         L[L_FWD0_COLOR].reset(sizeof(FwdLevelParams));
         for (int l = 1; l <= 3; l++) L[L_FWD0_COLOR + l].reset(sizeof(FwdLevelParams));
-        for (int k = L_THR_PART; k <= L_THR_WALK; k++) L[k].reset(thr_args_bytes());
+        for (int k = L_THR_PART; k <= L_THR16; k++) L[k].reset(thr_args_bytes());
         L[L_IIR_PRESEED].reset(iir_args_bytes());
         L[L_IIR].reset(iir_args_bytes());
         for (int k = L_INV3; k <= L_INV0_COLOR; k++) L[k].reset(sizeof(InvLevelParams));
@@ -415,11 +415,13 @@ public:
                 if (l == 0) p.src_u8 = in[k];
                 else
                     for (int c = 0; c < nch; c++) p.src_planes[c] = q.ll[c][l - 1];
+                const bool h = S.cfg.planes_fp16;
                 for (int c = 0; c < nch; c++) {
-                    p.coef[c] = q.coef[c] + g.uoff[l];
-                    p.prev[c] = l > 0 ? q.coef[c] + g.uoff[l - 1] : nullptr;
+                    p.coef[c] = plane_at(q.coef[c], g.uoff[l], h);
+                    p.prev[c] = l > 0 ? plane_at(q.coef[c], g.uoff[l - 1], h) : nullptr;
                     p.ll_out[c] = q.ll[c][l];
                 }
+                p.h16 = h;
                 p.prev_n = l > 0 ? g.n[l - 1] : 0;
                 unsigned gx, gy;
                 if (l == 0) {
@@ -433,12 +435,13 @@ public:
             // ---- threshold
             PyrView views[3];
             for (int c = 0; c < nch; c++) views[c] = S.view(0, c);
-            unsigned grids[4][2];
+            unsigned grids[5][2];
             if (!cuda_ok(thr_args_fill(targs.data(), views, nch, S.thr_s, q.thr, q.thr + 4,
                                        S.cfg.threshold_form, S.thr_hist ? 1 : 0, grids),
                          "threshold setup"))
                 return false;
-            for (int st = 0; st < 4; st++) {
+            for (int st = 0; st < 5; st++) {
+                if ((st == 4) != (S.cfg.planes_fp16 != 0)) continue;   // FP16 planes: one kernel
                 if (st < 2 && S.thr_hist) continue;   // partial sums + prefix: first frame only
                 L[L_THR_PART + st].add(targs.data(), grids[st][0], grids[st][1],
                                        grids[st][0] * grids[st][1]);
@@ -463,10 +466,11 @@ public:
                 iq.sh = g.sh[l];
                 iq.n = g.n[l];
                 iq.thr = q.thr;
+                iq.h16 = S.cfg.planes_fp16;
                 for (int c = 0; c < nch; c++) {
                     iq.ll[c] = (l == LV - 1) ? q.ll[c][LV - 1] : q.rec[c][l + 1];
-                    iq.coef[c] = q.coef[c] + g.uoff[l];
-                    iq.delta[c] = q.delta[c] + g.uoff[l];
+                    iq.coef[c] = plane_at(q.coef[c], g.uoff[l], iq.h16);
+                    iq.delta[c] = plane_at(q.delta[c], g.uoff[l], iq.h16);
                     iq.alpha[c] = l == 0 ? q.alpha[c] * 0.5f : q.alpha[c];
                     iq.out_planes[c] = (l > 0 || nch == 1) ? q.rec[c][l] : nullptr;
                 }
@@ -489,6 +493,7 @@ public:
                 tp.gray_out = q.rec[0][0];
                 tp.out_u8 = out[k];
                 tp.edge_aware = S.cfg.edge_aware;
+                tp.h16 = S.cfg.planes_fp16;
                 unsigned gx, gy;
                 const unsigned b = transfer_grid(tp, gx, gy);
                 L[tp.edge_aware ? L_XFER_GUIDED : L_XFER_GAUSS].add(&tp, gx, gy, b);
@@ -546,7 +551,7 @@ public:
         if (!mark(T_FWD, 1, st_main)) return false;
         if (!cuda_ok(cudaEventRecord(ev_fwd, st_main), "event record")) return false;
         if (!mark(T_THR, 0, st_main)) return false;
-        for (int k = L_THR_PART; k <= L_THR_WALK; k++)
+        for (int k = L_THR_PART; k <= L_THR16; k++)
             if (!go(k, [&] { return launch_threshold_multi(k - L_THR_PART, P(k), M(k), L[k].total, st_main); }, "threshold"))
                 return false;
         if (!mark(T_THR, 1, st_main)) return false;

@@ -1,6 +1,7 @@
 // common.cuh - shared definitions for the sm_100a kernels and the host runtime.
 #pragma once
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stddef.h>
@@ -97,6 +98,24 @@ __device__ __forceinline__ void ycbcr_tail(float r, float g, float b, float& y, 
     y = luma_tail(r, g, b);
     cb = __fadd_rn(__fmaf_rn(-g, 0.331f, __fmul_rn(b, 0.5f)), __fmaf_rn(r, -0.169f, 0.5f));
     cr = __fmaf_rn(__fadd_rn(r, 1.0f), 0.5f, -__fmaf_rn(g, 0.419f, __fmul_rn(b, 0.081f)));
+}
+
+// Pyramid planes are FP32, or FP16 in the planes_fp16 precision variant
+// (arithmetic stays FP32): an element of plane p at index i, with the
+// storage type given by h (uniform over a launch).  Host-side pointers to
+// FP16 planes keep the float* type; plane_at() offsets them by elements.
+__device__ __forceinline__ float pl_ld(const float* p, long long i, bool h) {
+    return h ? __half2float(__ldg(reinterpret_cast<const __half*>(p) + i)) : __ldg(p + i);
+}
+__device__ __forceinline__ void pl_st(float* p, long long i, float v, bool h) {
+    if (h) reinterpret_cast<__half*>(p)[i] = __float2half_rn(v);
+    else p[i] = v;
+}
+__host__ __device__ inline float* plane_at(float* p, long long i, bool h) {
+    return p ? (h ? reinterpret_cast<float*>(reinterpret_cast<__half*>(p) + i) : p + i) : nullptr;
+}
+__host__ __device__ inline const float* plane_at(const float* p, long long i, bool h) {
+    return p ? (h ? reinterpret_cast<const float*>(reinterpret_cast<const __half*>(p) + i) : p + i) : nullptr;
 }
 
 __device__ __forceinline__ float clamp01(float v) {

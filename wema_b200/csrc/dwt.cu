@@ -139,9 +139,9 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
 #pragma unroll
         for (int r = 0; r < RPW; r++) {
             const int ly = warp + r * NWARP;
-            const float* src = p.src_planes[ch0] + (ry0 + ly) * iw + rx0;
-            v[r][0] = (ly < RH && lane < RW) ? src[lane] : 0.0f;
-            v[r][1] = (ly < RH && lane + 32 < RW) ? src[lane + 32] : 0.0f;
+            const int row0 = (ry0 + ly) * iw + rx0;
+            v[r][0] = (ly < RH && lane < RW) ? pl_ld(p.src_planes[ch0], row0 + lane, p.h16) : 0.0f;
+            v[r][1] = (ly < RH && lane + 32 < RW) ? pl_ld(p.src_planes[ch0], row0 + lane + 32, p.h16) : 0.0f;
         }
 #pragma unroll
         for (int r = 0; r < RPW; r++) {
@@ -299,11 +299,13 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
             const int j = py0 + jj, ry = qy0 + jj;
             const int o = j * sw + i;
             const bool hy = 2 * j + 1 < ih;
-            ll[o] = pl[ry * RS];
-            bands[o] = hy ? pl[(32 + ry) * RS] : (prev ? prev[o] : 0.0f);                        // LH
-            bands[n + o] = (hx && hy) ? pl[(32 + ry) * RS + ODD_COL]
-                                      : (prev ? prev[pn + o] : 0.0f);                          // HH
-            bands[2 * n + o] = hx ? pl[ry * RS + ODD_COL] : (prev ? prev[2 * pn + o] : 0.0f);  // HL
+            const bool h = p.h16;
+            pl_st(ll, o, pl[ry * RS], h);
+            pl_st(bands, o, hy ? pl[(32 + ry) * RS] : (prev ? pl_ld(prev, o, h) : 0.0f), h);         // LH
+            pl_st(bands, n + o, (hx && hy) ? pl[(32 + ry) * RS + ODD_COL]
+                                           : (prev ? pl_ld(prev, pn + o, h) : 0.0f), h);           // HH
+            pl_st(bands, 2 * n + o, hx ? pl[ry * RS + ODD_COL] : (prev ? pl_ld(prev, 2 * pn + o, h) : 0.0f),
+                  h);                                                                              // HL
         }
     }
 }
@@ -336,16 +338,16 @@ __device__ __forceinline__ void dwt_inv_body(const InvLevelParams& p, int bx, in
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const int boff = q == 1 ? 2 * n : (q == 2 ? 0 : n);   // HL 2, LH 0, HH 1
-            const float* src = q == 0 ? p.ll[ch] : p.coef[ch] + boff;
-            const float* dsrc = p.delta[ch] + boff;
+            const float* src = q == 0 ? p.ll[ch] : plane_at(p.coef[ch], boff, p.h16);
+            const float* dsrc = plane_at(p.delta[ch], boff, p.h16);
             const bool okx = 2 * lane + (q & 1) < RW;
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 const int qy = warp + NWARP * u;
                 const bool ok = okx && 2 * qy + (q >> 1) < RH;
                 const int o = o0 + qy * sw;
-                xv[cc][q][u] = ok ? __ldg(src + o) : 0.0f;
-                if (q != 0) dv[cc][q - 1][u] = ok ? __ldg(dsrc + o) : 0.0f;
+                xv[cc][q][u] = ok ? pl_ld(src, o, p.h16) : 0.0f;
+                if (q != 0) dv[cc][q - 1][u] = ok ? pl_ld(dsrc, o, p.h16) : 0.0f;
             }
         }
     }
@@ -416,15 +418,15 @@ __device__ __forceinline__ void dwt_inv_body(const InvLevelParams& p, int bx, in
             const int idx = pr + pcol(lx);
             if (OUT == kOutPlanes) {
 #pragma unroll
-                for (int cc = 0; cc < C; cc++) p.out_planes[c0 + cc][pi] = planes[cc * PLANE + idx];
+                for (int cc = 0; cc < C; cc++) pl_st(p.out_planes[c0 + cc], pi, planes[cc * PLANE + idx], p.h16);
             } else {
                 const float y = planes[idx];
                 const float cb = planes[(C > 1 ? PLANE : 0) + idx];
                 const float cr = planes[(C > 2 ? 2 * PLANE : 0) + idx];
                 if (p.out_planes[0]) {
-                    p.out_planes[0][pi] = y;
-                    p.out_planes[1][pi] = cb;
-                    p.out_planes[2][pi] = cr;
+                    pl_st(p.out_planes[0], pi, y, p.h16);
+                    pl_st(p.out_planes[1], pi, cb, p.h16);
+                    pl_st(p.out_planes[2], pi, cr, p.h16);
                 }
                 float r, g, b;
                 ycbcr_to_rgb(y, cb, cr, r, g, b);

@@ -95,7 +95,7 @@ __device__ __forceinline__ void iir_preseed_body(const IirDev& a, int block, int
     const long long pu = a.p.uoff[a.p.levels];
     for (long long u = block * (long long)IIR_THREADS + threadIdx.x; u < pu;
          u += (long long)nblocks * IIR_THREADS) {
-        const float x = a.coef[u];
+        const float x = pl_ld(a.coef, u, a.p.h16);
         if (a.fp64) {
             double2* s = static_cast<double2*>(a.state) + 2 * u;
             double2 hp = s[0], lp = s[1];
@@ -129,7 +129,7 @@ __device__ __forceinline__ void iir_body64(const IirDev& a, int block, int nbloc
         for (int j = 0; j < U; j++) {
             const long long u = u0 + j * B;
             if (u < pu) {
-                x[j] = __ldg(coef + u);
+                x[j] = pl_ld(coef, u, a.p.h16);
                 hp[j] = __ldcs(state + 2 * u);
                 lp[j] = __ldcs(state + 2 * u + 1);
             }
@@ -138,7 +138,7 @@ __device__ __forceinline__ void iir_body64(const IirDev& a, int block, int nbloc
         for (int j = 0; j < U; j++) {
             const long long u = u0 + j * B;
             if (u < pu) {
-                dout[u] = cascade64(a.p.c, hp[j], lp[j], x[j]);
+                pl_st(dout, u, cascade64(a.p.c, hp[j], lp[j], x[j]), a.p.h16);
                 __stcs(state + 2 * u, hp[j]);
                 __stcs(state + 2 * u + 1, lp[j]);
             }
@@ -164,7 +164,7 @@ __device__ __forceinline__ void iir_body(const IirDev& a, int block, int nblocks
         for (int j = 0; j < U; j++) {
             const long long u = u0 + j * B;
             if (u < pu) {
-                x[j] = __ldg(coef + u);
+                x[j] = pl_ld(coef, u, a.p.h16);
                 st[j] = __ldcs(state + u);          // touched once per frame: evict first
             }
         }
@@ -174,7 +174,7 @@ __device__ __forceinline__ void iir_body(const IirDev& a, int block, int nblocks
             if (u < pu) {
                 bool tail;
                 level_of(a.p, u, tail);
-                dout[u] = cascade(a.p.c, st[j], x[j], tail);
+                pl_st(dout, u, cascade(a.p.c, st[j], x[j], tail), a.p.h16);
                 __stcs(state + u, st[j]);
             }
         }
@@ -233,8 +233,8 @@ __global__ void __launch_bounds__(IIR_THREADS) k_amplify(IirDev a) {
          u += (long long)gridDim.x * IIR_THREADS) {
         bool tail;
         const int l = level_of(a.p, u, tail);
-        const float x = a.coef[u];
-        a.amplified[u] = fabsf(x) > thr ? __fmaf_rn(a.delta_out[u], l == 0 ? alpha0 : a.alpha, x) : x;
+        const float x = pl_ld(a.coef, u, a.p.h16);
+        a.amplified[u] = fabsf(x) > thr ? __fmaf_rn(pl_ld(a.delta_out, u, a.p.h16), l == 0 ? alpha0 : a.alpha, x) : x;
     }
 }
 

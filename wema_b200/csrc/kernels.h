@@ -23,6 +23,7 @@ struct FwdLevelParams {
     const float* prev[3];       // previous level's bands (stale entries), or null
     long long prev_n;
     float* ll_out[3];           // LL (next level's input or the lowpass)
+    int h16;                    // src_planes, coef, prev, ll_out are FP16 planes
 };
 
 struct InvLevelParams {
@@ -37,6 +38,7 @@ struct InvLevelParams {
     float* out_planes[3];       // reconstructed planes (kOutPlanes), optional for kOutRgb
     uint8_t* out_u8;            // kOutRgb: RGB24 output (optional)
     float* out_f32;             // kOutRgb: float RGB output (optional)
+    int h16;                    // ll, coef, delta, out_planes are FP16 planes
 };
 
 cudaError_t dwt_prepare_device();
@@ -70,8 +72,10 @@ void thr_scratch_bind(ThrScratch& s, void* base, long long n6);
 // (sum/N)*0.2, or batch form (0.2/N)*sum); optionally the raw sums.
 // use_hist: predict binades from scratch.hist (written by the previous call on
 // the same geometry) instead of the FP64 partial sums - skips two kernels.
+// h16: the planes are FP16 (planes_fp16 variant): an FP64 sum instead of the
+// bit-exact one (the other arguments as above; use_hist unused).
 cudaError_t launch_threshold(const PyrView* views, int nch, ThrScratch* scratch, float* thr,
-                             float* sums, int batch_form, int use_hist, cudaStream_t st);
+                             float* sums, int batch_form, int use_hist, int h16, cudaStream_t st);
 
 // ---- IIR + amplification (iir.cu) ------------------------------------------
 struct IirParams {
@@ -81,6 +85,7 @@ struct IirParams {
     long long n[4];
     long long off6[5];
     long long simd_end;         // 6-slot positions >= simd_end take the scalar-tail form
+    int h16;                    // coefficient and delta planes are FP16
 };
 // preseed: run `warmup` iterations with the current coefficients as input
 // state: float4 per position, or (fp64) two double2 per position
@@ -106,6 +111,7 @@ struct TransferParams {
     float* out_f32;             // output float RGB (optional)
     int edge_aware;             // 1: guided filter r=4 eps=0.01; 0: 5-tap Gaussian
     int seg_rows;               // guided filter: output rows per sweep segment (0: the device's)
+    int h16;                    // gray_out is an FP16 plane (planes_fp16)
 };
 cudaError_t launch_transfer(const TransferParams& p, cudaStream_t st);
 cudaError_t spatial_prepare_device();
@@ -119,9 +125,12 @@ struct WindowParams {
     int ws, head;               // window size, ring slot of the oldest sample
     int bilateral;
     int fp16;                   // ring elements are __half (else float)
+    int h16;                    // the delta plane written is FP16 (planes_fp16)
     float time_w[256];
 };
-cudaError_t launch_ring_push(const float* coef, void* ring, int fp16, long long pu, int slot, cudaStream_t st);
+// coef: FP16 plane when h16 (planes_fp16); ring: __half elements when fp16 (ring_fp16)
+cudaError_t launch_ring_push(const float* coef, int h16, void* ring, int fp16, long long pu, int slot,
+                             cudaStream_t st);
 cudaError_t launch_window(const WindowParams& wp, const void* ring, float* delta,
                           cudaStream_t st);
 
@@ -137,7 +146,7 @@ cudaError_t launch_dwt_inv_multi(int channels, int out_mode, const InvLevelParam
 size_t thr_args_bytes();
 // grids[stage] = {x, y} for stage 0 partials, 1 prefix, 2 monoids, 3 walk
 cudaError_t thr_args_fill(void* dst, const PyrView* views, int nch, const ThrScratch* scratch,
-                          float* thr, float* sums, int batch_form, int use_hist, unsigned grids[4][2]);
+                          float* thr, float* sums, int batch_form, int use_hist, unsigned grids[5][2]);
 cudaError_t launch_threshold_multi(int stage, const void* d_args, const int* d_map, unsigned blocks,
                                    cudaStream_t st);
 size_t iir_args_bytes();

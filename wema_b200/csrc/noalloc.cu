@@ -88,7 +88,7 @@ extern "C" __attribute__((visibility("default"))) int wema_cuda_threshold_flat_n
     v.coef = d_x;
     v.levels = 0;
     v.off6[0] = (long long)n;
-    return cuda_ok(launch_threshold(&v, 1, &ts, d_thr, d_sum, threshold_form, 0,
+    return cuda_ok(launch_threshold(&v, 1, &ts, d_thr, d_sum, threshold_form, 0, 0,
                                     (cudaStream_t)cuda_stream),
                    "threshold")
                ? 0

@@ -632,7 +632,7 @@ WEMA_API void coeff_amplify(const float* delta_coeff, const float* orig_coeff, f
     v.coef = d_orig;
     v.levels = 0;
     v.off6[0] = total;
-    if (!cuda_ok(launch_threshold(&v, 1, &ts, d_thr, nullptr, WEMA_CUDA_THR_SINGLE, 0, st), "threshold"))
+    if (!cuda_ok(launch_threshold(&v, 1, &ts, d_thr, nullptr, WEMA_CUDA_THR_SINGLE, 0, 0, st), "threshold"))
         return;
     IirParams ip{};
     ip.levels = coeffs->num_levels;

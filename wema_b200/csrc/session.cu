@@ -120,12 +120,15 @@ static void layout(Arena& A, Session& s) {
     const long long n6 = g.off6[g.levels];
     for (int b = 0; b < s.nslots; b++) {
         Slot& q = s.slot[b];
+        // pyramid planes: FP32, or FP16 in the planes_fp16 variant (float* kept)
+        auto plane = [&](long long n) {
+            return s.cfg.planes_fp16 ? reinterpret_cast<float*>(A.take<uint16_t>(n)) : A.take<float>(n);
+        };
         for (int c = 0; c < s.nch; c++) {
-            q.coef[c] = A.take<float>(pu);
-            q.delta[c] = A.take<float>(pu);
-            for (int l = 0; l < g.levels; l++) q.ll[c][l] = A.take<float>(g.n[l]);
-            for (int l = 0; l < g.levels; l++)
-                q.rec[c][l] = A.take<float>((size_t)g.in_w[l] * g.in_h[l]);
+            q.coef[c] = plane(pu);
+            q.delta[c] = plane(pu);
+            for (int l = 0; l < g.levels; l++) q.ll[c][l] = plane(g.n[l]);
+            for (int l = 0; l < g.levels; l++) q.rec[c][l] = plane((long long)g.in_w[l] * g.in_h[l]);
             q.gray_in[c] = A.take<float>(g.pixels);
         }
         q.thr = A.take<float>(8);
@@ -150,6 +153,7 @@ static bool valid_config(const wema_cuda_config& c) {
     }
     if (c.iir_state_fp64 != 0 && c.iir_state_fp64 != 1) { set_error("iir_state_fp64 must be 0 or 1"); return false; }
     if (c.ring_fp16 != 0 && c.ring_fp16 != 1) { set_error("ring_fp16 must be 0 or 1"); return false; }
+    if (c.planes_fp16 != 0 && c.planes_fp16 != 1) { set_error("planes_fp16 must be 0 or 1"); return false; }
     return true;
 }
 
@@ -215,6 +219,7 @@ bool Session::init(const wema_cuda_config& c, int ns, cudaStream_t alloc_stream)
     for (int l = 0; l <= g.levels; l++) { ip.uoff[l] = g.uoff[l]; ip.off6[l] = g.off6[l]; }
     for (int l = 0; l < g.levels; l++) ip.n[l] = g.n[l];
     ip.simd_end = g.off6[g.levels] & ~15LL;
+    ip.h16 = c.planes_fp16;
 
     Arena A;
     layout(A, *this);
@@ -322,12 +327,14 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
         } else {
             for (int c = 0; c < nch; c++) p.src_planes[c] = q.ll[c][l - 1];
         }
+        const bool h = cfg.planes_fp16;
         for (int c = 0; c < nch; c++) {
-            p.coef[c] = q.coef[c] + g.uoff[l];
-            p.prev[c] = l > 0 ? q.coef[c] + g.uoff[l - 1] : nullptr;
+            p.coef[c] = plane_at(q.coef[c], g.uoff[l], h);
+            p.prev[c] = l > 0 ? plane_at(q.coef[c], g.uoff[l - 1], h) : nullptr;
             p.ll_out[c] = q.ll[c][l];
         }
         p.prev_n = l > 0 ? g.n[l - 1] : 0;
+        p.h16 = h;
         if (!cuda_ok(launch_dwt_fwd(mode, nch, p, s_fwd), "forward DWT")) return false;
         launches++;
         if (l == 0) {
@@ -360,7 +367,8 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
         launches += nch;
     } else {
         for (int c = 0; c < nch; c++)
-            if (!cuda_ok(launch_ring_push(q.coef[c], ring[c], cfg.ring_fp16, pu, head, s_tmp), "ring push"))
+            if (!cuda_ok(launch_ring_push(q.coef[c], cfg.planes_fp16, ring[c], cfg.ring_fp16, pu, head, s_tmp),
+                         "ring push"))
                 return false;
         launches += nch;
         head = (head + 1) % cfg.temporal_window;
@@ -375,6 +383,7 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
             wp.head = head;   // oldest sample (temporal_filter.c:221)
             wp.bilateral = cfg.bilateral_temp;
             wp.fp16 = cfg.ring_fp16;
+            wp.h16 = cfg.planes_fp16;
             const int ws = cfg.temporal_window, center = ws / 2;
             const float ts = (float)ws * 0.15f;
             const float inv2 = 0.5f / (ts * ts);
@@ -400,10 +409,11 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
         for (int c = 0; c < nch; c++) ts[c] = thr_s[c];
         mark(2 * ST_THR, s_thr);
         if (!cuda_ok(launch_threshold(views, nch, ts, q.thr, q.thr + 4, cfg.threshold_form,
-                                      thr_hist ? 1 : 0, s_thr),
+                                      thr_hist ? 1 : 0, cfg.planes_fp16, s_thr),
                      "threshold"))
             return false;
-        launches += thr_hist ? 2 : 4;   // monoids + walk; partial sums + prefix without history
+        // monoids + walk; partial sums + prefix without history; one launch over FP16 planes
+        launches += cfg.planes_fp16 ? 1 : (thr_hist ? 2 : 4);
         thr_hist = true;
         mark(2 * ST_THR + 1, s_thr);
         if (!cuda_ok(cudaEventRecord(q.ev_thr, s_thr), "event record")) return false;
@@ -433,10 +443,12 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
             iq.sh = g.sh[l];
             iq.n = g.n[l];
             iq.thr = q.thr;
+            const bool h = cfg.planes_fp16;
+            iq.h16 = h;
             for (int c = 0; c < nch; c++) {
                 iq.ll[c] = (l == L - 1) ? q.ll[c][L - 1] : q.rec[c][l + 1];
-                iq.coef[c] = q.coef[c] + g.uoff[l];
-                iq.delta[c] = q.delta[c] + g.uoff[l];
+                iq.coef[c] = plane_at(q.coef[c], g.uoff[l], h);
+                iq.delta[c] = plane_at(q.delta[c], g.uoff[l], h);
                 iq.alpha[c] = l == 0 ? q.alpha[c] * 0.5f : q.alpha[c];
                 iq.out_planes[c] = (l > 0 || nch == 1 || inspect) ? q.rec[c][l] : nullptr;
             }
@@ -466,6 +478,7 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
             tp.out_u8 = out_u8;
             tp.out_f32 = out_f32;
             tp.edge_aware = cfg.edge_aware;
+            tp.h16 = cfg.planes_fp16;
             if (!cuda_ok(launch_transfer(tp, s_inv), "luma transfer")) return false;
             launches++;
         }
@@ -567,6 +580,23 @@ bool Session::restore(const void* host, size_t bytes) {
         for (int c = 0; c < 3; c++) slot[i].alpha[c] = h.alpha[i][c];
     }
     return true;
+}
+
+// IEEE binary16 bits -> float (exact)
+static float half_bits_to_float(uint16_t h) {
+    const uint32_t sgn = (uint32_t)(h & 0x8000u) << 16;
+    uint32_t e = (h >> 10) & 0x1fu, m = h & 0x3ffu, bits;
+    if (e == 0x1f) bits = sgn | 0x7f800000u | (m << 13);                  // inf / nan
+    else if (e) bits = sgn | ((e + 112u) << 23) | (m << 13);              // normal
+    else if (!m) bits = sgn;                                              // zero
+    else {                                                                // subnormal: renormalise
+        int sh = 0;
+        while (!(m & 0x400u)) { m <<= 1; sh++; }
+        bits = sgn | ((uint32_t)(113 - sh) << 23) | ((m & 0x3ffu) << 13);
+    }
+    float f;
+    memcpy(&f, &bits, sizeof f);
+    return f;
 }
 
 struct wema_cuda_session {
@@ -755,16 +785,24 @@ WEMA_API long wema_cuda_session_read(wema_cuda_session* s, int what, int channel
     const Geom& g = S.g;
     const Slot& q = S.slot[S.last_slot];
     const long long pu = g.uoff[g.levels], n6 = g.off6[g.levels];
-    auto rd = [&](const float* src, size_t n) -> long {
-        if (n > cap) { set_error("buffer too small (%zu needed)", n); return -1; }
-        return cuda_ok(cudaMemcpy(h_dst, src, n * sizeof(float), cudaMemcpyDeviceToHost), "D2H")
-                   ? (long)n : -1;
+    // a device plane into host floats (FP16 pyramid planes converted exactly)
+    auto fetch = [&](float* dst, const float* src, size_t n, bool h) -> bool {
+        if (!h) return cuda_ok(cudaMemcpy(dst, src, n * sizeof(float), cudaMemcpyDeviceToHost), "D2H");
+        std::vector<uint16_t> b(n);
+        if (!cuda_ok(cudaMemcpy(b.data(), src, n * sizeof(uint16_t), cudaMemcpyDeviceToHost), "D2H"))
+            return false;
+        for (size_t i = 0; i < n; i++) dst[i] = half_bits_to_float(b[i]);
+        return true;
     };
-    auto rd6 = [&](const float* src) -> long {
+    const bool h16 = S.cfg.planes_fp16;
+    auto rd = [&](const float* src, size_t n, bool h) -> long {
+        if (n > cap) { set_error("buffer too small (%zu needed)", n); return -1; }
+        return fetch(h_dst, src, n, h) ? (long)n : -1;
+    };
+    auto rd6 = [&](const float* src, bool h) -> long {
         if ((size_t)n6 > cap) { set_error("buffer too small (%lld needed)", n6); return -1; }
         std::vector<float> u(pu);
-        if (!cuda_ok(cudaMemcpy(u.data(), src, pu * sizeof(float), cudaMemcpyDeviceToHost), "D2H"))
-            return -1;
+        if (!fetch(u.data(), src, pu, h)) return -1;
         for (int l = 0; l < g.levels; l++)
             for (int slot = 0; slot < 6; slot++) {
                 const int band = slot < 3 ? slot : 5 - slot;
@@ -778,15 +816,16 @@ WEMA_API long wema_cuda_session_read(wema_cuda_session* s, int what, int channel
         case WEMA_CUDA_READ_GRAY_IN:
         case WEMA_CUDA_READ_GRAY_OUT:
             if (!planes) { set_error("enable wema_cuda_set_inspect before processing"); return -1; }
-            return rd(what == WEMA_CUDA_READ_GRAY_IN ? q.gray_in[channel] : q.rec[channel][0], g.pixels);
-        case WEMA_CUDA_READ_ORIG6: return rd6(q.coef[channel]);
-        case WEMA_CUDA_READ_DELTA6: return rd6(q.delta[channel]);
+            if (what == WEMA_CUDA_READ_GRAY_IN) return rd(q.gray_in[channel], g.pixels, false);
+            return rd(q.rec[channel][0], g.pixels, h16);
+        case WEMA_CUDA_READ_ORIG6: return rd6(q.coef[channel], h16);
+        case WEMA_CUDA_READ_DELTA6: return rd6(q.delta[channel], h16);
         case WEMA_CUDA_READ_AMP6:
             if (!S.materialize_amplified()) return -1;
-            return rd6(S.ampl[channel]);
-        case WEMA_CUDA_READ_LOWPASS: return rd(q.ll[channel][g.levels - 1], g.low_n);
-        case WEMA_CUDA_READ_THRESHOLD: return rd(q.thr, S.nch);
-        case WEMA_CUDA_READ_MAGSUM: return rd(q.thr + 4, S.nch);
+            return rd6(S.ampl[channel], false);
+        case WEMA_CUDA_READ_LOWPASS: return rd(q.ll[channel][g.levels - 1], g.low_n, h16);
+        case WEMA_CUDA_READ_THRESHOLD: return rd(q.thr, S.nch, false);
+        case WEMA_CUDA_READ_MAGSUM: return rd(q.thr + 4, S.nch, false);
     }
     set_error("unknown stage %d", what);
     return -1;
@@ -836,7 +875,7 @@ WEMA_API int wema_cuda_threshold_flat(const float* d_x, size_t n, int threshold_
     v.coef = d_x;
     v.levels = 0;
     v.off6[0] = (long long)n;
-    bool ok = cuda_ok(launch_threshold(&v, 1, &ts, d_thr, d_sum, threshold_form, 0, st), "threshold");
+    bool ok = cuda_ok(launch_threshold(&v, 1, &ts, d_thr, d_sum, threshold_form, 0, 0, st), "threshold");
     cudaFreeAsync(scratch, st);
     return ok ? 0 : -1;
 }

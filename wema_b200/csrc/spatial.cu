@@ -146,7 +146,15 @@ struct RowLoad {
                 w[0] = __ldg(q);
                 w[1] = __ldg(q + 1);
                 w[2] = __ldg(q + 2);
-                g = __ldg(reinterpret_cast<const float4*>(p.gray_out + pi));
+                if (p.h16) {
+                    const uint2 hb = __ldg(reinterpret_cast<const uint2*>(
+                        reinterpret_cast<const __half*>(p.gray_out) + pi));
+                    const float2 lo = __half22float2(*reinterpret_cast<const __half2*>(&hb.x));
+                    const float2 hi = __half22float2(*reinterpret_cast<const __half2*>(&hb.y));
+                    g = make_float4(lo.x, lo.y, hi.x, hi.y);
+                } else {
+                    g = __ldg(reinterpret_cast<const float4*>(p.gray_out + pi));
+                }
             }
         } else {
 #pragma unroll
@@ -154,7 +162,7 @@ struct RowLoad {
                 const int x = cx + j;
                 const bool in = any && x >= 0 && x < p.w;
                 const long long pi = (long long)r * p.w + x;
-                gv[j] = in ? __ldg(p.gray_out + pi) : 0.f;
+                gv[j] = in ? pl_ld(p.gray_out, pi, p.h16) : 0.f;
 #pragma unroll
                 for (int c = 0; c < 3; c++)
                     rgb[3 * j + c] = !in ? 0.f
@@ -451,7 +459,7 @@ __device__ __forceinline__ void gauss_body(const TransferParams& p, int bx, int 
             float r, g, b;
             load_rgb(p, lut, pi, r, g, b);
             const float I = pi < p.vec_end ? luma_vec(r, g, b) : luma_tail(r, g, b);
-            v = __fadd_rn(p.gray_out[pi], -I);
+            v = __fadd_rn(pl_ld(p.gray_out, pi, p.h16), -I);
         }
         P[ly][lx] = v;
     }

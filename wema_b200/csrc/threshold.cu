@@ -40,8 +40,10 @@
 //                   stored monoids or the sequential adds.  The lane that
 //                   finishes last reduces the eight lane sums and divides.
 // Predictions only decide speed, never the result.
-#include <atomic>
 #include <string.h>
+
+#include <algorithm>
+#include <atomic>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -194,15 +196,20 @@ __host__ __device__ inline ThrGeom thr_geom(long long n6) {
     return g;
 }
 
+// entries of each lane-major array: at least T16_MAXBLK (the FP16-plane
+// threshold's per-block partial sums use `part`)
+constexpr int T16_MAXBLK = 1024;
+static size_t thr_per(const ThrGeom& g) { return std::max<size_t>((size_t)g.nsub * LANES, T16_MAXBLK); }
+
 size_t thr_scratch_bytes(long long n6) {
     const ThrGeom g = thr_geom(n6);
-    const size_t per = (size_t)g.nsub * LANES;
+    const size_t per = thr_per(g);
     return per * (2 * sizeof(double) + sizeof(int4) + sizeof(int2) + sizeof(int)) + 256;
 }
 
 void thr_scratch_bind(ThrScratch& s, void* base, long long n6) {
     const ThrGeom g = thr_geom(n6);
-    const size_t per = (size_t)g.nsub * LANES;
+    const size_t per = thr_per(g);
     char* p = (char*)base;
     s.part = (double*)p;    p += per * sizeof(double);
     s.prefix = (double*)p;  p += per * sizeof(double);
@@ -1048,7 +1055,68 @@ __device__ __forceinline__ void thr_walk_body(const ThrArgs& a, int bx, int by) 
     }
 }
 
+// ---- the planes_fp16 precision variant: the threshold of FP16 planes.
+// Not the reference's vectorised FP32 sum: the sum of |x| over the 6-slot
+// array (each unique band twice - slots 3-5 mirror 2-0) in FP64 from
+// per-block partial sums, which the last block to finish adds in block
+// order (the result does not depend on timing), then (S / N6) * 0.2 or
+// (0.2 / N6) * S in FP64, rounded to FP32 once.  Grid: nblk x channels.
+constexpr int T16_THREADS = 256;
+
+__device__ __forceinline__ void thr16_body(const ThrArgs& a, int bx, int by, int nblk) {
+    const int ch = by;
+    const PyrView& v = a.v[ch];
+    const ThrScratch& sc = a.s[ch];
+    const long long pu = v.uoff[v.levels];
+    const __half* x = reinterpret_cast<const __half*>(v.coef);
+    double acc = 0.0;
+    for (long long u = (long long)bx * T16_THREADS + threadIdx.x; u < pu; u += (long long)nblk * T16_THREADS)
+        acc += (double)fabsf(__half2float(x[u]));
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) acc += __shfl_xor_sync(FULL, acc, d);
+    __shared__ double ws[T16_THREADS / 32];
+    __shared__ bool last;
+    const int warp = threadIdx.x >> 5, ln = threadIdx.x & 31;
+    if (ln == 0) ws[warp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = 0.0;
+        for (int w = 0; w < T16_THREADS / 32; w++) b += ws[w];
+        sc.part[bx] = b;
+        __threadfence();
+        last = atomicAdd(sc.counter, 1u) == (unsigned)(nblk - 1);
+    }
+    __syncthreads();
+    if (!last || warp != 0) return;
+    __threadfence();
+    const volatile double* part = sc.part;
+    double t = 0.0;
+    for (int i = ln; i < nblk; i += 32) t += part[i];
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) t += __shfl_xor_sync(FULL, t, d);
+    if (ln == 0) {
+        const double s6 = 2.0 * t, n6 = (double)v.off6[v.levels];
+        a.thr[ch] = (float)(a.batch_form ? (0.2 / n6) * s6 : (s6 / n6) * 0.2);
+        if (a.sums) a.sums[ch] = (float)s6;
+        *sc.counter = 0u;
+    }
+}
+
+static int thr16_blocks(const PyrView& v) {
+    const long long pu = v.uoff[v.levels];
+    const long long b = (pu + 8LL * T16_THREADS - 1) / (8LL * T16_THREADS);
+    return (int)std::min<long long>(std::max<long long>(b, 1), T16_MAXBLK);
+}
+
 // ------------------------------------------------------------- wrappers
+__global__ void __launch_bounds__(T16_THREADS) k_thr16(ThrArgs a, int nblk) {
+    thr16_body(a, blockIdx.x, blockIdx.y, nblk);
+}
+__global__ void __launch_bounds__(T16_THREADS)
+    k_thr16_multi(const ThrArgs* __restrict__ as, const int* __restrict__ map) {
+    const TaskBlock t = task_block(map, blockIdx.x);
+    thr16_body(as[t.task], t.x, t.y, map[map[0] + 2 + t.task]);
+}
 __global__ void __launch_bounds__(THR_THREADS) k_thr_partials(ThrArgs a) {
     thr_partials_body(a, blockIdx.x, blockIdx.y);
 }
@@ -1099,7 +1167,7 @@ cudaError_t thr_prepare_device() {
 }
 
 cudaError_t launch_threshold(const PyrView* views, int nch, ThrScratch* scratch, float* thr,
-                             float* sums, int batch_form, int use_hist, cudaStream_t st) {
+                             float* sums, int batch_form, int use_hist, int h16, cudaStream_t st) {
     if (nch < 1 || nch > 3) return cudaErrorInvalidValue;
     cudaError_t e = thr_prepare_device();
     if (e != cudaSuccess) return e;
@@ -1114,6 +1182,11 @@ cudaError_t launch_threshold(const PyrView* views, int nch, ThrScratch* scratch,
     a.sums = sums;
     a.batch_form = batch_form;
     a.use_hist = use_hist;
+    if (h16) {
+        const int nb = thr16_blocks(views[0]);
+        k_thr16<<<dim3(nb, nch), T16_THREADS, 0, st>>>(a, nb);
+        return cudaGetLastError();
+    }
     if (!use_hist && nsub > 0) {
         k_thr_partials<<<dim3(nsub, nch), THR_THREADS, 0, st>>>(a);
         k_thr_prefix<<<dim3(LANES, nch), THR_THREADS, 0, st>>>(a);
@@ -1127,7 +1200,7 @@ cudaError_t launch_threshold(const PyrView* views, int nch, ThrScratch* scratch,
 size_t thr_args_bytes() { return sizeof(ThrArgs); }
 
 cudaError_t thr_args_fill(void* dst, const PyrView* views, int nch, const ThrScratch* scratch,
-                          float* thr, float* sums, int batch_form, int use_hist, unsigned grids[4][2]) {
+                          float* thr, float* sums, int batch_form, int use_hist, unsigned grids[5][2]) {
     if (nch < 1 || nch > 3) return cudaErrorInvalidValue;
     ThrArgs a{};
     int nsub = 0;
@@ -1145,7 +1218,8 @@ cudaError_t thr_args_fill(void* dst, const PyrView* views, int nch, const ThrScr
     grids[1][0] = LANES;                                                  // prefix
     grids[2][0] = (unsigned)max((nsub + MON_WARPS - 1) / MON_WARPS, 1);   // monoids
     grids[3][0] = LANES;                                                  // walk
-    for (int k = 0; k < 4; k++) grids[k][1] = (unsigned)nch;
+    grids[4][0] = (unsigned)thr16_blocks(views[0]);                        // FP16 planes
+    for (int k = 0; k < 5; k++) grids[k][1] = (unsigned)nch;
     if (nsub == 0) grids[0][0] = 0;
     return cudaSuccess;
 }
@@ -1161,6 +1235,7 @@ cudaError_t launch_threshold_multi(int stage, const void* d_args, const int* d_m
         case 1: k_thr_prefix_multi<<<blocks, THR_THREADS, 0, st>>>(as, d_map); break;
         case 2: k_thr_monoids_multi<<<blocks, 32 * MON_WARPS, 0, st>>>(as, d_map); break;
         case 3: k_thr_walk_multi<<<blocks, THR_THREADS, sizeof(WalkSmem), st>>>(as, d_map); break;
+        case 4: k_thr16_multi<<<blocks, T16_THREADS, 0, st>>>(as, d_map); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

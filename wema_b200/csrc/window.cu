@@ -32,11 +32,11 @@ __device__ __forceinline__ float get(const float* p) { return *p; }
 __device__ __forceinline__ float get(const __half* p) { return __half2float(*p); }
 
 template <class T>
-__global__ void k_ring_push(const float* coef, T* ring, long long pu, int slot) {
+__global__ void k_ring_push(const float* coef, int h16, T* ring, long long pu, int slot) {
     T* dst = ring + (long long)slot * pu;
     for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < pu;
          u += (long long)gridDim.x * blockDim.x)
-        put(dst + u, coef[u]);
+        put(dst + u, pl_ld(coef, u, h16));
 }
 
 template <class T>
@@ -84,16 +84,16 @@ __global__ void __launch_bounds__(WIN_THREADS) k_window(WinDev<T> a) {
             }
             if (wsum > 1e-8f) d = __fmul_rn(res, __fdiv_rn(1.0f, wsum));
         }
-        a.delta_out[u] = d;
+        pl_st(a.delta_out, u, d, a.w.h16);
     }
 }
 
-cudaError_t launch_ring_push(const float* coef, void* ring, int fp16, long long pu, int slot,
+cudaError_t launch_ring_push(const float* coef, int h16, void* ring, int fp16, long long pu, int slot,
                              cudaStream_t st) {
     long long b = (pu + 255) / 256;
     const int g = (int)(b < 148 * 8 ? (b > 0 ? b : 1) : 148 * 8);
-    if (fp16) k_ring_push<__half><<<g, 256, 0, st>>>(coef, static_cast<__half*>(ring), pu, slot);
-    else k_ring_push<float><<<g, 256, 0, st>>>(coef, static_cast<float*>(ring), pu, slot);
+    if (fp16) k_ring_push<__half><<<g, 256, 0, st>>>(coef, h16, static_cast<__half*>(ring), pu, slot);
+    else k_ring_push<float><<<g, 256, 0, st>>>(coef, h16, static_cast<float*>(ring), pu, slot);
     return cudaGetLastError();
 }
 

@@ -24,7 +24,7 @@ class Config(C.Structure):
                 ("temporal_window", C.c_int), ("edge_aware", C.c_int),
                 ("bilateral_temp", C.c_int), ("color_mode", C.c_int), ("use_iir", C.c_int),
                 ("threshold_form", C.c_int), ("device", C.c_int), ("iir_state_fp64", C.c_int),
-                ("ring_fp16", C.c_int)]
+                ("ring_fp16", C.c_int), ("planes_fp16", C.c_int)]
 
 
 _lib = None
@@ -137,7 +137,8 @@ def _check(rc: int, what: str):
 
 def make_config(width, height, fps=30.0, amp=120.0, f_low=0.5, f_high=None, window=32,
                 edge_aware=True, bilateral=False, color=False, use_iir=True,
-                threshold_form=THR_SINGLE, device=0, state_fp64=False, ring_fp16=False) -> Config:
+                threshold_form=THR_SINGLE, device=0, state_fp64=False, ring_fp16=False,
+                planes_fp16=False) -> Config:
     c = Config()
     lib().wema_cuda_config_default(C.byref(c), int(width), int(height), float(fps))
     c.amp_factor = float(amp)
@@ -150,6 +151,7 @@ def make_config(width, height, fps=30.0, amp=120.0, f_low=0.5, f_high=None, wind
     c.threshold_form, c.device = int(threshold_form), int(device)
     c.iir_state_fp64 = int(bool(state_fp64))
     c.ring_fp16 = int(bool(ring_fp16))
+    c.planes_fp16 = int(bool(planes_fp16))
     return c
 
 
