@@ -521,7 +521,7 @@ def bench_mixed(a, rank, world, local):
     e2e_runs = {}
     for overlap in (False, True):               # True last: the library's default
         b.set_host_overlap(overlap)
-        for i in range(2):                       # untimed: the library allocates its staging sets
+        for i in range(3):                       # untimed: the library allocates its staging sets
             b.tick_host(ids, v_in[i % K], v_out[i % 2])
         b.sync()
         barrier()

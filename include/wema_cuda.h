@@ -160,7 +160,8 @@ int wema_cuda_threshold_flat(const float *d_x, size_t n, int threshold_form, flo
  * before any stream capture.  All calls on a device share the array, so calls
  * whose work overlaps on the GPU race with each other: order them on one
  * stream or synchronise between them.  Nothing in the array needs to start
- * zeroed. */
+ * zeroed.  The looked-up address is kept for the library's lifetime, so a
+ * cudaDeviceReset while the library stays loaded is not supported here. */
 int wema_cuda_threshold_flat_noalloc(const float *d_x, size_t n, int threshold_form,
                                      float *d_thr, float *d_sum, void *cuda_stream);
 
@@ -190,11 +191,11 @@ int wema_cuda_batch_tick(wema_cuda_batch *b, const int *ids, const void *const *
                          void *const *d_out_u8, int n, void *wait_event, void *done_event);
 int wema_cuda_batch_sync(wema_cuda_batch *b);
 /* The same tick with HOST frames (RGB24; pin them, e.g. with cudaHostAlloc,
- * for the copies to overlap): the tick's frames are copied into one of two
+ * for the copies to overlap): the tick's frames are copied into one of three
  * device staging sets the batch keeps (each a pair of arenas holding the
  * tick's frames back to back), the tick runs, the outputs are copied back -
- * so tick i's outputs go out while tick i+1's inputs come in and tick i runs
- * (the reference's async_io.c double buffering, on copy engines).  Frames
+ * so tick i-1's outputs go out while tick i+1's inputs come in and tick i
+ * runs (the reference's async_io.c double buffering, on copy engines).  Frames
  * that lie back to back in host memory (in `ids` order) move in one copy;
  * many small copies in both directions at once run well below the host
  * link's rate.  Asynchronous: the copies in wait for wait_event (may be NULL)

@@ -103,23 +103,26 @@ public:
     double stage_ms[T_COUNT] = {};
     long long ticks_timed = 0;
 
-    // host-frame ticks: two device staging sets, each one arena for a tick's
+    // host-frame ticks: three device staging sets, each one arena for a tick's
     // frames in and one for its frames out (the tick's streams back to back),
-    // copies on their own streams, so tick i's outputs go out while tick i+1's
-    // inputs come in (async_io.c's double buffering, on copy engines instead
-    // of threads).  Host frames that lie back to back move in one copy.
+    // copies on their own streams, so tick i-1's outputs go out while tick
+    // i+1's inputs come in and tick i runs (async_io.c's double buffering, on
+    // copy engines instead of threads; with two sets, tick i+1's copies in
+    // would wait for tick i-1's copies out and the two directions would
+    // alternate instead of overlapping).  Host frames that lie back to back
+    // move in one copy.
     struct HostSet {
         cudaEvent_t h2d = nullptr, tick = nullptr, d2h = nullptr;
         bool used = false;
         uint8_t* din = nullptr;
         uint8_t* dout = nullptr;
         size_t cap = 0;                 // bytes of each arena
-    } hs[2];
+    } hs[3];
     cudaStream_t st_h2d = nullptr, st_d2h = nullptr;
     int hcur = 0;
-    // copies in wait only for their staging set's previous tick (two ticks
-    // back), so they overlap the previous tick's kernels; off: they also wait
-    // for the previous tick to finish
+    // copies in wait only for their staging set's previous tick (three ticks
+    // back), so they overlap the previous tick's kernels and copies out; off:
+    // they also wait for the previous tick to finish
     bool host_overlap = true;
     int cur = 0;
     long long launches = 0;
@@ -288,12 +291,12 @@ public:
             const size_t fb = 3 * (size_t)streams[id]->g.pixels;
             off[k + 1] = off[k] + ((fb + 255) & ~(size_t)255);   // 256-byte aligned frames
         }
-        // this set was last used two ticks ago: its tick has read the inputs and
+        // this set was last used three ticks ago: its tick has read the inputs and
         // its outputs have gone out before they are overwritten
         if (S.used && (!cuda_ok(cudaStreamWaitEvent(st_h2d, S.tick, 0), "stream wait") ||
                        !cuda_ok(cudaStreamWaitEvent(st_h2d, S.d2h, 0), "stream wait")))
             return false;
-        const HostSet& P = hs[hcur ^ 1];
+        const HostSet& P = hs[(hcur + 2) % 3];   // the previous tick's set
         if (!host_overlap && P.used && !cuda_ok(cudaStreamWaitEvent(st_h2d, P.tick, 0), "stream wait"))
             return false;
         if (wait && !cuda_ok(cudaStreamWaitEvent(st_h2d, wait, 0), "stream wait")) return false;
@@ -346,7 +349,7 @@ public:
         if (!cuda_ok(cudaEventRecord(S.d2h, st_d2h), "event record")) return false;
         if (done && !cuda_ok(cudaEventRecord(done, st_d2h), "event record")) return false;
         S.used = true;
-        hcur ^= 1;
+        hcur = (hcur + 1) % 3;
         return true;
     }
 
