@@ -290,17 +290,25 @@ int wema_cuda_server_stats(wema_cuda_server *srv, int reset, wema_cuda_serve_sta
  *     default, unless another is more than 3% faster);
  *   - the batched guided filter's sweep at 64, 128 and 256 output rows per
  *     segment (a 3840x8640 trial frame) and keeps the fastest (128 until then);
- * allocating ~550 MB for the trials and freeing it.  Every later launch on the
- * device uses the choices.  Returns the positions per thread (or -1) and
- * writes the timings to `report` (may be NULL).  Results do not depend on
- * either choice - each position's and each pixel's arithmetic is the same -
- * only speed does.  set / get fix or read a choice directly (positions 2, 4
- * or 8; rows a multiple of 16 in 16..4096). */
+ *   - the batched luma DWT level-0 kernels, forward and inverse, in nine
+ *     variants each: CTAs per SM asked of the register allocator {1 (the
+ *     compiler's choice), 3, 4} x lines lifted per warp at a time {2, 4, 8}
+ *     (variant = 3 * index + index; a 3840x4320 trial frame) and keeps the
+ *     fastest of each (forward 3x4, inverse 1x4 until then);
+ * allocating ~550 MB for the trials (one at a time) and freeing it.  Every
+ * later launch on the device uses the choices.  Returns the positions per
+ * thread (or -1) and writes the timings to `report` (may be NULL; 1 KiB is
+ * enough).  Results do not depend on any choice - each position's and each
+ * pixel's arithmetic is the same - only speed does.  set / get fix or read a
+ * choice directly (positions 2, 4 or 8; rows a multiple of 16 in 16..4096;
+ * DWT variant 0..8, inverse = 0 forward, 1 inverse). */
 int wema_cuda_autotune(int device, char *report, size_t cap);
 int wema_cuda_set_iir_positions(int device, int positions);
 int wema_cuda_get_iir_positions(int device);
 int wema_cuda_set_guided_rows(int device, int rows);
 int wema_cuda_get_guided_rows(int device);
+int wema_cuda_set_dwt_variant(int device, int inverse, int variant);
+int wema_cuda_get_dwt_variant(int device, int inverse);
 
 /* Message of the last failure on this thread ("" if none). */
 const char *wema_cuda_last_error(void);

@@ -92,3 +92,38 @@ def test_guided_rows_choice_independence(torch_cuda):
     with pytest.raises(RuntimeError):
         wc.set_guided_rows(0, 40)
     wc.set_guided_rows(0, before)
+
+
+def test_dwt_variants_choice_independence(torch_cuda):
+    """Every tuning variant of the batched luma DWT kernels (CTAs per SM x
+    lines per warp, forward and inverse) gives the same frames, bit for bit;
+    the autotuner reports its trial and keeps a variant."""
+    torch = torch_cuda
+    report = wc.autotune(0)[1]
+    assert "forward DWT level 0" in report and "inverse DWT level 0" in report
+    keep = (wc.dwt_variant(0, False), wc.dwt_variant(0, True))
+    F = 3
+    cfgs = [(640, 480, dict(amp=90.0)), (137, 91, dict(amp=60.0)), (1920, 1080, dict(amp=40.0))]
+    data = [torch.from_numpy(SynthVideo(SynthSpec(w, h, 30.0, 13 + k, [1.1], [0.4], 14.0, 2.0))
+                             .frames(0, F)).cuda() for k, (w, h, _) in enumerate(cfgs)]
+    outs = {}
+    for v in range(9):
+        wc.set_dwt_variant(0, False, v)
+        wc.set_dwt_variant(0, True, (v + 4) % 9)
+        b = wc.Batch(device=0, max_streams=len(cfgs))
+        ids = [b.add(w, h, **c) for (w, h, c) in cfgs]
+        got = [[torch.empty((h, w, 3), dtype=torch.uint8, device="cuda") for _ in range(F)]
+               for (w, h, _) in cfgs]
+        for t in range(F):
+            b.tick(ids, [d[t] for d in data], [g[t] for g in got])
+        b.sync()
+        outs[v] = [[x.cpu().numpy() for x in g] for g in got]
+        b.close()
+    for v in range(1, 9):
+        for k in range(len(cfgs)):
+            for t in range(F):
+                assert np.array_equal(outs[v][k][t], outs[0][k][t]), f"variant {v}, stream {k}, frame {t}"
+    with pytest.raises(RuntimeError):
+        wc.set_dwt_variant(0, False, 9)
+    wc.set_dwt_variant(0, False, keep[0])
+    wc.set_dwt_variant(0, True, keep[1])

@@ -26,6 +26,8 @@
 // inward by at most two lanes, all inside the halo.  Arithmetic is the
 // reference's: x = fma(left + right, c, x), scalings as separate multiplies
 // (dwt.c:45-170 as GCC -Ofast evaluates it), so coefficients are bit-exact.
+#include <atomic>
+
 #include "common.cuh"
 #include "kernels.h"
 #include "multi.cuh"
@@ -85,27 +87,28 @@ __device__ __forceinline__ void lift_inv(float& e, float& o, int s, int n) {
 #undef WEMA_UPDATE
 }
 
-// Four lines of one plane at a time: their lifting chains are independent, so
-// the warp interleaves them.  b[u] is line u's base (a valid line even when
+// LPW lines of one plane at a time (2, 4 or 8: a tuning choice, the result
+// is the same): their lifting chains are independent, so the warp
+// interleaves them.  b[u] is line u's base (a valid line even when
 // act[u] is false - then nothing is stored); ei / oi address this lane's even
 // and odd sample, s is its even sample's global index, n the line length, lim
 // the staged length.
-template <bool FWD>
-__device__ __forceinline__ void lift4(float* const (&b)[4], const bool (&act)[4], int ei, int oi,
+template <bool FWD, int LPW>
+__device__ __forceinline__ void liftN(float* const (&b)[LPW], const bool (&act)[LPW], int ei, int oi,
                                       int s, int n, int lim, int lane) {
-    float e[4], o[4];
+    float e[LPW], o[LPW];
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
+    for (int u = 0; u < LPW; u++) {
         e[u] = b[u][ei];
         o[u] = b[u][oi];
     }
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
+    for (int u = 0; u < LPW; u++) {
         if (FWD) lift_fwd(e[u], o[u], s, n);
         else lift_inv(e[u], o[u], s, n);
     }
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
+    for (int u = 0; u < LPW; u++) {
         if (!act[u]) continue;
         if (2 * lane < lim) b[u][ei] = e[u];
         if (2 * lane + 1 < lim) b[u][oi] = o[u];
@@ -115,7 +118,7 @@ __device__ __forceinline__ void lift4(float* const (&b)[4], const bool (&act)[4]
 // ----------------------------------------------------------------- forward
 // C == 3: level 0 of a colour frame, all channels in one CTA, grid (tx, ty, 1).
 // C == 1: channel blockIdx.z (planes in), or the luma of an RGB frame.
-template <int C, int MODE>
+template <int C, int MODE, int LPW>
 __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, int by, int bz) {
     extern __shared__ __align__(16) float dyn[];
     float* planes = dyn;                                   // [C][PLANE]
@@ -249,16 +252,16 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
     if (iw >= 2) {   // rows: every staged row of every plane
 #pragma unroll
         for (int cc = 0; cc < C; cc++)
-            for (int l0 = warp; l0 < RH; l0 += 4 * NWARP) {
-                float* b[4];
-                bool act[4];
+            for (int l0 = warp; l0 < RH; l0 += LPW * NWARP) {
+                float* b[LPW];
+                bool act[LPW];
 #pragma unroll
-                for (int u = 0; u < 4; u++) {
+                for (int u = 0; u < LPW; u++) {
                     const int ly = l0 + u * NWARP;
                     act[u] = ly < RH;
                     b[u] = planes + cc * PLANE + prow(min(ly, RH - 1)) * RS;
                 }
-                lift4<true>(b, act, lane, ODD_COL + lane, rx0 + 2 * lane, iw, RW, lane);
+                liftN<true, LPW>(b, act, lane, ODD_COL + lane, rx0 + 2 * lane, iw, RW, lane);
             }
         __syncthreads();
     }
@@ -266,16 +269,16 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
     if (ih >= 2) {   // columns: the tile's own
 #pragma unroll
         for (int cc = 0; cc < C; cc++)
-            for (int l0 = cx0 + warp; l0 < cx1; l0 += 4 * NWARP) {
-                float* b[4];
-                bool act[4];
+            for (int l0 = cx0 + warp; l0 < cx1; l0 += LPW * NWARP) {
+                float* b[LPW];
+                bool act[LPW];
 #pragma unroll
-                for (int u = 0; u < 4; u++) {
+                for (int u = 0; u < LPW; u++) {
                     const int lx = l0 + u * NWARP;
                     act[u] = lx < cx1;
                     b[u] = planes + cc * PLANE + pcol(min(lx, cx1 - 1));
                 }
-                lift4<true>(b, act, lane * RS, (32 + lane) * RS, ry0 + 2 * lane, ih, RH, lane);
+                liftN<true, LPW>(b, act, lane * RS, (32 + lane) * RS, ry0 + 2 * lane, ih, RH, lane);
             }
         __syncthreads();
     }
@@ -313,7 +316,7 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
 // ----------------------------------------------------------------- inverse
 // C == 1: grid (tiles_x, tiles_y, channels), planes out.
 // C == 3: one CTA per tile does all three channels (YCbCr -> RGB at level 0).
-template <int C, int OUT>
+template <int C, int OUT, int LPW>
 __device__ __forceinline__ void dwt_inv_body(const InvLevelParams& p, int bx, int by, int bz) {
     extern __shared__ __align__(16) float dyn[];
     float* planes = dyn;   // [C][PLANE]
@@ -375,16 +378,16 @@ __device__ __forceinline__ void dwt_inv_body(const InvLevelParams& p, int bx, in
     if (oh >= 2) {   // columns over the whole staged region
 #pragma unroll
         for (int cc = 0; cc < C; cc++)
-            for (int l0 = warp; l0 < RW; l0 += 4 * NWARP) {
-                float* b[4];
-                bool act[4];
+            for (int l0 = warp; l0 < RW; l0 += LPW * NWARP) {
+                float* b[LPW];
+                bool act[LPW];
 #pragma unroll
-                for (int u = 0; u < 4; u++) {
+                for (int u = 0; u < LPW; u++) {
                     const int lx = l0 + u * NWARP;
                     act[u] = lx < RW;
                     b[u] = planes + cc * PLANE + pcol(min(lx, RW - 1));
                 }
-                lift4<false>(b, act, lane * RS, (32 + lane) * RS, ry0 + 2 * lane, oh, RH, lane);
+                liftN<false, LPW>(b, act, lane * RS, (32 + lane) * RS, ry0 + 2 * lane, oh, RH, lane);
             }
         __syncthreads();
     }
@@ -393,16 +396,16 @@ __device__ __forceinline__ void dwt_inv_body(const InvLevelParams& p, int bx, in
     if (ow >= 2) {   // rows of the tile
 #pragma unroll
         for (int cc = 0; cc < C; cc++)
-            for (int l0 = ty0 + warp; l0 < ty1; l0 += 4 * NWARP) {
-                float* b[4];
-                bool act[4];
+            for (int l0 = ty0 + warp; l0 < ty1; l0 += LPW * NWARP) {
+                float* b[LPW];
+                bool act[LPW];
 #pragma unroll
-                for (int u = 0; u < 4; u++) {
+                for (int u = 0; u < LPW; u++) {
                     const int ly = l0 + u * NWARP;
                     act[u] = ly < ty1;
                     b[u] = planes + cc * PLANE + prow(min(ly, ty1 - 1)) * RS;
                 }
-                lift4<false>(b, act, lane, ODD_COL + lane, rx0 + 2 * lane, ow, RW, lane);
+                liftN<false, LPW>(b, act, lane, ODD_COL + lane, rx0 + 2 * lane, ow, RW, lane);
             }
         __syncthreads();
     }
@@ -449,26 +452,57 @@ __device__ __forceinline__ void dwt_inv_body(const InvLevelParams& p, int bx, in
 
 // ------------------------------------------------------------- wrappers
 // one stream per launch, and the batched form (task = stream; params in device
-// memory, one entry per task)
+// memory, one entry per task).  The batched luma kernels also come in tuning
+// variants: MINB CTAs per SM asked of the register allocator (1: the
+// compiler's choice, 3 or 4) and
+// LPW lines per warp in flight (2, 4 or 8); every variant computes the same
+// coefficients, bit for bit.
+constexpr int LPW_DEF = 4;
 template <int C, int MODE>
 __global__ void __launch_bounds__(DWT_THREADS, 3) k_dwt_fwd(FwdLevelParams p) {
-    dwt_fwd_body<C, MODE>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+    dwt_fwd_body<C, MODE, LPW_DEF>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
-template <int C, int MODE>
-__global__ void __launch_bounds__(DWT_THREADS, 3)
+template <int C, int MODE, int MINB, int LPW>
+__global__ void __launch_bounds__(DWT_THREADS, MINB)
     k_dwt_fwd_multi(const FwdLevelParams* __restrict__ ps, const int* __restrict__ map) {
     const TaskBlock t = task_block(map, blockIdx.x);
-    dwt_fwd_body<C, MODE>(ps[t.task], t.x, t.y, t.z);
+    dwt_fwd_body<C, MODE, LPW>(ps[t.task], t.x, t.y, t.z);
 }
 template <int C, int OUT>
 __global__ void __launch_bounds__(DWT_THREADS) k_dwt_inv(InvLevelParams p) {
-    dwt_inv_body<C, OUT>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+    dwt_inv_body<C, OUT, LPW_DEF>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
-template <int C, int OUT>
-__global__ void __launch_bounds__(DWT_THREADS)
+template <int C, int OUT, int MINB, int LPW>
+__global__ void __launch_bounds__(DWT_THREADS, MINB)
     k_dwt_inv_multi(const InvLevelParams* __restrict__ ps, const int* __restrict__ map) {
     const TaskBlock t = task_block(map, blockIdx.x);
-    dwt_inv_body<C, OUT>(ps[t.task], t.x, t.y, t.z);
+    dwt_inv_body<C, OUT, LPW>(ps[t.task], t.x, t.y, t.z);
+}
+
+// ---- tuning of the batched luma kernels, per device: variant index
+// v = 3 * minb_index + lpw_index over MINB {1, 3, 4} x LPW {2, 4, 8}
+constexpr int kDwtVariants = 9;
+static const int kMinb[3] = {1, 3, 4}, kLpw[3] = {2, 4, 8};
+static std::atomic<int> g_dwt_var[64][2];     // [device][0 forward, 1 inverse], value + 1
+
+static int dwt_dev_now() {
+    int d = 0;
+    cudaGetDevice(&d);
+    return d;
+}
+int dwt_variant(int dev, int inverse) {
+    const int v = (dev >= 0 && dev < 64) ? g_dwt_var[dev][inverse ? 1 : 0].load() : 0;
+    // defaults (4 lines per warp): forward 3 CTAs per SM, inverse the compiler's choice
+    return v > 0 ? v - 1 : (inverse ? 0 * 3 + 1 : 1 * 3 + 1);
+}
+bool dwt_set_variant(int dev, int inverse, int v) {
+    if (dev < 0 || dev >= 64 || v < 0 || v >= kDwtVariants) return false;
+    g_dwt_var[dev][inverse ? 1 : 0].store(v + 1);
+    return true;
+}
+void dwt_variant_shape(int v, int* minb, int* lpw) {
+    *minb = kMinb[v / 3];
+    *lpw = kLpw[v % 3];
 }
 
 // ----------------------------------------------------------------- launch
@@ -489,8 +523,8 @@ cudaError_t dwt_prepare_device() {
     cudaError_t e = allow_smem(k_dwt_inv<3, kOutRgb>, inv_smem(3));
     if (e == cudaSuccess) e = allow_smem(k_dwt_fwd<3, kSrcRgbU8>, fwd_smem(3));
     if (e == cudaSuccess) e = allow_smem(k_dwt_fwd<3, kSrcRgbF32>, fwd_smem(3));
-    if (e == cudaSuccess) e = allow_smem(k_dwt_inv_multi<3, kOutRgb>, inv_smem(3));
-    if (e == cudaSuccess) e = allow_smem(k_dwt_fwd_multi<3, kSrcRgbU8>, fwd_smem(3));
+    if (e == cudaSuccess) e = allow_smem(k_dwt_inv_multi<3, kOutRgb, 1, LPW_DEF>, inv_smem(3));
+    if (e == cudaSuccess) e = allow_smem(k_dwt_fwd_multi<3, kSrcRgbU8, 3, LPW_DEF>, fwd_smem(3));
     return e;
 }
 
@@ -509,26 +543,47 @@ unsigned dwt_inv_grid(const InvLevelParams& p, int channels_z, unsigned& gx, uns
 cudaError_t launch_dwt_fwd_multi(int mode, int channels, const FwdLevelParams* d_params,
                                  const int* d_map, unsigned blocks, cudaStream_t st) {
     if (blocks == 0) return cudaSuccess;
-    if (mode == kSrcPlanes)
-        k_dwt_fwd_multi<1, kSrcPlanes><<<blocks, DWT_THREADS, fwd_smem(1), st>>>(d_params, d_map);
-    else if (mode == kSrcRgbU8 && channels == 3)
-        k_dwt_fwd_multi<3, kSrcRgbU8><<<blocks, DWT_THREADS, fwd_smem(3), st>>>(d_params, d_map);
-    else if (mode == kSrcRgbU8 && channels == 1)
-        k_dwt_fwd_multi<1, kSrcRgbU8><<<blocks, DWT_THREADS, fwd_smem(1), st>>>(d_params, d_map);
-    else
-        return cudaErrorInvalidValue;
+    if (mode == kSrcRgbU8 && channels == 3) {
+        k_dwt_fwd_multi<3, kSrcRgbU8, 3, LPW_DEF><<<blocks, DWT_THREADS, fwd_smem(3), st>>>(d_params, d_map);
+        return cudaGetLastError();
+    }
+    if ((mode != kSrcPlanes && mode != kSrcRgbU8) || channels != 1) return cudaErrorInvalidValue;
+    const int v = dwt_variant(dwt_dev_now(), 0);
+    const size_t sm = fwd_smem(1);
+#define WEMA_FWD_CASE(I, MB, LP)                                                                        \
+    case I:                                                                                             \
+        if (mode == kSrcPlanes) k_dwt_fwd_multi<1, kSrcPlanes, MB, LP><<<blocks, DWT_THREADS, sm, st>>>(d_params, d_map); \
+        else k_dwt_fwd_multi<1, kSrcRgbU8, MB, LP><<<blocks, DWT_THREADS, sm, st>>>(d_params, d_map);     \
+        break;
+    switch (v) {
+        WEMA_FWD_CASE(0, 1, 2) WEMA_FWD_CASE(1, 1, 4) WEMA_FWD_CASE(2, 1, 8)
+        WEMA_FWD_CASE(3, 3, 2) WEMA_FWD_CASE(4, 3, 4) WEMA_FWD_CASE(5, 3, 8)
+        WEMA_FWD_CASE(6, 4, 2) WEMA_FWD_CASE(7, 4, 4) WEMA_FWD_CASE(8, 4, 8)
+        default: return cudaErrorInvalidValue;
+    }
+#undef WEMA_FWD_CASE
     return cudaGetLastError();
 }
 
 cudaError_t launch_dwt_inv_multi(int channels, int out_mode, const InvLevelParams* d_params,
                                  const int* d_map, unsigned blocks, cudaStream_t st) {
     if (blocks == 0) return cudaSuccess;
-    if (out_mode == kOutPlanes)
-        k_dwt_inv_multi<1, kOutPlanes><<<blocks, DWT_THREADS, inv_smem(1), st>>>(d_params, d_map);
-    else if (out_mode == kOutRgb && channels == 3)
-        k_dwt_inv_multi<3, kOutRgb><<<blocks, DWT_THREADS, inv_smem(3), st>>>(d_params, d_map);
-    else
-        return cudaErrorInvalidValue;
+    if (out_mode == kOutRgb && channels == 3) {
+        k_dwt_inv_multi<3, kOutRgb, 1, LPW_DEF><<<blocks, DWT_THREADS, inv_smem(3), st>>>(d_params, d_map);
+        return cudaGetLastError();
+    }
+    if (out_mode != kOutPlanes) return cudaErrorInvalidValue;
+    const int v = dwt_variant(dwt_dev_now(), 1);
+    const size_t sm = inv_smem(1);
+#define WEMA_INV_CASE(I, MB, LP)                                                                        \
+    case I: k_dwt_inv_multi<1, kOutPlanes, MB, LP><<<blocks, DWT_THREADS, sm, st>>>(d_params, d_map); break;
+    switch (v) {
+        WEMA_INV_CASE(0, 1, 2) WEMA_INV_CASE(1, 1, 4) WEMA_INV_CASE(2, 1, 8)
+        WEMA_INV_CASE(3, 3, 2) WEMA_INV_CASE(4, 3, 4) WEMA_INV_CASE(5, 3, 8)
+        WEMA_INV_CASE(6, 4, 2) WEMA_INV_CASE(7, 4, 4) WEMA_INV_CASE(8, 4, 8)
+        default: return cudaErrorInvalidValue;
+    }
+#undef WEMA_INV_CASE
     return cudaGetLastError();
 }
 
@@ -558,6 +613,101 @@ cudaError_t launch_dwt_inv(int channels, int out_mode, const InvLevelParams& p, 
     else
         return cudaErrorInvalidValue;
     return cudaGetLastError();
+}
+
+}  // namespace wema
+
+namespace wema {
+
+// ---- the autotuner's trial of the batched luma kernels' variants: the
+// forward level-0 transform of a 3840 x 4320 RGB24 frame (two 2160-row frames'
+// worth of tiles) and the inverse level-0 transform of its planes, each
+// variant timed over five launches after one warm-up through the batched
+// launch path (one task); the fastest of each is kept for the device.
+cudaError_t dwt_autotune(int dev, float fwd_ms[9], float inv_ms[9], int* fwd_best, int* inv_best) {
+    cudaError_t e = cudaSetDevice(dev);
+    if (e != cudaSuccess) return e;
+    const int W = 3840, H = 4320, SW = W / 2, SH = H / 2;
+    const size_t P = (size_t)W * H, N = (size_t)SW * SH;
+    uint8_t* rgb = nullptr;
+    float *coef = nullptr, *delta = nullptr, *ll = nullptr, *out = nullptr, *thr = nullptr;
+    void *dp = nullptr, *dmap = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaStream_t st = nullptr;
+    const int keep_f = dwt_variant(dev, 0), keep_i = dwt_variant(dev, 1);
+    auto done = [&](cudaError_t r) {
+        for (void* p : {(void*)rgb, (void*)coef, (void*)delta, (void*)ll, (void*)out, (void*)thr, dp, dmap})
+            if (p) cudaFree(p);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (st) cudaStreamDestroy(st);
+        if (r != cudaSuccess) {                   // leave the device's choices as they were
+            dwt_set_variant(dev, 0, keep_f);
+            dwt_set_variant(dev, 1, keep_i);
+        }
+        return r;
+    };
+    if ((e = cudaMalloc(&rgb, 3 * P)) != cudaSuccess) return done(e);
+    if ((e = cudaMalloc(&coef, 3 * N * sizeof(float))) != cudaSuccess) return done(e);
+    if ((e = cudaMalloc(&delta, 3 * N * sizeof(float))) != cudaSuccess) return done(e);
+    if ((e = cudaMalloc(&ll, N * sizeof(float))) != cudaSuccess) return done(e);
+    if ((e = cudaMalloc(&out, P * sizeof(float))) != cudaSuccess) return done(e);
+    if ((e = cudaMalloc(&thr, 8 * sizeof(float))) != cudaSuccess) return done(e);
+    if ((e = cudaMalloc(&dp, sizeof(FwdLevelParams) + sizeof(InvLevelParams))) != cudaSuccess) return done(e);
+    if ((e = cudaMalloc(&dmap, 8 * sizeof(int))) != cudaSuccess) return done(e);
+    if ((e = cudaMemset(rgb, 0x5a, 3 * P)) != cudaSuccess) return done(e);
+    if ((e = cudaMemset(delta, 0, 3 * N * sizeof(float))) != cudaSuccess) return done(e);
+    if ((e = cudaMemset(thr, 0, 8 * sizeof(float))) != cudaSuccess) return done(e);
+    if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) return done(e);
+    if ((e = cudaEventCreate(&e0)) != cudaSuccess || (e = cudaEventCreate(&e1)) != cudaSuccess) return done(e);
+    if ((e = dwt_prepare_device()) != cudaSuccess) return done(e);
+    FwdLevelParams fp{};
+    fp.iw = W; fp.ih = H; fp.sw = SW; fp.sh = SH; fp.n = (long long)N;
+    fp.vec_end = (long long)P;
+    fp.src_u8 = rgb;
+    fp.coef[0] = coef;
+    fp.ll_out[0] = ll;
+    InvLevelParams ip{};
+    ip.ow = W; ip.oh = H; ip.sw = SW; ip.sh = SH; ip.n = (long long)N;
+    ip.ll[0] = ll;
+    ip.coef[0] = coef;
+    ip.delta[0] = delta;
+    ip.thr = thr;
+    ip.alpha[0] = 1.0f;
+    ip.out_planes[0] = out;
+    if ((e = cudaMemcpy(dp, &fp, sizeof fp, cudaMemcpyHostToDevice)) != cudaSuccess) return done(e);
+    char* dpi = static_cast<char*>(dp) + sizeof(FwdLevelParams);
+    if ((e = cudaMemcpy(dpi, &ip, sizeof ip, cudaMemcpyHostToDevice)) != cudaSuccess) return done(e);
+    unsigned gx, gy;
+    const unsigned fblocks = dwt_fwd_grid(fp, 1, gx, gy);
+    const int fmap[5] = {1, 0, (int)fblocks, (int)gx, (int)gy};
+    const unsigned iblocks = dwt_inv_grid(ip, 1, gx, gy);
+    const int imap[5] = {1, 0, (int)iblocks, (int)gx, (int)gy};
+    int* map = static_cast<int*>(dmap);
+    for (int inv = 0; inv < 2; inv++) {
+        if ((e = cudaMemcpy(map, inv ? imap : fmap, sizeof fmap, cudaMemcpyHostToDevice)) != cudaSuccess)
+            return done(e);
+        float* ms = inv ? inv_ms : fwd_ms;
+        int best = 0;
+        for (int v = 0; v < kDwtVariants; v++) {
+            dwt_set_variant(dev, inv, v);
+            for (int rep = 0; rep < 6; rep++) {
+                if (rep == 1 && (e = cudaEventRecord(e0, st)) != cudaSuccess) return done(e);
+                e = inv ? launch_dwt_inv_multi(1, kOutPlanes, (const InvLevelParams*)dpi, map, iblocks, st)
+                        : launch_dwt_fwd_multi(kSrcRgbU8, 1, (const FwdLevelParams*)dp, map, fblocks, st);
+                if (e != cudaSuccess) return done(e);
+            }
+            if ((e = cudaEventRecord(e1, st)) != cudaSuccess) return done(e);
+            if ((e = cudaEventSynchronize(e1)) != cudaSuccess) return done(e);
+            float t = 0.f;
+            if ((e = cudaEventElapsedTime(&t, e0, e1)) != cudaSuccess) return done(e);
+            ms[v] = t / 5.f;
+            if (ms[v] < ms[best]) best = v;
+        }
+        dwt_set_variant(dev, inv, best);
+        (inv ? *inv_best : *fwd_best) = best;
+    }
+    return done(cudaSuccess);
 }
 
 }  // namespace wema

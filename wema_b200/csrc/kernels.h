@@ -45,6 +45,13 @@ cudaError_t dwt_prepare_device();
 size_t dwt_smem_bytes(int channels);
 cudaError_t launch_dwt_fwd(int src_mode, int channels, const FwdLevelParams& p, cudaStream_t st);
 cudaError_t launch_dwt_inv(int channels, int out_mode, const InvLevelParams& p, cudaStream_t st);
+// tuning variant (0..8) of the batched luma DWT kernels on a device:
+// CTAs per SM {1: the compiler's choice, 3, 4}[v / 3] x lines per warp {2, 4, 8}[v % 3]
+int dwt_variant(int dev, int inverse);
+bool dwt_set_variant(int dev, int inverse, int v);
+void dwt_variant_shape(int v, int* minb, int* lpw);
+// times every variant of the forward and inverse level-0 luma kernels, keeps the fastest
+cudaError_t dwt_autotune(int dev, float fwd_ms[9], float inv_ms[9], int* fwd_best, int* inv_best);
 
 // ---- exact threshold (threshold.cu) ---------------------------------------
 // Views the unique detail planes of one channel as the reference's 6-slot

@@ -704,16 +704,33 @@ WEMA_API int wema_cuda_session_sync(wema_cuda_session* s) {
 WEMA_API int wema_cuda_autotune(int device, char* report, size_t cap) {
     clear_error();
     if (!ensure_device(device)) return -1;
-    float ms[3] = {0.f, 0.f, 0.f}, gms[3] = {0.f, 0.f, 0.f};
+    float ms[3] = {0.f, 0.f, 0.f}, gms[3] = {0.f, 0.f, 0.f}, fms[9] = {}, ims[9] = {};
     const int rows[3] = {64, 128, 256};
-    int chosen = 0, grows = 0;
+    int chosen = 0, grows = 0, fbest = 0, ibest = 0;
     if (!cuda_ok(iir_autotune(device, ms, &chosen), "autotune")) return -1;
     if (!cuda_ok(guided_autotune(device, rows, 3, gms, &grows), "autotune")) return -1;
-    if (report && cap)
-        snprintf(report, cap,
-                 "iir positions per thread: 2 %.4f ms, 4 %.4f ms, 8 %.4f ms -> %d; "
-                 "guided sweep rows per segment: 64 %.4f ms, 128 %.4f ms, 256 %.4f ms -> %d",
-                 ms[0], ms[1], ms[2], chosen, gms[0], gms[1], gms[2], grows);
+    if (!cuda_ok(dwt_autotune(device, fms, ims, &fbest, &ibest), "autotune")) return -1;
+    if (report && cap) {
+        int n = snprintf(report, cap,
+                         "iir positions per thread: 2 %.4f ms, 4 %.4f ms, 8 %.4f ms -> %d; "
+                         "guided sweep rows per segment: 64 %.4f ms, 128 %.4f ms, 256 %.4f ms -> %d",
+                         ms[0], ms[1], ms[2], chosen, gms[0], gms[1], gms[2], grows);
+        for (int inv = 0; inv < 2 && n > 0 && (size_t)n < cap; inv++) {
+            const float* t = inv ? ims : fms;
+            n += snprintf(report + n, cap - n, "; %s DWT level 0 (CTAs/SM x lines/warp):",
+                          inv ? "inverse" : "forward");
+            for (int v = 0; v < 9 && n > 0 && (size_t)n < cap; v++) {
+                int mb, lp;
+                dwt_variant_shape(v, &mb, &lp);
+                n += snprintf(report + n, cap - n, " %dx%d %.4f", mb, lp, t[v]);
+            }
+            if (n > 0 && (size_t)n < cap) {
+                int mb, lp;
+                dwt_variant_shape(inv ? ibest : fbest, &mb, &lp);
+                n += snprintf(report + n, cap - n, " ms -> %dx%d", mb, lp);
+            }
+        }
+    }
     return chosen;
 }
 
@@ -729,6 +746,20 @@ WEMA_API int wema_cuda_set_guided_rows(int device, int rows) {
 WEMA_API int wema_cuda_get_guided_rows(int device) {
     clear_error();
     return guided_rows(device);
+}
+
+WEMA_API int wema_cuda_set_dwt_variant(int device, int inverse, int variant) {
+    clear_error();
+    if (!dwt_set_variant(device, inverse, variant)) {
+        set_error("DWT variant must be 0..8");
+        return -1;
+    }
+    return 0;
+}
+
+WEMA_API int wema_cuda_get_dwt_variant(int device, int inverse) {
+    clear_error();
+    return dwt_variant(device, inverse);
 }
 
 WEMA_API int wema_cuda_set_iir_positions(int device, int positions) {

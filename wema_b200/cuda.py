@@ -96,6 +96,8 @@ def lib() -> C.CDLL:
         L.wema_cuda_get_iir_positions.argtypes = [i]
         L.wema_cuda_set_guided_rows.argtypes = [i, i]
         L.wema_cuda_get_guided_rows.argtypes = [i]
+        L.wema_cuda_set_dwt_variant.argtypes = [i, i, i]
+        L.wema_cuda_get_dwt_variant.argtypes = [i, i]
         L.wema_cuda_batch_tick_host.argtypes = [vp, C.POINTER(i), C.POINTER(vp), C.POINTER(vp), i, vp, vp]
         L.wema_cuda_session_snapshot_bytes.argtypes = [vp]
         L.wema_cuda_session_snapshot_bytes.restype = sz
@@ -440,8 +442,8 @@ class Server:
 def autotune(device=0):
     """Times the filter step at 2 / 4 / 8 positions per thread and keeps the
     fastest for the device -> (positions, report)."""
-    buf = C.create_string_buffer(512)
-    u = lib().wema_cuda_autotune(int(device), buf, 512)
+    buf = C.create_string_buffer(1024)
+    u = lib().wema_cuda_autotune(int(device), buf, 1024)
     if u < 0:
         raise RuntimeError(f"autotune failed: {last_error()}")
     return u, buf.value.decode()
@@ -461,3 +463,11 @@ def set_guided_rows(device, rows):
 
 def guided_rows(device=0) -> int:
     return lib().wema_cuda_get_guided_rows(int(device))
+
+
+def set_dwt_variant(device, inverse, variant):
+    _check(lib().wema_cuda_set_dwt_variant(int(device), int(bool(inverse)), int(variant)), "set_dwt_variant")
+
+
+def dwt_variant(device=0, inverse=False) -> int:
+    return lib().wema_cuda_get_dwt_variant(int(device), int(bool(inverse)))
