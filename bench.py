@@ -80,10 +80,8 @@ METRIC = "Mpix-frames/s"
 # 48-stream tick; the threshold of the plain workload is monoids + walk.
 _MIX = 77.722 / 19.046
 TRAFFIC_NCU = {
-    ("mixed_streams_48", "luma_transfer"): int((133387008 + 37206784) * _MIX),
-    ("mixed_streams_48", "fwd_dwt_level0"): int((57178624 + 28476672) * _MIX),
+    ("mixed_streams_48", "luma_transfer"): int((148669184 + 34321152) * _MIX),
     ("mixed_streams_48", "inv_dwt_level0"): int((133352960 + 47001344) * _MIX),
-    ("mixed_streams_48", "temporal_amplify"): int((379583232 + 321814528) * _MIX),
     ("plain_fullhd_color", "threshold"): 25081088 + 2323456,
 }
 
@@ -168,21 +166,28 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def stage_bytes(w, h, channels, levels_dims, pu):
+def stage_bytes(w, h, channels, levels_dims, pu, fused=True):
     """Algorithmic HBM bytes per frame of each stage: every plane its stage
     reads or writes, once (the 6-slot mirror of the threshold is the same
-    memory as the unique planes, so it is counted once)."""
+    memory as the unique planes, so it is counted once).  fused: the IIR
+    step runs inside the forward transform (every frame after a stream's
+    first): its state in / out and delta out (36 B per coefficient) count
+    with the forward stage of the coefficient's level, and the coefficient
+    is not read again."""
     P = w * h
     C = channels
     n0 = levels_dims[0][0] * levels_dims[0][1]
+    step = C * (32 + 4) * 3                            # per position of a level: 3 coefficients
     fwd0 = 3 * P + C * 4 * 4 * n0                      # RGB24 in; LL + 3 bands out
+    if fused:
+        fwd0 += step * n0
     rest = 0
     for l in range(1, len(levels_dims)):
         pw, ph = levels_dims[l - 1]
         sw, sh = levels_dims[l]
-        rest += C * 4 * (pw * ph + 4 * sw * sh)
+        rest += C * 4 * (pw * ph + 4 * sw * sh) + (step * sw * sh if fused else 0)
     thr = C * 4 * pu                                   # |x| of every unique coefficient
-    temporal = C * (4 + 32 + 4) * pu                   # coef in, state in/out, delta out
+    temporal = 0 if fused else C * (4 + 32 + 4) * pu   # coef in, state in/out, delta out
     inv = {}
     for l in range(len(levels_dims)):
         sw, sh = levels_dims[l]
@@ -200,10 +205,10 @@ def stage_bytes(w, h, channels, levels_dims, pu):
 
 # kernels behind each stage of a batched tick (one launch per tick over every stream)
 STAGE_KERNELS_MULTI = {
-    "fwd_dwt_level0": "k_dwt_fwd_multi<1,1> (level 0, RGB in)",
-    "fwd_dwt_levels": "k_dwt_fwd_multi<1,0> x 3",
+    "fwd_dwt_level0": "k_dwt_fwd_multi<1,1> (level 0, RGB in, with the IIR step)",
+    "fwd_dwt_levels": "k_dwt_fwd_multi<1,0> x 3 (with the IIR step)",
     "threshold": "k_thr_monoids_multi + k_thr_walk_multi",
-    "temporal_amplify": "k_iir_multi",
+    "temporal_amplify": "k_iir_multi (first frames only; else inside the forward transform)",
     "inv_dwt_levels": "k_dwt_inv_multi<1,0> x 3",
     "inv_dwt_level0": "k_dwt_inv_multi<1,0> (level 0)",
     "luma_transfer": "k_guided_transfer_multi",
@@ -211,10 +216,10 @@ STAGE_KERNELS_MULTI = {
 
 # kernels behind each stage (one launch per frame unless noted)
 STAGE_KERNELS = {
-    "fwd_dwt_level0": "k_dwt_fwd<1|2> (level 0, RGB in)",
-    "fwd_dwt_levels": "k_dwt_fwd<0> x (levels - 1)",
+    "fwd_dwt_level0": "k_dwt_fwd<1|2> (level 0, RGB in, with the IIR step)",
+    "fwd_dwt_levels": "k_dwt_fwd<0> x (levels - 1) (with the IIR step)",
     "threshold": "k_thr_monoids + k_thr_walk",
-    "temporal_amplify": "k_iir x channels",
+    "temporal_amplify": "k_iir x channels (first frame only; else inside the forward transform)",
     "inv_dwt_levels": "k_dwt_inv<1,0> x (levels - 1)",
     "inv_dwt_level0": "k_dwt_inv<3,1> (colour, RGB out) / k_dwt_inv<1,0> (luma)",
     "luma_transfer": "k_guided_transfer / k_gauss_transfer",

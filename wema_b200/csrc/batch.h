@@ -426,6 +426,7 @@ public:
                 }
                 p.h16 = h;
                 p.prev_n = l > 0 ? g.n[l - 1] : 0;
+                if (S.frames_processed > 0) S.fill_temporal(p, l);   // the filter's step inside the transform
                 unsigned gx, gy;
                 if (l == 0) {
                     const unsigned b = dwt_fwd_grid(p, 1, gx, gy);
@@ -449,12 +450,13 @@ public:
                 L[L_THR_PART + st].add(targs.data(), grids[st][0], grids[st][1],
                                        grids[st][0] * grids[st][1]);
             }
-            // ---- IIR (first frame: preseed), fade-in alpha
+            // ---- IIR: a stream's first frame takes the preseed and the filter as
+            // launches of their own; after it the forward transform runs the step
             const bool first = S.frames_processed == 0;
-            for (int c = 0; c < nch; c++) {
+            for (int c = 0; first && c < nch; c++) {
                 const unsigned b = iir_args_fill(iargs.data(), S.ip, q.coef[c], S.state[c], S.cfg.iir_state_fp64, q.delta[c],
                                                  S.warmup);
-                if (first) L[L_IIR_PRESEED].add(iargs.data(), b, 1, b);
+                L[L_IIR_PRESEED].add(iargs.data(), b, 1, b);
                 L[L_IIR].add(iargs.data(), b, 1, b);
             }
             // ---- inverse DWT (+ colour output) and the luma transfer

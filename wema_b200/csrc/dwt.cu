@@ -28,6 +28,7 @@
 // (dwt.c:45-170 as GCC -Ofast evaluates it), so coefficients are bit-exact.
 #include <atomic>
 
+#include "cascade.cuh"
 #include "common.cuh"
 #include "kernels.h"
 #include "multi.cuh"
@@ -112,6 +113,48 @@ __device__ __forceinline__ void liftN(float* const (&b)[LPW], const bool (&act)[
         if (!act[u]) continue;
         if (2 * lane < lim) b[u][ei] = e[u];
         if (2 * lane + 1 < lim) b[u][oi] = o[u];
+    }
+}
+
+// The temporal filter's step (cascade.cuh) on the three coefficients of one
+// position of a level, LH / HH / HL (slots 0-2, unique offsets b*n + o), as
+// the forward transform writes them: the filter reads the coefficient as
+// stored (FP16-rounded in the planes_fp16 variant), so the deltas equal
+// those of the separate filter kernel bit for bit.  All state loads first.
+__device__ __forceinline__ void temporal_step3(const FwdLevelParams& p, int ch, void* st, int o, int n,
+                                               const float (&v)[3], bool h) {
+    float x[3];
+#pragma unroll
+    for (int b = 0; b < 3; b++) x[b] = h ? __half2float(__float2half_rn(v[b])) : v[b];
+    float* dl = p.iir_delta[ch];
+    if (p.iir_fp64) {
+        double2* s2 = static_cast<double2*>(st);
+        double2 hp[3], lp[3];
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            const long long u = (long long)b * n + o;
+            hp[b] = __ldcs(s2 + 2 * u);
+            lp[b] = __ldcs(s2 + 2 * u + 1);
+        }
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            const long long u = (long long)b * n + o;
+            pl_st(dl, u, cascade64(p.iir_c, hp[b], lp[b], x[b]), h);
+            __stcs(s2 + 2 * u, hp[b]);
+            __stcs(s2 + 2 * u + 1, lp[b]);
+        }
+    } else {
+        float4* s4 = static_cast<float4*>(st);
+        float4 sv[3];
+#pragma unroll
+        for (int b = 0; b < 3; b++) sv[b] = __ldcs(s4 + (long long)b * n + o);   // touched once: evict first
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            const long long u = (long long)b * n + o;
+            const bool tail = p.iir_off6 + u >= p.iir_simd_end;
+            pl_st(dl, u, cascade(p.iir_c, sv[b], x[b], tail), h);
+            __stcs(s4 + u, sv[b]);
+        }
     }
 }
 
@@ -297,18 +340,21 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
         float* ll = p.ll_out[ch];
         float* bands = p.coef[ch];
         const float* prev = p.prev[ch];
+        void* const st = p.iir_state[ch];
         for (int jj = warp; jj < nj; jj += NWARP) {
             if (lane >= ni) continue;
             const int j = py0 + jj, ry = qy0 + jj;
             const int o = j * sw + i;
             const bool hy = 2 * j + 1 < ih;
             const bool h = p.h16;
+            float v[3];                                                                         // LH, HH, HL
+            v[0] = hy ? pl[(32 + ry) * RS] : (prev ? pl_ld(prev, o, h) : 0.0f);
+            v[1] = (hx && hy) ? pl[(32 + ry) * RS + ODD_COL] : (prev ? pl_ld(prev, pn + o, h) : 0.0f);
+            v[2] = hx ? pl[ry * RS + ODD_COL] : (prev ? pl_ld(prev, 2 * pn + o, h) : 0.0f);
             pl_st(ll, o, pl[ry * RS], h);
-            pl_st(bands, o, hy ? pl[(32 + ry) * RS] : (prev ? pl_ld(prev, o, h) : 0.0f), h);         // LH
-            pl_st(bands, n + o, (hx && hy) ? pl[(32 + ry) * RS + ODD_COL]
-                                           : (prev ? pl_ld(prev, pn + o, h) : 0.0f), h);           // HH
-            pl_st(bands, 2 * n + o, hx ? pl[ry * RS + ODD_COL] : (prev ? pl_ld(prev, 2 * pn + o, h) : 0.0f),
-                  h);                                                                              // HL
+#pragma unroll
+            for (int b = 0; b < 3; b++) pl_st(bands, b * n + o, v[b], h);
+            if (st) temporal_step3(p, ch, st, o, n, v, h);
         }
     }
 }

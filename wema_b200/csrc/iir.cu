@@ -19,6 +19,7 @@
 // rounded to FP32 once.  Poles near the unit circle (a low f_low at a high
 // frame rate) accumulate FP32 rounding in the recursive state; this keeps it
 // out.  State: {w1_hp, w2_hp} and {w1_lp, w2_lp} as two double2.
+#include "cascade.cuh"
 #include "common.cuh"
 #include "kernels.h"
 #include "multi.cuh"
@@ -48,36 +49,6 @@ struct IirDev {
     float alpha;           // single frame: the channel's alpha
     int warmup;
 };
-
-__device__ __forceinline__ float cascade(const float* c, float4& st, float x, bool tail) {
-    // high-pass section
-    float y = __fmaf_rn(c[0], x, st.x);
-    float w1 = __fmaf_rn(-c[3], y, __fmaf_rn(c[1], x, st.y));
-    float w2 = tail ? __fmaf_rn(c[2], x, -__fmul_rn(c[4], y)) : __fmaf_rn(-c[4], y, __fmul_rn(c[2], x));
-    st.x = w1;
-    st.y = w2;
-    x = y;
-    // low-pass section
-    y = __fmaf_rn(c[5], x, st.z);
-    w1 = __fmaf_rn(-c[8], y, __fmaf_rn(c[6], x, st.w));
-    w2 = tail ? __fmaf_rn(c[7], x, -__fmul_rn(c[9], y)) : __fmaf_rn(-c[9], y, __fmul_rn(c[7], x));
-    st.z = w1;
-    st.w = w2;
-    return y;
-}
-
-// the fp64 variant of cascade(): one rounding, at the end
-__device__ __forceinline__ float cascade64(const float* c, double2& hp, double2& lp, float xf) {
-    const double x = (double)xf;
-    double y = fma((double)c[0], x, hp.x);
-    hp.x = fma(-(double)c[3], y, fma((double)c[1], x, hp.y));
-    hp.y = fma(-(double)c[4], y, (double)c[2] * x);
-    const double x2 = y;
-    y = fma((double)c[5], x2, lp.x);
-    lp.x = fma(-(double)c[8], y, fma((double)c[6], x2, lp.y));
-    lp.y = fma(-(double)c[9], y, (double)c[7] * x2);
-    return __double2float_rn(y);
-}
 
 // level of unique position u, and whether its 6-slot index is in the
 // reference's scalar tail

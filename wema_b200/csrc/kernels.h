@@ -24,6 +24,14 @@ struct FwdLevelParams {
     long long prev_n;
     float* ll_out[3];           // LL (next level's input or the lowpass)
     int h16;                    // src_planes, coef, prev, ll_out are FP16 planes
+    // the temporal filter's step on each coefficient as it is written (IIR
+    // streams after their first frame); iir_state[c] null: off
+    void* iir_state[3];         // this level's biquad state (float4, or 2 x double2 with iir_fp64)
+    float* iir_delta[3];        // this level's band-passed delta planes
+    float iir_c[10];            // {b0,b1,b2,a1,a2} high-pass, then low-pass
+    long long iir_off6;         // this level's first 6-slot index
+    long long iir_simd_end;     // 6-slot indices from here take the scalar-tail form
+    int iir_fp64;
 };
 
 struct InvLevelParams {

@@ -98,6 +98,8 @@ public:
     bool run_on(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, float* out_f32,
                 cudaStream_t st);
     bool sync_all();
+    // the forward transform's temporal-filter fields for level l of the frame being issued
+    void fill_temporal(FwdLevelParams& p, int l) const;
     PyrView view(int b, int c) const;
     bool ensure_staging();
     bool materialize_amplified();      // ampl[] = amplified coefficients of the last frame

@@ -1067,7 +1067,7 @@ __device__ __forceinline__ void thr16_body(const ThrArgs& a, int bx, int by, int
     const int ch = by;
     const PyrView& v = a.v[ch];
     const ThrScratch& sc = a.s[ch];
-    const long long pu = v.uoff[v.levels];
+    const long long pu = v.off6[v.levels] / 2;             // unique positions: half the 6-slot count
     const __half* x = reinterpret_cast<const __half*>(v.coef);
     double acc = 0.0;
     for (long long u = (long long)bx * T16_THREADS + threadIdx.x; u < pu; u += (long long)nblk * T16_THREADS)
@@ -1103,7 +1103,7 @@ __device__ __forceinline__ void thr16_body(const ThrArgs& a, int bx, int by, int
 }
 
 static int thr16_blocks(const PyrView& v) {
-    const long long pu = v.uoff[v.levels];
+    const long long pu = v.off6[v.levels] / 2;
     const long long b = (pu + 8LL * T16_THREADS - 1) / (8LL * T16_THREADS);
     return (int)std::min<long long>(std::max<long long>(b, 1), T16_MAXBLK);
 }
