@@ -216,10 +216,10 @@ STAGE_KERNELS_MULTI = {
 
 # kernels behind each stage (one launch per frame unless noted)
 STAGE_KERNELS = {
-    "fwd_dwt_level0": "k_dwt_fwd<1|2> (level 0, RGB in, with the IIR step)",
-    "fwd_dwt_levels": "k_dwt_fwd<0> x (levels - 1) (with the IIR step)",
+    "fwd_dwt_level0": "k_dwt_fwd<1|2> (level 0, RGB in)",
+    "fwd_dwt_levels": "k_dwt_fwd<0> x (levels - 1)",
     "threshold": "k_thr_monoids + k_thr_walk",
-    "temporal_amplify": "k_iir x channels (first frame only; else inside the forward transform)",
+    "temporal_amplify": "k_iir x channels",
     "inv_dwt_levels": "k_dwt_inv<1,0> x (levels - 1)",
     "inv_dwt_level0": "k_dwt_inv<3,1> (colour, RGB out) / k_dwt_inv<1,0> (luma)",
     "luma_transfer": "k_guided_transfer / k_gauss_transfer",
@@ -1234,7 +1234,7 @@ def main():
     dims = dims_of(w, h)
     pu = sum(3 * sw * sh for sw, sh in dims)
     C = 3 if kw.get("color") else 1
-    sb = stage_bytes(w, h, C, dims, pu)
+    sb = stage_bytes(w, h, C, dims, pu, fused=False)   # a plain session runs the IIR on its own
     per_frame = {k: v / max(nst, 1) for k, v in stages.items()}
     peak, peak_kind = peaks()
     dom = max(per_frame, key=per_frame.get)

@@ -287,7 +287,8 @@ PyrView Session::view(int b, int c) const {
 }
 
 // The forward transform's parameters for running the filter's step on level
-// l's coefficients of the current slot (state, deltas, coefficients, tail bound).
+// l's coefficients of the current slot (state, deltas, coefficients, tail
+// bound): a batched stream after its first frame (Batch::tick).
 void Session::fill_temporal(FwdLevelParams& p, int l) const {
     const Slot& q = slot[(int)(frames_run % nslots)];
     memcpy(p.iir_c, coef10, sizeof coef10);
@@ -322,14 +323,6 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
     if (wait && !cuda_ok(cudaStreamWaitEvent(s_fwd, wait, 0), "stream wait")) return false;
     if (q.valid && !cuda_ok(cudaStreamWaitEvent(s_fwd, q.ev_done, 0), "stream wait")) return false;
 
-    // IIR streams after their first frame: the filter's step runs inside the
-    // forward transform, on each coefficient as it is written (in frame order:
-    // every forward runs on s_fwd; after the first frame it also waits for
-    // that frame's separate preseed and filter)
-    const bool fuse = cfg.use_iir && frames_processed > 0;
-    if (fuse && last_slot >= 0 && !cuda_ok(cudaStreamWaitEvent(s_fwd, slot[last_slot].ev_tmp, 0), "stream wait"))
-        return false;
-
     // ---- forward DWT
     mark(2 * ST_FWD0, s_fwd);
     for (int l = 0; l < L; l++) {
@@ -358,7 +351,6 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
         }
         p.prev_n = l > 0 ? g.n[l - 1] : 0;
         p.h16 = h;
-        if (fuse) fill_temporal(p, l);
         if (!cuda_ok(launch_dwt_fwd(mode, nch, p, s_fwd), "forward DWT")) return false;
         launches++;
         if (l == 0) {
@@ -386,12 +378,14 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
         frames_processed++;
         q.alpha[0] = amp;
         q.alpha[1] = q.alpha[2] = amp * 0.5f;
-        if (!fuse) {
-            for (int c = 0; c < nch; c++)
-                if (!cuda_ok(launch_iir(ip, q.coef[c], state[c], cfg.iir_state_fp64, q.delta[c], s_tmp), "IIR"))
-                    return false;
-            launches += nch;
-        }
+        // (a batched stream runs this step inside its forward transform after
+        // its first frame, Batch::tick; here the filter is its own launch on
+        // s_tmp, beside the threshold - the shorter latency for a frame that
+        // is waited for)
+        for (int c = 0; c < nch; c++)
+            if (!cuda_ok(launch_iir(ip, q.coef[c], state[c], cfg.iir_state_fp64, q.delta[c], s_tmp), "IIR"))
+                return false;
+        launches += nch;
     } else {
         for (int c = 0; c < nch; c++)
             if (!cuda_ok(launch_ring_push(q.coef[c], cfg.planes_fp16, ring[c], cfg.ring_fp16, pu, head, s_tmp),
