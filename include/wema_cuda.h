@@ -207,6 +207,13 @@ int wema_cuda_batch_tick_host(wema_cuda_batch *b, const int *ids, const void *co
  * stream, the WEMA_CUDA_STAGES order of wema_cuda_stage_times): times_ms[7]
  * receives the milliseconds summed over every timed tick, *ticks their
  * count.  Both wait for the batch. */
+/* A steady tick - every listed stream past its first frame, stage timing
+ * off - replays CUDA graphs of its launches (forward transforms and
+ * threshold; inverse transforms; luma transfer), captured per parameter
+ * table and set of launches, with the same kernels, parameters and results
+ * as the launches themselves; the waits between the three stay stream
+ * operations.  enable = 0: launch the kernels one by one; default 1. */
+int wema_cuda_batch_set_graphs(wema_cuda_batch *b, int enable);
 /* enable = 0: a host tick's copies in also wait for the previous tick to
  * finish (no overlap of copies in with kernels); default 1. */
 int wema_cuda_batch_set_host_overlap(wema_cuda_batch *b, int enable);

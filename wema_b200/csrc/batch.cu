@@ -89,6 +89,14 @@ WEMA_API int wema_cuda_batch_tick_host(wema_cuda_batch* b, const int* ids, const
                : -1;
 }
 
+WEMA_API int wema_cuda_batch_set_graphs(wema_cuda_batch* b, int enable) {
+    clear_error();
+    if (!b) { set_error("null argument"); return -1; }
+    std::lock_guard<std::mutex> lk(b->mu);
+    b->b.use_graphs = enable != 0;
+    return 0;
+}
+
 WEMA_API int wema_cuda_batch_set_host_overlap(wema_cuda_batch* b, int enable) {
     clear_error();
     if (!b) { set_error("null argument"); return -1; }

@@ -87,6 +87,9 @@ public:
     int max_streams = 0;
     std::vector<Session*> streams;        // by id; null when removed
     cudaStream_t st_main = nullptr, st_iir = nullptr, st_xfer = nullptr;
+    // streams' state is allocated and zeroed on its own stream: a tick being
+    // captured into a graph on st_main from another thread must not see it
+    cudaStream_t st_alloc = nullptr;
     cudaEvent_t ev_fwd = nullptr, ev_iir = nullptr, ev_inv = nullptr, ev_xfer = nullptr;
     bool xfer_pending = false;            // ev_xfer marks a transfer tick t+1 must wait for
     static constexpr int NBUF = 3;
@@ -98,7 +101,15 @@ public:
         bool used = false;
         cudaEvent_t tev[T_COUNT][2] = {};  // stage start / end (timing on)
         bool timed = false;               // tev holds a tick not yet added to stage_ms
+        // steady ticks replay CUDA graphs of their launches, one set per table:
+        // forward + threshold, inverse, transfer (the waits between them stay
+        // stream operations, so the next tick's forward still overlaps this
+        // tick's transfer); `sig` identifies the launches they hold
+        cudaGraphExec_t g_fwd = nullptr, g_inv = nullptr, g_xfer = nullptr;
+        std::vector<long long> sig;
     } tb[NBUF];
+    bool use_graphs = true;
+    long long per_graph_launches = 0;  // kernels in one replay of a table's graphs
     bool timing = false;
     double stage_ms[T_COUNT] = {};
     long long ticks_timed = 0;
@@ -131,7 +142,7 @@ public:
     std::vector<char> image;
 
     ~Batch() {
-        for (cudaStream_t st : {st_main, st_iir, st_xfer, st_h2d, st_d2h})
+        for (cudaStream_t st : {st_main, st_iir, st_xfer, st_h2d, st_d2h, st_alloc})
             if (st) cudaStreamSynchronize(st);
         for (HostSet& h : hs) {
             if (h.din) cudaFree(h.din);
@@ -139,6 +150,7 @@ public:
         }
         for (Session* s : streams) delete s;
         for (Table& t : tb) {
+            drop_graphs(t);
             if (t.host) cudaFreeHost(t.host);
             if (t.dev) cudaFree(t.dev);
             if (t.done) cudaEventDestroy(t.done);
@@ -146,7 +158,7 @@ public:
                 for (cudaEvent_t e : p)
                     if (e) cudaEventDestroy(e);
         }
-        for (cudaStream_t st : {st_main, st_iir, st_xfer, st_h2d, st_d2h})
+        for (cudaStream_t st : {st_main, st_iir, st_xfer, st_h2d, st_d2h, st_alloc})
             if (st) cudaStreamDestroy(st);
         for (cudaEvent_t e : {ev_fwd, ev_iir, ev_inv, ev_xfer})
             if (e) cudaEventDestroy(e);
@@ -176,7 +188,7 @@ public:
             return false;
         if (!cuda_ok(cudaStreamCreateWithPriority(&st_xfer, cudaStreamNonBlocking, lo), "cudaStreamCreate"))
             return false;
-        for (cudaStream_t* st : {&st_h2d, &st_d2h})
+        for (cudaStream_t* st : {&st_h2d, &st_d2h, &st_alloc})
             if (!cuda_ok(cudaStreamCreateWithFlags(st, cudaStreamNonBlocking), "cudaStreamCreate"))
                 return false;
         for (HostSet& h : hs)
@@ -204,15 +216,16 @@ public:
         return s ? insert(s) : -1;
     }
 
-    // A stream's state, allocated and zeroed in order on the batch's main
-    // stream; the batch itself is untouched, so another host thread may call
-    // this while ticks are issued (then insert() it from the ticking thread).
+    // A stream's state, allocated and zeroed on the allocation stream, which
+    // this call then waits for (so the state is ready for any later tick); the
+    // batch itself is untouched, so another host thread may call this while
+    // ticks are issued (then insert() it from the ticking thread).
     Session* make(const wema_cuda_config& c) {
         if (!c.use_iir) { set_error("batched streams use the IIR filter (use_iir = 1)"); return nullptr; }
         if (c.device != device) { set_error("stream device %d differs from the batch's %d", c.device, device); return nullptr; }
         Session* s = new (std::nothrow) Session();
         if (!s) { set_error("out of host memory"); return nullptr; }
-        if (!s->init(c, 1, st_main)) {
+        if (!s->init(c, 1, st_alloc) || !cuda_ok(cudaStreamSynchronize(st_alloc), "state allocation")) {
             delete s;
             return nullptr;
         }
@@ -351,6 +364,31 @@ public:
         S.used = true;
         hcur = (hcur + 1) % 3;
         return true;
+    }
+
+    static void drop_graphs(Table& t) {
+        for (cudaGraphExec_t* g : {&t.g_fwd, &t.g_inv, &t.g_xfer})
+            if (*g) {
+                cudaGraphExecDestroy(*g);
+                *g = nullptr;
+            }
+        t.sig.clear();
+    }
+
+    // records what `issue` launches on `st` as a graph (nothing runs)
+    template <class F>
+    bool capture(cudaStream_t st, cudaGraphExec_t* out, F issue) {
+        if (!cuda_ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture")) return false;
+        const bool ok = issue();
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(st, &g);
+        if (!ok || !cuda_ok(e, "end capture")) {
+            if (g) cudaGraphDestroy(g);
+            return false;
+        }
+        const bool inst = cuda_ok(cudaGraphInstantiate(out, g, 0), "graph instantiate");
+        cudaGraphDestroy(g);
+        return inst;
     }
 
     // the table image: every launch's parameter array, then its task map
@@ -543,53 +581,103 @@ public:
                 for (cudaEvent_t& e : p)
                     if (!cuda_ok(cudaEventCreate(&e), "cudaEventCreate")) return false;
 
-        // forward, then the filter beside the threshold
-        if (!mark(T_FWD0, 0, st_main)) return false;
-        if (!go(L_FWD0_LUMA, [&] { return launch_dwt_fwd_multi(kSrcRgbU8, 1, (const FwdLevelParams*)P(L_FWD0_LUMA), M(L_FWD0_LUMA), L[L_FWD0_LUMA].total, st_main); }, "forward DWT"))
-            return false;
-        if (!go(L_FWD0_COLOR, [&] { return launch_dwt_fwd_multi(kSrcRgbU8, 3, (const FwdLevelParams*)P(L_FWD0_COLOR), M(L_FWD0_COLOR), L[L_FWD0_COLOR].total, st_main); }, "forward DWT"))
-            return false;
-        if (!mark(T_FWD0, 1, st_main) || !mark(T_FWD, 0, st_main)) return false;
-        for (int k = L_FWD1; k <= L_FWD3; k++)
-            if (!go(k, [&] { return launch_dwt_fwd_multi(kSrcPlanes, 1, (const FwdLevelParams*)P(k), M(k), L[k].total, st_main); }, "forward DWT"))
+        // the launches in three groups; a steady tick (every stream past its
+        // first frame: no preseed, filter or threshold prefix launches, timing
+        // off) replays them as CUDA graphs captured for this table and set of
+        // launches
+        auto fwd = [&] {
+            if (!mark(T_FWD0, 0, st_main)) return false;
+            if (!go(L_FWD0_LUMA, [&] { return launch_dwt_fwd_multi(kSrcRgbU8, 1, (const FwdLevelParams*)P(L_FWD0_LUMA), M(L_FWD0_LUMA), L[L_FWD0_LUMA].total, st_main); }, "forward DWT"))
                 return false;
-        if (!mark(T_FWD, 1, st_main)) return false;
-        if (!cuda_ok(cudaEventRecord(ev_fwd, st_main), "event record")) return false;
-        if (!mark(T_THR, 0, st_main)) return false;
-        for (int k = L_THR_PART; k <= L_THR16; k++)
-            if (!go(k, [&] { return launch_threshold_multi(k - L_THR_PART, P(k), M(k), L[k].total, st_main); }, "threshold"))
+            if (!go(L_FWD0_COLOR, [&] { return launch_dwt_fwd_multi(kSrcRgbU8, 3, (const FwdLevelParams*)P(L_FWD0_COLOR), M(L_FWD0_COLOR), L[L_FWD0_COLOR].total, st_main); }, "forward DWT"))
                 return false;
-        if (!mark(T_THR, 1, st_main)) return false;
-        if (!cuda_ok(cudaStreamWaitEvent(st_iir, ev_fwd, 0), "stream wait")) return false;
-        if (!mark(T_IIR, 0, st_iir)) return false;
-        if (!go(L_IIR_PRESEED, [&] { return launch_iir_multi(P(L_IIR_PRESEED), M(L_IIR_PRESEED), L[L_IIR_PRESEED].total, 1, st_iir); }, "IIR preseed"))
-            return false;
-        if (!go(L_IIR, [&] { return launch_iir_multi(P(L_IIR), M(L_IIR), L[L_IIR].total, 0, st_iir); }, "IIR"))
-            return false;
-        if (!mark(T_IIR, 1, st_iir)) return false;
-        if (!cuda_ok(cudaEventRecord(ev_iir, st_iir), "event record")) return false;
-        if (!cuda_ok(cudaStreamWaitEvent(st_main, ev_iir, 0), "stream wait")) return false;
-        // the previous tick's transfer still reads its reconstructed luma
-        if (xfer_pending && !cuda_ok(cudaStreamWaitEvent(st_main, ev_xfer, 0), "stream wait")) return false;
-        if (!mark(T_INV, 0, st_main)) return false;
-        for (int k = L_INV3; k <= L_INV1; k++)
-            if (!go(k, [&] { return launch_dwt_inv_multi(1, kOutPlanes, (const InvLevelParams*)P(k), M(k), L[k].total, st_main); }, "inverse DWT"))
+            if (!mark(T_FWD0, 1, st_main) || !mark(T_FWD, 0, st_main)) return false;
+            for (int k = L_FWD1; k <= L_FWD3; k++)
+                if (!go(k, [&] { return launch_dwt_fwd_multi(kSrcPlanes, 1, (const FwdLevelParams*)P(k), M(k), L[k].total, st_main); }, "forward DWT"))
+                    return false;
+            return mark(T_FWD, 1, st_main);
+        };
+        auto thr = [&] {
+            if (!mark(T_THR, 0, st_main)) return false;
+            for (int k = L_THR_PART; k <= L_THR16; k++)
+                if (!go(k, [&] { return launch_threshold_multi(k - L_THR_PART, P(k), M(k), L[k].total, st_main); }, "threshold"))
+                    return false;
+            return mark(T_THR, 1, st_main);
+        };
+        auto fwd_thr = [&] { return fwd() && thr(); };
+        auto inverse = [&] {
+            if (!mark(T_INV, 0, st_main)) return false;
+            for (int k = L_INV3; k <= L_INV1; k++)
+                if (!go(k, [&] { return launch_dwt_inv_multi(1, kOutPlanes, (const InvLevelParams*)P(k), M(k), L[k].total, st_main); }, "inverse DWT"))
+                    return false;
+            if (!mark(T_INV, 1, st_main) || !mark(T_INV0, 0, st_main)) return false;
+            if (!go(L_INV0_LUMA, [&] { return launch_dwt_inv_multi(1, kOutPlanes, (const InvLevelParams*)P(L_INV0_LUMA), M(L_INV0_LUMA), L[L_INV0_LUMA].total, st_main); }, "inverse DWT"))
                 return false;
-        if (!mark(T_INV, 1, st_main) || !mark(T_INV0, 0, st_main)) return false;
-        if (!go(L_INV0_LUMA, [&] { return launch_dwt_inv_multi(1, kOutPlanes, (const InvLevelParams*)P(L_INV0_LUMA), M(L_INV0_LUMA), L[L_INV0_LUMA].total, st_main); }, "inverse DWT"))
-            return false;
-        if (!go(L_INV0_COLOR, [&] { return launch_dwt_inv_multi(3, kOutRgb, (const InvLevelParams*)P(L_INV0_COLOR), M(L_INV0_COLOR), L[L_INV0_COLOR].total, st_main); }, "inverse DWT"))
-            return false;
-        if (!mark(T_INV0, 1, st_main)) return false;
-        // the transfer on its own stream, so the next tick's forward half overlaps it
-        if (!cuda_ok(cudaEventRecord(ev_inv, st_main), "event record")) return false;
-        if (!cuda_ok(cudaStreamWaitEvent(st_xfer, ev_inv, 0), "stream wait")) return false;
-        if (!mark(T_XFER, 0, st_xfer)) return false;
-        if (!go(L_XFER_GUIDED, [&] { return launch_transfer_multi(1, (const TransferParams*)P(L_XFER_GUIDED), M(L_XFER_GUIDED), L[L_XFER_GUIDED].total, st_xfer); }, "luma transfer"))
-            return false;
-        if (!go(L_XFER_GAUSS, [&] { return launch_transfer_multi(0, (const TransferParams*)P(L_XFER_GAUSS), M(L_XFER_GAUSS), L[L_XFER_GAUSS].total, st_xfer); }, "luma transfer"))
-            return false;
-        if (!mark(T_XFER, 1, st_xfer)) return false;
+            if (!go(L_INV0_COLOR, [&] { return launch_dwt_inv_multi(3, kOutRgb, (const InvLevelParams*)P(L_INV0_COLOR), M(L_INV0_COLOR), L[L_INV0_COLOR].total, st_main); }, "inverse DWT"))
+                return false;
+            return mark(T_INV0, 1, st_main);
+        };
+        auto transfer = [&] {
+            if (!mark(T_XFER, 0, st_xfer)) return false;
+            if (!go(L_XFER_GUIDED, [&] { return launch_transfer_multi(1, (const TransferParams*)P(L_XFER_GUIDED), M(L_XFER_GUIDED), L[L_XFER_GUIDED].total, st_xfer); }, "luma transfer"))
+                return false;
+            if (!go(L_XFER_GAUSS, [&] { return launch_transfer_multi(0, (const TransferParams*)P(L_XFER_GAUSS), M(L_XFER_GAUSS), L[L_XFER_GAUSS].total, st_xfer); }, "luma transfer"))
+                return false;
+            return mark(T_XFER, 1, st_xfer);
+        };
+        const bool steady = use_graphs && !timing && L[L_IIR].n() == 0 && L[L_IIR_PRESEED].n() == 0 &&
+                            L[L_THR_PART].n() == 0 && L[L_THR_PREFIX].n() == 0;
+        if (steady) {
+            // what the graphs hold: the table, every launch's blocks and offsets,
+            // the device's kernel variants
+            std::vector<long long> sig = {(long long)(uintptr_t)t.dev, dwt_variant(device, 0), dwt_variant(device, 1)};
+            for (const Launch& l : L) {
+                sig.push_back(l.total);
+                sig.push_back((long long)l.params_off);
+                sig.push_back((long long)l.map_off);
+            }
+            if (sig != t.sig) {
+                drop_graphs(t);
+                const long long before = launches;
+                if (!capture(st_main, &t.g_fwd, fwd_thr) || !capture(st_main, &t.g_inv, inverse) ||
+                    !capture(st_xfer, &t.g_xfer, transfer)) {
+                    drop_graphs(t);
+                    return false;
+                }
+                per_graph_launches = launches - before;
+                launches = before;
+                t.sig = sig;
+            }
+            launches += per_graph_launches;
+            if (!cuda_ok(cudaGraphLaunch(t.g_fwd, st_main), "graph launch")) return false;
+            // the previous tick's transfer still reads its reconstructed luma
+            if (xfer_pending && !cuda_ok(cudaStreamWaitEvent(st_main, ev_xfer, 0), "stream wait")) return false;
+            if (!cuda_ok(cudaGraphLaunch(t.g_inv, st_main), "graph launch")) return false;
+            if (!cuda_ok(cudaEventRecord(ev_inv, st_main), "event record")) return false;
+            if (!cuda_ok(cudaStreamWaitEvent(st_xfer, ev_inv, 0), "stream wait")) return false;
+            if (!cuda_ok(cudaGraphLaunch(t.g_xfer, st_xfer), "graph launch")) return false;
+        } else {
+            // forward, then the filter (first frames) beside the threshold
+            if (!fwd()) return false;
+            if (!cuda_ok(cudaEventRecord(ev_fwd, st_main), "event record")) return false;
+            if (!thr()) return false;
+            if (!cuda_ok(cudaStreamWaitEvent(st_iir, ev_fwd, 0), "stream wait")) return false;
+            if (!mark(T_IIR, 0, st_iir)) return false;
+            if (!go(L_IIR_PRESEED, [&] { return launch_iir_multi(P(L_IIR_PRESEED), M(L_IIR_PRESEED), L[L_IIR_PRESEED].total, 1, st_iir); }, "IIR preseed"))
+                return false;
+            if (!go(L_IIR, [&] { return launch_iir_multi(P(L_IIR), M(L_IIR), L[L_IIR].total, 0, st_iir); }, "IIR"))
+                return false;
+            if (!mark(T_IIR, 1, st_iir)) return false;
+            if (!cuda_ok(cudaEventRecord(ev_iir, st_iir), "event record")) return false;
+            if (!cuda_ok(cudaStreamWaitEvent(st_main, ev_iir, 0), "stream wait")) return false;
+            // the previous tick's transfer still reads its reconstructed luma
+            if (xfer_pending && !cuda_ok(cudaStreamWaitEvent(st_main, ev_xfer, 0), "stream wait")) return false;
+            if (!inverse()) return false;
+            // the transfer on its own stream, so the next tick's forward half overlaps it
+            if (!cuda_ok(cudaEventRecord(ev_inv, st_main), "event record")) return false;
+            if (!cuda_ok(cudaStreamWaitEvent(st_xfer, ev_inv, 0), "stream wait")) return false;
+            if (!transfer()) return false;
+        }
         if (!cuda_ok(cudaEventRecord(ev_xfer, st_xfer), "event record")) return false;
         xfer_pending = true;
         t.timed = timing;

@@ -134,9 +134,9 @@ public:
         const size_t want = std::min(budget, free_b > margin ? free_b - margin : (size_t)0);
         if (want == 0) return true;
         void* p = nullptr;
-        if (!cuda_ok(cudaMallocAsync(&p, want, batch.st_main), "cudaMallocAsync(reserve)")) return false;
-        if (!cuda_ok(cudaFreeAsync(p, batch.st_main), "cudaFreeAsync(reserve)")) return false;
-        return cuda_ok(cudaStreamSynchronize(batch.st_main), "reserve sync");
+        if (!cuda_ok(cudaMallocAsync(&p, want, batch.st_alloc), "cudaMallocAsync(reserve)")) return false;
+        if (!cuda_ok(cudaFreeAsync(p, batch.st_alloc), "cudaFreeAsync(reserve)")) return false;
+        return cuda_ok(cudaStreamSynchronize(batch.st_alloc), "reserve sync");
     }
 
     // allocation thread: Batch::make touches no batch state

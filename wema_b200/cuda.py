@@ -109,6 +109,7 @@ def lib() -> C.CDLL:
         L.wema_cuda_batch_restore.argtypes = [vp, i, vp, sz]
         L.wema_cuda_batch_set_timing.argtypes = [vp, i]
         L.wema_cuda_batch_set_host_overlap.argtypes = [vp, i]
+        L.wema_cuda_batch_set_graphs.argtypes = [vp, i]
         L.wema_cuda_batch_stage_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
         L.wema_cuda_batch_stats.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                                             C.POINTER(i)]
@@ -345,6 +346,9 @@ class Batch:
         w = C.c_void_p(wait_event.cuda_event) if wait_event is not None else None
         d = C.c_void_p(done_event.cuda_event) if done_event is not None else None
         _check(lib().wema_cuda_batch_tick_host(self.h, ia, pin, pout, n, w, d), "batch_tick_host")
+
+    def set_graphs(self, enable: bool):
+        _check(lib().wema_cuda_batch_set_graphs(self.h, int(bool(enable))), "set_graphs")
 
     def set_host_overlap(self, enable: bool):
         _check(lib().wema_cuda_batch_set_host_overlap(self.h, int(bool(enable))), "set_host_overlap")
