@@ -199,7 +199,8 @@ int wema_cuda_batch_sync(wema_cuda_batch *b);
  * that lie back to back in host memory (in `ids` order) move in one copy;
  * many small copies in both directions at once run well below the host
  * link's rate.  Asynchronous: the copies in wait for wait_event (may be NULL)
- * and for the staging set's previous tick; a host buffer may be reused once
+ * and for the previous tick (see wema_cuda_batch_set_host_overlap); a host
+ * buffer may be reused once
  * done_event (may be NULL) has completed, or after wema_cuda_batch_sync. */
 int wema_cuda_batch_tick_host(wema_cuda_batch *b, const int *ids, const void *const *h_in_u8,
                               void *const *h_out_u8, int n, void *wait_event, void *done_event);
@@ -214,8 +215,10 @@ int wema_cuda_batch_tick_host(wema_cuda_batch *b, const int *ids, const void *co
  * as the launches themselves; the waits between the three stay stream
  * operations.  enable = 0: launch the kernels one by one; default 1. */
 int wema_cuda_batch_set_graphs(wema_cuda_batch *b, int enable);
-/* enable = 0: a host tick's copies in also wait for the previous tick to
- * finish (no overlap of copies in with kernels); default 1. */
+/* enable = 1: a host tick's copies in start as soon as their staging set is
+ * free, beside the previous tick's kernels and copies out.  Default 0: they
+ * also wait for the previous tick to finish (measured faster on B200 hosts:
+ * copies beside the tick's kernels ran well below the host link's rate). */
 int wema_cuda_batch_set_host_overlap(wema_cuda_batch *b, int enable);
 int wema_cuda_batch_set_timing(wema_cuda_batch *b, int enable);
 int wema_cuda_batch_stage_times(wema_cuda_batch *b, double *times_ms, long long *ticks);
