@@ -950,7 +950,7 @@ def bench_precision(a, rank, world, local):
                      "delta_rel_l2_vs_fp64": {"max": float(max(rel[v])), "last": rel[v][-1]},
                      "delta_max_abs_vs_fp64": absmax[v],
                      "output_vs_fp64": cmp(outs[v], out64), "output_vs_reference": cmp(outs[v], out_ref)}
-    iir["fp16_planes"]["plane_bytes"] = "coefficient, delta, LL and reconstructed planes in FP16 (half the FP32 bytes)"
+    iir["fp16_planes"]["plane_bytes"] = "coefficient and delta planes and the reconstructed frame in FP16 (half the FP32 bytes)"
     iir["fp16_planes"]["output_vs_fp32_state"] = cmp(outs["h16"], outs[False].astype(int))
     for s in sess.values():
         s.close()

@@ -49,11 +49,11 @@ typedef struct {
     int   ring_fp16;         /* precision variant, window mode: the temporal ring stored
                                 in FP16 (round to nearest), arithmetic in FP32; halves
                                 the ring's bytes (read ws times per position per frame) */
-    int   planes_fp16;       /* precision variant: the pyramid's planes - detail
-                                coefficients, band-passed deltas, LL and reconstructed
-                                planes up to the reconstructed frame - stored in FP16
-                                (round to nearest), arithmetic in FP32; the IIR state
-                                stays FP32.  The threshold is then the FP64 sum of the
+    int   planes_fp16;       /* precision variant: the detail-coefficient and band-passed
+                                delta planes and the reconstructed frame (the level-0
+                                reconstruction) stored in FP16 (round to nearest),
+                                arithmetic in FP32; the IIR state and the LL / coarser
+                                reconstruction planes stay FP32.  The threshold is then the FP64 sum of the
                                 FP16 coefficients rounded once, not the reference's
                                 bit-exact FP32 sum: outputs are NOT within the bit-exact /
                                 1-LSB parity bars of the FP32 path (their error against an

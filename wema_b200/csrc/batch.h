@@ -514,6 +514,7 @@ public:
                 iq.n = g.n[l];
                 iq.thr = q.thr;
                 iq.h16 = S.cfg.planes_fp16;
+                iq.out16 = S.cfg.planes_fp16 && l == 0;
                 for (int c = 0; c < nch; c++) {
                     iq.ll[c] = (l == LV - 1) ? q.ll[c][LV - 1] : q.rec[c][l + 1];
                     iq.coef[c] = plane_at(q.coef[c], g.uoff[l], iq.h16);

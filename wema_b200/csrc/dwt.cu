@@ -158,6 +158,21 @@ __device__ __forceinline__ void temporal_step3(const FwdLevelParams& p, int ch, 
     }
 }
 
+// Bulk L2 prefetch (cp.async.bulk.prefetch.L2) of the IIR state of a tile's
+// positions: per band, each of the tile's rows is one contiguous run of
+// min(TP, sw - px0) positions (16 B each, or 32 B with the FP64 state), so
+// the sizes and addresses are multiples of 16 bytes.  One thread per run.
+__device__ __forceinline__ void prefetch_state_rows(const FwdLevelParams& p, int ch, int px0, int py0) {
+    const int ni = min(TP, p.sw - px0), nj = min(TP, p.sh - py0);
+    const int k = threadIdx.x;
+    if (ni <= 0 || k >= 3 * nj) return;
+    const int b = k / nj, jj = k - b * nj;
+    const long long u = (long long)b * p.n + (long long)(py0 + jj) * p.sw + px0;
+    const int esz = p.iir_fp64 ? 32 : 16;
+    const char* a = static_cast<const char*>(p.iir_state[ch]) + u * esz;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(ni * esz) : "memory");
+}
+
 // ----------------------------------------------------------------- forward
 // C == 3: level 0 of a colour frame, all channels in one CTA, grid (tx, ty, 1).
 // C == 1: channel blockIdx.z (planes in), or the luma of an RGB frame.
@@ -173,6 +188,10 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
     const int RW = min(SEG, iw - rx0), RH = min(SEG, ih - ry0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
+    // the IIR state rows this tile's write-out will update: bulk prefetches
+    // into L2 now, so the epilogue's state loads do not wait on DRAM
+    if (C == 1 && p.iir_state[ch0]) prefetch_state_rows(p, ch0, px0, py0);
+
     // ---- staging: one warp per region row
     if (MODE == kSrcRgbU8) {
         for (int i = threadIdx.x; i < 256; i += DWT_THREADS) lut[i] = __fdiv_rn((float)i, 255.0f);
@@ -186,8 +205,8 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
         for (int r = 0; r < RPW; r++) {
             const int ly = warp + r * NWARP;
             const int row0 = (ry0 + ly) * iw + rx0;
-            v[r][0] = (ly < RH && lane < RW) ? pl_ld(p.src_planes[ch0], row0 + lane, p.h16) : 0.0f;
-            v[r][1] = (ly < RH && lane + 32 < RW) ? pl_ld(p.src_planes[ch0], row0 + lane + 32, p.h16) : 0.0f;
+            v[r][0] = (ly < RH && lane < RW) ? __ldg(p.src_planes[ch0] + row0 + lane) : 0.0f;
+            v[r][1] = (ly < RH && lane + 32 < RW) ? __ldg(p.src_planes[ch0] + row0 + lane + 32) : 0.0f;
         }
 #pragma unroll
         for (int r = 0; r < RPW; r++) {
@@ -351,7 +370,7 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
             v[0] = hy ? pl[(32 + ry) * RS] : (prev ? pl_ld(prev, o, h) : 0.0f);
             v[1] = (hx && hy) ? pl[(32 + ry) * RS + ODD_COL] : (prev ? pl_ld(prev, pn + o, h) : 0.0f);
             v[2] = hx ? pl[ry * RS + ODD_COL] : (prev ? pl_ld(prev, 2 * pn + o, h) : 0.0f);
-            pl_st(ll, o, pl[ry * RS], h);
+            ll[o] = pl[ry * RS];
 #pragma unroll
             for (int b = 0; b < 3; b++) pl_st(bands, b * n + o, v[b], h);
             if (st) temporal_step3(p, ch, st, o, n, v, h);
@@ -395,7 +414,7 @@ __device__ __forceinline__ void dwt_inv_body(const InvLevelParams& p, int bx, in
                 const int qy = warp + NWARP * u;
                 const bool ok = okx && 2 * qy + (q >> 1) < RH;
                 const int o = o0 + qy * sw;
-                xv[cc][q][u] = ok ? pl_ld(src, o, p.h16) : 0.0f;
+                xv[cc][q][u] = ok ? pl_ld(src, o, q != 0 && p.h16) : 0.0f;
                 if (q != 0) dv[cc][q - 1][u] = ok ? pl_ld(dsrc, o, p.h16) : 0.0f;
             }
         }
@@ -467,15 +486,15 @@ __device__ __forceinline__ void dwt_inv_body(const InvLevelParams& p, int bx, in
             const int idx = pr + pcol(lx);
             if (OUT == kOutPlanes) {
 #pragma unroll
-                for (int cc = 0; cc < C; cc++) pl_st(p.out_planes[c0 + cc], pi, planes[cc * PLANE + idx], p.h16);
+                for (int cc = 0; cc < C; cc++) pl_st(p.out_planes[c0 + cc], pi, planes[cc * PLANE + idx], p.out16);
             } else {
                 const float y = planes[idx];
                 const float cb = planes[(C > 1 ? PLANE : 0) + idx];
                 const float cr = planes[(C > 2 ? 2 * PLANE : 0) + idx];
                 if (p.out_planes[0]) {
-                    pl_st(p.out_planes[0], pi, y, p.h16);
-                    pl_st(p.out_planes[1], pi, cb, p.h16);
-                    pl_st(p.out_planes[2], pi, cr, p.h16);
+                    pl_st(p.out_planes[0], pi, y, p.out16);
+                    pl_st(p.out_planes[1], pi, cb, p.out16);
+                    pl_st(p.out_planes[2], pi, cr, p.out16);
                 }
                 float r, g, b;
                 ycbcr_to_rgb(y, cb, cr, r, g, b);

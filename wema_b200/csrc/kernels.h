@@ -23,7 +23,7 @@ struct FwdLevelParams {
     const float* prev[3];       // previous level's bands (stale entries), or null
     long long prev_n;
     float* ll_out[3];           // LL (next level's input or the lowpass)
-    int h16;                    // src_planes, coef, prev, ll_out are FP16 planes
+    int h16;                    // coef and prev are FP16 planes (src_planes, ll_out stay FP32)
     // the temporal filter's step on each coefficient as it is written (IIR
     // streams after their first frame); iir_state[c] null: off
     void* iir_state[3];         // this level's biquad state (float4, or 2 x double2 with iir_fp64)
@@ -46,7 +46,8 @@ struct InvLevelParams {
     float* out_planes[3];       // reconstructed planes (kOutPlanes), optional for kOutRgb
     uint8_t* out_u8;            // kOutRgb: RGB24 output (optional)
     float* out_f32;             // kOutRgb: float RGB output (optional)
-    int h16;                    // ll, coef, delta, out_planes are FP16 planes
+    int h16;                    // coef and delta are FP16 planes (ll stays FP32)
+    int out16;                  // out_planes are FP16 (the level-0 reconstruction of planes_fp16)
 };
 
 cudaError_t dwt_prepare_device();

@@ -120,15 +120,19 @@ static void layout(Arena& A, Session& s) {
     const long long n6 = g.off6[g.levels];
     for (int b = 0; b < s.nslots; b++) {
         Slot& q = s.slot[b];
-        // pyramid planes: FP32, or FP16 in the planes_fp16 variant (float* kept)
-        auto plane = [&](long long n) {
-            return s.cfg.planes_fp16 ? reinterpret_cast<float*>(A.take<uint16_t>(n)) : A.take<float>(n);
+        // planes_fp16: coefficient and delta planes and the level-0 reconstruction
+        // (the frame) in FP16 (float* kept); the LL and coarser reconstructions
+        // stay FP32 - their values grow about 2x per level, so FP16 there would
+        // quantise the coarse bands far more coarsely than the frame
+        auto plane = [&](long long n, bool h) {
+            return h ? reinterpret_cast<float*>(A.take<uint16_t>(n)) : A.take<float>(n);
         };
+        const bool h = s.cfg.planes_fp16;
         for (int c = 0; c < s.nch; c++) {
-            q.coef[c] = plane(pu);
-            q.delta[c] = plane(pu);
-            for (int l = 0; l < g.levels; l++) q.ll[c][l] = plane(g.n[l]);
-            for (int l = 0; l < g.levels; l++) q.rec[c][l] = plane((long long)g.in_w[l] * g.in_h[l]);
+            q.coef[c] = plane(pu, h);
+            q.delta[c] = plane(pu, h);
+            for (int l = 0; l < g.levels; l++) q.ll[c][l] = plane(g.n[l], false);
+            for (int l = 0; l < g.levels; l++) q.rec[c][l] = plane((long long)g.in_w[l] * g.in_h[l], h && l == 0);
             q.gray_in[c] = A.take<float>(g.pixels);
         }
         q.thr = A.take<float>(8);
@@ -466,6 +470,7 @@ bool Session::run(const uint8_t* in_u8, const float* in_f32, uint8_t* out_u8, fl
             iq.thr = q.thr;
             const bool h = cfg.planes_fp16;
             iq.h16 = h;
+            iq.out16 = h && l == 0;
             for (int c = 0; c < nch; c++) {
                 iq.ll[c] = (l == L - 1) ? q.ll[c][L - 1] : q.rec[c][l + 1];
                 iq.coef[c] = plane_at(q.coef[c], g.uoff[l], h);
@@ -875,7 +880,7 @@ WEMA_API long wema_cuda_session_read(wema_cuda_session* s, int what, int channel
         case WEMA_CUDA_READ_AMP6:
             if (!S.materialize_amplified()) return -1;
             return rd6(S.ampl[channel], false);
-        case WEMA_CUDA_READ_LOWPASS: return rd(q.ll[channel][g.levels - 1], g.low_n, h16);
+        case WEMA_CUDA_READ_LOWPASS: return rd(q.ll[channel][g.levels - 1], g.low_n, false);
         case WEMA_CUDA_READ_THRESHOLD: return rd(q.thr, S.nch, false);
         case WEMA_CUDA_READ_MAGSUM: return rd(q.thr + 4, S.nch, false);
     }

@@ -82,8 +82,7 @@ constexpr int GR = 4;                   // guided-filter radius (wema.c:314)
 constexpr int GS_IN = 128;              // input columns per strip (4 per lane)
 constexpr int GS_OUT = GS_IN - 4 * GR;  // output columns per strip
 constexpr int GS_RING = 2 * GR + 1;     // rows in each ring
-constexpr int GS_WARPS = 1;             // strips per CTA (one per warp): a CTA frees its
-                                        // shared memory as soon as its own strip is done
+constexpr int GS_WARPS = 2;             // strips per CTA (one per warp)
 constexpr int GS_THREADS = 32 * GS_WARPS;
 constexpr int GS_ROWS_DEFAULT = 128;
 constexpr float kEps = 0.01f;           // wema.c:315
