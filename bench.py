@@ -408,6 +408,9 @@ def reference_mixed(a):
     return v, (total_s * 1e3 / max(steps_done, 1), steps_done), cb
 
 
+DEFAULT_GROUPS = 1                         # the library's pipeline groups per steady tick
+
+
 def mixed_config(world):
     from wema_b200 import synth as S
     pix = sum(spec.width * spec.height for spec, _ in S.mixed_streams(seed=7))
@@ -505,6 +508,25 @@ def bench_mixed(a, rank, world, local):
     barrier()
     frames_timed = a.steps * n + 2
     pix_timed = a.steps * sum(pix) + 2 * pix[0]
+
+    # ---- the same ticks with the streams in 1..4 pipelined groups (the
+    # library's default is the timed run above)
+    groups_ms = {}
+    for G in (1, 2, 3, 4):
+        b.set_groups(G)
+        for i in range(3):
+            tick(i)
+        b.sync()
+        barrier()
+        g0, g1 = ev(), ev()
+        g0.record(t_stream)
+        b.tick([ids[0]], [d_in[0][0]], [d_out[0]], wait_event=g0)
+        for i in range(a.steps):
+            tick(i)
+        b.tick([ids[0]], [d_in[0][1]], [d_out[0]], done_event=g1)
+        g1.synchronize()
+        groups_ms[str(G)] = round(g0.elapsed_time(g1) / a.steps, 4)
+    b.set_groups(DEFAULT_GROUPS)
 
     # ---- e2e through the host-frame tick (wema_cuda_batch_tick_host): every
     # tick's frames are copied in from pinned host memory and its outputs back,
@@ -624,6 +646,7 @@ def bench_mixed(a, rank, world, local):
                        "(one copy per direction), copies in after the previous tick",
                 "with_copies_in_beside_the_previous_tick": round(E * sum(pix) * world / (e2e_runs[True] * 1e-3) / 1e6, 2)},
         "gpu_launches": launches, "frames_timed": frames_timed,
+        "ms_per_step_by_pipeline_groups": groups_ms,
         "roofline": roofline, "pipeline": pipeline, "autotune": tune_report,
         "clocks": clocks,
     }

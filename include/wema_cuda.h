@@ -209,12 +209,17 @@ int wema_cuda_batch_tick_host(wema_cuda_batch *b, const int *ids, const void *co
  * receives the milliseconds summed over every timed tick, *ticks their
  * count.  Both wait for the batch. */
 /* A steady tick - every listed stream past its first frame, stage timing
- * off - replays CUDA graphs of its launches (forward transforms and
- * threshold; inverse transforms; luma transfer), captured per parameter
- * table and set of launches, with the same kernels, parameters and results
- * as the launches themselves; the waits between the three stay stream
- * operations.  enable = 0: launch the kernels one by one; default 1. */
+ * off - replays a CUDA graph of its launches, captured per parameter table
+ * and set of launches, with the same kernels, parameters and results as the
+ * launches themselves.  enable = 0: launch the kernels one by one, stage
+ * after stage; default 1. */
 int wema_cuda_batch_set_graphs(wema_cuda_batch *b, int enable);
+/* Pipeline groups of a steady tick's graph (1..4, default 1): the tick's
+ * streams are split into that many groups of about equal pixel count, and
+ * group g's threshold, inverse and transfer run beside group g+1's forward,
+ * threshold and inverse.  Results do not depend on it (on a B200 the
+ * 48-stream mix ran fastest with one group). */
+int wema_cuda_batch_set_groups(wema_cuda_batch *b, int groups);
 /* enable = 1: a host tick's copies in start as soon as their staging set is
  * free, beside the previous tick's kernels and copies out.  Default 0: they
  * also wait for the previous tick to finish (measured faster on B200 hosts:

@@ -274,24 +274,28 @@ def test_batch_tick_host_contiguous_frames(torch_cuda, overlap):
 
 
 def test_batch_graph_replay_equals_launches(oracle, torch_cuda):
-    """Steady ticks replayed as CUDA graphs give the frames of the same ticks
-    launched kernel by kernel, through changes of the tick's stream set (a
-    stream skipping ticks, one added, one removed: each change captures
-    again), and the oracle's."""
+    """Steady ticks replayed as CUDA graphs - with the streams in 1, 2 or 4
+    pipelined groups - give the frames of the same ticks launched kernel by
+    kernel, through changes of the tick's stream set (a stream skipping ticks,
+    one added, one removed: each change captures again), ticks issued back to
+    back (synchronised every third tick only), and the oracle's."""
     torch = torch_cuda
     F = 7
     sel = [STREAMS[0], STREAMS[2], STREAMS[3], STREAMS[4]]
     data = [frames(w, h, F, seed=k + 91, fps=cfg.get("fps", 30.0)) for k, (w, h, cfg) in enumerate(sel)]
     d_in = [torch.from_numpy(u).cuda() for u in data]
+    modes = [(False, 1), (True, 1), (True, 2), (True, 4)]
     outs = {}
-    for graphs in (False, True):
+    for graphs, groups in modes:
         b = wc.Batch(device=0, max_streams=8)
         b.set_graphs(graphs)
+        b.set_groups(groups)
         ids = [b.add(w, h, **cfg) for (w, h, cfg) in sel[:3]]
         got = [[None] * F for _ in sel]
         nxt = [0] * len(sel)
         for tick in range(F + 4):
             if tick == 3:
+                b.sync()
                 ids.append(b.add(sel[3][0], sel[3][1], **sel[3][2]))   # joins late
             live = [k for k in range(len(ids)) if nxt[k] < F and not (k == 1 and tick in (4, 5))]
             if tick == 8 and 0 in live:
@@ -300,17 +304,22 @@ def test_batch_graph_replay_equals_launches(oracle, torch_cuda):
                 continue
             o = [torch.empty((sel[k][1], sel[k][0], 3), dtype=torch.uint8, device="cuda") for k in live]
             b.tick([ids[k] for k in live], [d_in[k][nxt[k]] for k in live], o)
-            b.sync()
+            if tick % 3 == 2:
+                b.sync()
             for k, x in zip(live, o):
-                got[k][nxt[k]] = x.cpu().numpy()
+                got[k][nxt[k]] = x     # read after the last tick
                 nxt[k] += 1
-        outs[graphs] = got
+        b.sync()
+        outs[(graphs, groups)] = [[None if x is None else x.cpu().numpy() for x in row] for row in got]
         b.close()
+    base = outs[modes[0]]
     for k, (w, h, cfg) in enumerate(sel):
         want = oracle_u8(oracle, data[k], **cfg)
         for t in range(F):
-            if outs[False][k][t] is None:
-                assert outs[True][k][t] is None
-                continue
-            assert np.array_equal(outs[True][k][t], outs[False][k][t]), f"stream {k} frame {t}"
-            assert_close(outs[True][k][t], want[t], cfg.get("color", False), f"stream {k} frame {t}")
+            for m in modes[1:]:
+                if base[k][t] is None:
+                    assert outs[m][k][t] is None
+                    continue
+                assert np.array_equal(outs[m][k][t], base[k][t]), f"mode {m} stream {k} frame {t}"
+            if base[k][t] is not None:
+                assert_close(base[k][t], want[t], cfg.get("color", False), f"stream {k} frame {t}")

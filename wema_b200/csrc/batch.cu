@@ -97,6 +97,18 @@ WEMA_API int wema_cuda_batch_set_graphs(wema_cuda_batch* b, int enable) {
     return 0;
 }
 
+WEMA_API int wema_cuda_batch_set_groups(wema_cuda_batch* b, int groups) {
+    clear_error();
+    if (!b) { set_error("null argument"); return -1; }
+    if (groups < 1 || groups > wema::Batch::MAXG) {
+        set_error("groups %d outside 1..%d", groups, wema::Batch::MAXG);
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(b->mu);
+    b->b.groups = groups;
+    return 0;
+}
+
 WEMA_API int wema_cuda_batch_set_host_overlap(wema_cuda_batch* b, int enable) {
     clear_error();
     if (!b) { set_error("null argument"); return -1; }

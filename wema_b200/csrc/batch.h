@@ -16,11 +16,20 @@
 // arithmetic is the per-stream path's, so a stream's frames are bit-identical
 // alone and in any mix.
 //
-// Consecutive ticks overlap: the luma transfer of tick t runs on its own
-// lower-priority CUDA stream while tick t+1's forward DWT, threshold and IIR
-// run (their blocks are placed first, the transfer's fill what is left of
-// each SM); tick t+1's inverse DWT, which rewrites the reconstructed luma the
-// transfer reads, waits for it.  The tick's done event follows its transfer.
+// A steady tick (every stream past its first frame) replays one CUDA graph
+// of all its launches, captured per table and launch set.  The streams may be
+// split into groups of about equal pixel count that run as a pipeline (group
+// g's threshold beside group g+1's forward transform, its inverse beside group
+// g+1's threshold, its transfer beside group g+1's inverse; threshold and
+// inverse launches at the highest priority, the transfer at the lowest); one
+// group is the default - on the 48-stream mix one graph per tick measured
+// 2.56 ms, two to four groups 2.64-2.69 ms, and the earlier three graphs per
+// tick with the transfer beside the next tick's forward 2.65 ms.  Other ticks
+// (first frames, stage timing, graphs off) issue the stages in turn over all
+// groups on streams: the luma transfer of tick t on its own lower-priority
+// stream while tick t+1's forward, threshold and IIR run; tick t+1's inverse
+// DWT, which rewrites the reconstructed luma the transfer reads, waits for it.
+// The tick's done event follows its transfer.
 //
 // Supported per stream: IIR band-pass, luma (guided filter or Gaussian
 // transfer) or colour, RGB24 frames in device memory.
@@ -101,15 +110,18 @@ public:
         bool used = false;
         cudaEvent_t tev[T_COUNT][2] = {};  // stage start / end (timing on)
         bool timed = false;               // tev holds a tick not yet added to stage_ms
-        // steady ticks replay CUDA graphs of their launches, one set per table:
-        // forward + threshold, inverse, transfer (the waits between them stay
-        // stream operations, so the next tick's forward still overlaps this
-        // tick's transfer); `sig` identifies the launches they hold
-        cudaGraphExec_t g_fwd = nullptr, g_inv = nullptr, g_xfer = nullptr;
+        // steady ticks replay a CUDA graph of their launches, one per table;
+        // `sig` identifies the launches it holds
+        cudaGraphExec_t g_tick = nullptr;
         std::vector<long long> sig;
+        long long graph_launches = 0;   // kernels in one replay
     } tb[NBUF];
     bool use_graphs = true;
-    long long per_graph_launches = 0;  // kernels in one replay of a table's graphs
+    // pipelined groups of a steady tick; the streams and events that build its graph
+    static constexpr int MAXG = 4;
+    int groups = 1;
+    cudaStream_t cs_fwd = nullptr, cs_xfer = nullptr, cs_chain[MAXG] = {};
+    cudaEvent_t ce_fork = nullptr, ce_f[MAXG] = {}, ce_i[MAXG] = {}, ce_join[MAXG + 2] = {};
     bool timing = false;
     double stage_ms[T_COUNT] = {};
     long long ticks_timed = 0;
@@ -142,7 +154,7 @@ public:
     int cur = 0;
     long long launches = 0;
     long long ticks = 0;
-    Launch L[L_COUNT];
+    Launch L[MAXG][L_COUNT];
     std::vector<char> image;
 
     ~Batch() {
@@ -162,9 +174,17 @@ public:
                 for (cudaEvent_t e : p)
                     if (e) cudaEventDestroy(e);
         }
-        for (cudaStream_t st : {st_main, st_iir, st_xfer, st_h2d, st_d2h, st_alloc})
+        for (cudaStream_t st : {st_main, st_iir, st_xfer, st_h2d, st_d2h, st_alloc, cs_fwd, cs_xfer})
             if (st) cudaStreamDestroy(st);
-        for (cudaEvent_t e : {ev_fwd, ev_iir, ev_inv, ev_xfer})
+        for (cudaStream_t st : cs_chain)
+            if (st) cudaStreamDestroy(st);
+        for (cudaEvent_t e : {ev_fwd, ev_iir, ev_inv, ev_xfer, ce_fork})
+            if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : ce_f)
+            if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : ce_i)
+            if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : ce_join)
             if (e) cudaEventDestroy(e);
         for (HostSet& h : hs)
             for (cudaEvent_t e : {h.h2d, h.tick, h.d2h})
@@ -195,6 +215,23 @@ public:
         for (cudaStream_t* st : {&st_h2d, &st_d2h, &st_alloc})
             if (!cuda_ok(cudaStreamCreateWithFlags(st, cudaStreamNonBlocking), "cudaStreamCreate"))
                 return false;
+        // graph building: forward launches at the middle priority, threshold and
+        // inverse chains at the highest, the transfer at the lowest (the graph
+        // keeps each launch's priority)
+        if (!cuda_ok(cudaStreamCreateWithPriority(&cs_fwd, cudaStreamNonBlocking, mid), "cudaStreamCreate") ||
+            !cuda_ok(cudaStreamCreateWithPriority(&cs_xfer, cudaStreamNonBlocking, lo), "cudaStreamCreate"))
+            return false;
+        for (cudaStream_t& st : cs_chain)
+            if (!cuda_ok(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, hi), "cudaStreamCreate"))
+                return false;
+        for (cudaEvent_t* e : {&ce_fork})
+            if (!cuda_ok(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate")) return false;
+        for (int g = 0; g < MAXG; g++)
+            if (!cuda_ok(cudaEventCreateWithFlags(&ce_f[g], cudaEventDisableTiming), "cudaEventCreate") ||
+                !cuda_ok(cudaEventCreateWithFlags(&ce_i[g], cudaEventDisableTiming), "cudaEventCreate"))
+                return false;
+        for (cudaEvent_t& e : ce_join)
+            if (!cuda_ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate")) return false;
         for (HostSet& h : hs)
             for (cudaEvent_t* e : {&h.h2d, &h.tick, &h.d2h})
                 if (!cuda_ok(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate"))
@@ -371,11 +408,10 @@ public:
     }
 
     static void drop_graphs(Table& t) {
-        for (cudaGraphExec_t* g : {&t.g_fwd, &t.g_inv, &t.g_xfer})
-            if (*g) {
-                cudaGraphExecDestroy(*g);
-                *g = nullptr;
-            }
+        if (t.g_tick) {
+            cudaGraphExecDestroy(t.g_tick);
+            t.g_tick = nullptr;
+        }
         t.sig.clear();
     }
 
@@ -390,7 +426,8 @@ public:
             if (g) cudaGraphDestroy(g);
             return false;
         }
-        const bool inst = cuda_ok(cudaGraphInstantiate(out, g, 0), "graph instantiate");
+        const bool inst = cuda_ok(cudaGraphInstantiateWithFlags(out, g, cudaGraphInstantiateFlagUseNodePriority),
+                                  "graph instantiate");
         cudaGraphDestroy(g);
         return inst;
     }
@@ -432,19 +469,42 @@ public:
             for (int q = 0; q < k; q++)
                 if (ids[q] == ids[k]) { set_error("stream %d listed twice in one tick", ids[k]); return false; }
         }
-        L[L_FWD0_LUMA].reset(sizeof(FwdLevelParams));
-        L[L_FWD0_COLOR].reset(sizeof(FwdLevelParams));
-        for (int l = 1; l <= 3; l++) L[L_FWD0_COLOR + l].reset(sizeof(FwdLevelParams));
-        for (int k = L_THR_PART; k <= L_THR16; k++) L[k].reset(thr_args_bytes());
-        L[L_IIR_PRESEED].reset(iir_args_bytes());
-        L[L_IIR].reset(iir_args_bytes());
-        for (int k = L_INV3; k <= L_INV0_COLOR; k++) L[k].reset(sizeof(InvLevelParams));
-        L[L_XFER_GUIDED].reset(sizeof(TransferParams));
-        L[L_XFER_GAUSS].reset(sizeof(TransferParams));
+        for (auto& LG : L) {
+            LG[L_FWD0_LUMA].reset(sizeof(FwdLevelParams));
+            LG[L_FWD0_COLOR].reset(sizeof(FwdLevelParams));
+            for (int l = 1; l <= 3; l++) LG[L_FWD0_COLOR + l].reset(sizeof(FwdLevelParams));
+            for (int k = L_THR_PART; k <= L_THR16; k++) LG[k].reset(thr_args_bytes());
+            LG[L_IIR_PRESEED].reset(iir_args_bytes());
+            LG[L_IIR].reset(iir_args_bytes());
+            for (int k = L_INV3; k <= L_INV0_COLOR; k++) LG[k].reset(sizeof(InvLevelParams));
+            LG[L_XFER_GUIDED].reset(sizeof(TransferParams));
+            LG[L_XFER_GAUSS].reset(sizeof(TransferParams));
+        }
         std::vector<char> targs(thr_args_bytes()), iargs(iir_args_bytes());
+
+        // the pipeline's groups: streams largest first, each to the group with the
+        // fewest pixels so far
+        const int G = std::max(1, std::min(groups, n));
+        std::vector<int> grp(n, 0);
+        {
+            std::vector<int> order(n);
+            for (int k = 0; k < n; k++) order[k] = k;
+            std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+                return streams[ids[a]]->g.pixels > streams[ids[b]]->g.pixels;
+            });
+            long long load[MAXG] = {};
+            for (int k : order) {
+                int best = 0;
+                for (int g = 1; g < G; g++)
+                    if (load[g] < load[best]) best = g;
+                grp[k] = best;
+                load[best] += streams[ids[k]]->g.pixels;
+            }
+        }
 
         for (int k = 0; k < n; k++) {
             Session& S = *streams[ids[k]];
+            Launch* const LK = L[grp[k]];
             const Geom& g = S.g;
             const int LV = g.levels, nch = S.nch;
             Slot& q = S.slot[0];
@@ -472,10 +532,10 @@ public:
                 unsigned gx, gy;
                 if (l == 0) {
                     const unsigned b = dwt_fwd_grid(p, 1, gx, gy);
-                    L[nch == 3 ? L_FWD0_COLOR : L_FWD0_LUMA].add(&p, gx, gy, b);
+                    LK[nch == 3 ? L_FWD0_COLOR : L_FWD0_LUMA].add(&p, gx, gy, b);
                 } else {
                     const unsigned b = dwt_fwd_grid(p, nch, gx, gy);
-                    L[L_FWD0_COLOR + l].add(&p, gx, gy, b);
+                    LK[L_FWD0_COLOR + l].add(&p, gx, gy, b);
                 }
             }
             // ---- threshold
@@ -489,7 +549,7 @@ public:
             for (int st = 0; st < 5; st++) {
                 if ((st == 4) != (S.cfg.planes_fp16 != 0)) continue;   // FP16 planes: one kernel
                 if (st < 2 && S.thr_hist) continue;   // partial sums + prefix: first frame only
-                L[L_THR_PART + st].add(targs.data(), grids[st][0], grids[st][1],
+                LK[L_THR_PART + st].add(targs.data(), grids[st][0], grids[st][1],
                                        grids[st][0] * grids[st][1]);
             }
             // ---- IIR: a stream's first frame takes the preseed and the filter as
@@ -498,8 +558,8 @@ public:
             for (int c = 0; first && c < nch; c++) {
                 const unsigned b = iir_args_fill(iargs.data(), S.ip, q.coef[c], S.state[c], S.cfg.iir_state_fp64, q.delta[c],
                                                  S.warmup);
-                L[L_IIR_PRESEED].add(iargs.data(), b, 1, b);
-                L[L_IIR].add(iargs.data(), b, 1, b);
+                LK[L_IIR_PRESEED].add(iargs.data(), b, 1, b);
+                LK[L_IIR].add(iargs.data(), b, 1, b);
             }
             // ---- inverse DWT (+ colour output) and the luma transfer
             const float amp = fade_amp(S.cfg.amp_factor, first ? S.warmup : S.frames_processed, S.warmup);
@@ -526,10 +586,10 @@ public:
                 if (l == 0 && nch == 3) {
                     iq.out_u8 = out[k];
                     const unsigned b = dwt_inv_grid(iq, 1, gx, gy);
-                    L[L_INV0_COLOR].add(&iq, gx, gy, b);
+                    LK[L_INV0_COLOR].add(&iq, gx, gy, b);
                 } else {
                     const unsigned b = dwt_inv_grid(iq, nch, gx, gy);
-                    L[l == 0 ? L_INV0_LUMA : L_INV1 - (l - 1)].add(&iq, gx, gy, b);
+                    LK[l == 0 ? L_INV0_LUMA : L_INV1 - (l - 1)].add(&iq, gx, gy, b);
                 }
             }
             if (nch == 1) {
@@ -544,12 +604,13 @@ public:
                 tp.h16 = S.cfg.planes_fp16;
                 unsigned gx, gy;
                 const unsigned b = transfer_grid(tp, gx, gy);
-                L[tp.edge_aware ? L_XFER_GUIDED : L_XFER_GAUSS].add(&tp, gx, gy, b);
+                LK[tp.edge_aware ? L_XFER_GUIDED : L_XFER_GAUSS].add(&tp, gx, gy, b);
             }
         }
         // ---- the table image, its buffer, one H2D copy
         image.clear();
-        for (Launch& l : L) emit(l);
+        for (auto& LG : L)
+            for (Launch& l : LG) emit(l);
         Table& t = tb[cur];
         if (t.used && !cuda_ok(cudaEventSynchronize(t.done), "table reuse")) return false;
         if (!collect(t)) return false;
@@ -568,14 +629,14 @@ public:
         if (wait && !cuda_ok(cudaStreamWaitEvent(st_main, wait, 0), "stream wait")) return false;
         if (!cuda_ok(cudaMemcpyAsync(t.dev, t.host, image.size(), cudaMemcpyHostToDevice, st_main), "table copy"))
             return false;
-        auto P = [&](int k) { return (const void*)(t.dev + L[k].params_off); };
-        auto M = [&](int k) { return (const int*)(t.dev + L[k].map_off); };
+        auto P = [&](int g, int k) { return (const void*)(t.dev + L[g][k].params_off); };
+        auto M = [&](int g, int k) { return (const int*)(t.dev + L[g][k].map_off); };
         auto ok = [&](cudaError_t e, const char* what) {
             launches += 1;
             return cuda_ok(e, what);
         };
-        auto go = [&](int k, auto fn, const char* what) {
-            if (L[k].n() == 0) return true;
+        auto go = [&](int g, int k, auto fn, const char* what) {
+            if (L[g][k].n() == 0) return true;
             return ok(fn(), what);
         };
         auto mark = [&](int stage, int end, cudaStream_t st) {
@@ -586,102 +647,127 @@ public:
                 for (cudaEvent_t& e : p)
                     if (!cuda_ok(cudaEventCreate(&e), "cudaEventCreate")) return false;
 
-        // the launches in three groups; a steady tick (every stream past its
-        // first frame: no preseed, filter or threshold prefix launches, timing
-        // off) replays them as CUDA graphs captured for this table and set of
-        // launches
-        auto fwd = [&] {
-            if (!mark(T_FWD0, 0, st_main)) return false;
-            if (!go(L_FWD0_LUMA, [&] { return launch_dwt_fwd_multi(kSrcRgbU8, 1, (const FwdLevelParams*)P(L_FWD0_LUMA), M(L_FWD0_LUMA), L[L_FWD0_LUMA].total, st_main); }, "forward DWT"))
-                return false;
-            if (!go(L_FWD0_COLOR, [&] { return launch_dwt_fwd_multi(kSrcRgbU8, 3, (const FwdLevelParams*)P(L_FWD0_COLOR), M(L_FWD0_COLOR), L[L_FWD0_COLOR].total, st_main); }, "forward DWT"))
-                return false;
-            if (!mark(T_FWD0, 1, st_main) || !mark(T_FWD, 0, st_main)) return false;
+        // the stages of one group on one stream
+        auto fwd0 = [&](int g, cudaStream_t st) {
+            return go(g, L_FWD0_LUMA, [&] { return launch_dwt_fwd_multi(kSrcRgbU8, 1, (const FwdLevelParams*)P(g, L_FWD0_LUMA), M(g, L_FWD0_LUMA), L[g][L_FWD0_LUMA].total, st); }, "forward DWT") &&
+                   go(g, L_FWD0_COLOR, [&] { return launch_dwt_fwd_multi(kSrcRgbU8, 3, (const FwdLevelParams*)P(g, L_FWD0_COLOR), M(g, L_FWD0_COLOR), L[g][L_FWD0_COLOR].total, st); }, "forward DWT");
+        };
+        auto fwdl = [&](int g, cudaStream_t st) {
             for (int k = L_FWD1; k <= L_FWD3; k++)
-                if (!go(k, [&] { return launch_dwt_fwd_multi(kSrcPlanes, 1, (const FwdLevelParams*)P(k), M(k), L[k].total, st_main); }, "forward DWT"))
+                if (!go(g, k, [&] { return launch_dwt_fwd_multi(kSrcPlanes, 1, (const FwdLevelParams*)P(g, k), M(g, k), L[g][k].total, st); }, "forward DWT"))
                     return false;
-            return mark(T_FWD, 1, st_main);
+            return true;
         };
-        auto thr = [&] {
-            if (!mark(T_THR, 0, st_main)) return false;
+        auto thr = [&](int g, cudaStream_t st) {
             for (int k = L_THR_PART; k <= L_THR16; k++)
-                if (!go(k, [&] { return launch_threshold_multi(k - L_THR_PART, P(k), M(k), L[k].total, st_main); }, "threshold"))
+                if (!go(g, k, [&] { return launch_threshold_multi(k - L_THR_PART, P(g, k), M(g, k), L[g][k].total, st); }, "threshold"))
                     return false;
-            return mark(T_THR, 1, st_main);
+            return true;
         };
-        auto fwd_thr = [&] { return fwd() && thr(); };
-        auto inverse = [&] {
-            if (!mark(T_INV, 0, st_main)) return false;
+        auto iir = [&](int g, cudaStream_t st) {
+            return go(g, L_IIR_PRESEED, [&] { return launch_iir_multi(P(g, L_IIR_PRESEED), M(g, L_IIR_PRESEED), L[g][L_IIR_PRESEED].total, 1, st); }, "IIR preseed") &&
+                   go(g, L_IIR, [&] { return launch_iir_multi(P(g, L_IIR), M(g, L_IIR), L[g][L_IIR].total, 0, st); }, "IIR");
+        };
+        auto invl = [&](int g, cudaStream_t st) {
             for (int k = L_INV3; k <= L_INV1; k++)
-                if (!go(k, [&] { return launch_dwt_inv_multi(1, kOutPlanes, (const InvLevelParams*)P(k), M(k), L[k].total, st_main); }, "inverse DWT"))
+                if (!go(g, k, [&] { return launch_dwt_inv_multi(1, kOutPlanes, (const InvLevelParams*)P(g, k), M(g, k), L[g][k].total, st); }, "inverse DWT"))
                     return false;
-            if (!mark(T_INV, 1, st_main) || !mark(T_INV0, 0, st_main)) return false;
-            if (!go(L_INV0_LUMA, [&] { return launch_dwt_inv_multi(1, kOutPlanes, (const InvLevelParams*)P(L_INV0_LUMA), M(L_INV0_LUMA), L[L_INV0_LUMA].total, st_main); }, "inverse DWT"))
-                return false;
-            if (!go(L_INV0_COLOR, [&] { return launch_dwt_inv_multi(3, kOutRgb, (const InvLevelParams*)P(L_INV0_COLOR), M(L_INV0_COLOR), L[L_INV0_COLOR].total, st_main); }, "inverse DWT"))
-                return false;
-            return mark(T_INV0, 1, st_main);
+            return true;
         };
-        auto transfer = [&] {
-            if (!mark(T_XFER, 0, st_xfer)) return false;
-            if (!go(L_XFER_GUIDED, [&] { return launch_transfer_multi(1, (const TransferParams*)P(L_XFER_GUIDED), M(L_XFER_GUIDED), L[L_XFER_GUIDED].total, st_xfer); }, "luma transfer"))
-                return false;
-            if (!go(L_XFER_GAUSS, [&] { return launch_transfer_multi(0, (const TransferParams*)P(L_XFER_GAUSS), M(L_XFER_GAUSS), L[L_XFER_GAUSS].total, st_xfer); }, "luma transfer"))
-                return false;
-            return mark(T_XFER, 1, st_xfer);
+        auto inv0 = [&](int g, cudaStream_t st) {
+            return go(g, L_INV0_LUMA, [&] { return launch_dwt_inv_multi(1, kOutPlanes, (const InvLevelParams*)P(g, L_INV0_LUMA), M(g, L_INV0_LUMA), L[g][L_INV0_LUMA].total, st); }, "inverse DWT") &&
+                   go(g, L_INV0_COLOR, [&] { return launch_dwt_inv_multi(3, kOutRgb, (const InvLevelParams*)P(g, L_INV0_COLOR), M(g, L_INV0_COLOR), L[g][L_INV0_COLOR].total, st); }, "inverse DWT");
         };
-        const bool steady = use_graphs && !timing && L[L_IIR].n() == 0 && L[L_IIR_PRESEED].n() == 0 &&
-                            L[L_THR_PART].n() == 0 && L[L_THR_PREFIX].n() == 0;
-        if (steady) {
-            // what the graphs hold: the table, every launch's blocks and offsets,
-            // the device's kernel variants
-            std::vector<long long> sig = {(long long)(uintptr_t)t.dev, dwt_variant(device, 0), dwt_variant(device, 1)};
-            for (const Launch& l : L) {
-                sig.push_back(l.total);
-                sig.push_back((long long)l.params_off);
-                sig.push_back((long long)l.map_off);
+        auto xfer = [&](int g, cudaStream_t st) {
+            return go(g, L_XFER_GUIDED, [&] { return launch_transfer_multi(1, (const TransferParams*)P(g, L_XFER_GUIDED), M(g, L_XFER_GUIDED), L[g][L_XFER_GUIDED].total, st); }, "luma transfer") &&
+                   go(g, L_XFER_GAUSS, [&] { return launch_transfer_multi(0, (const TransferParams*)P(g, L_XFER_GAUSS), M(g, L_XFER_GAUSS), L[g][L_XFER_GAUSS].total, st); }, "luma transfer");
+        };
+        // a stage over every group in turn, between its timing marks
+        auto all = [&](auto stage, int tstage, cudaStream_t st) {
+            if (!mark(tstage, 0, st)) return false;
+            for (int g = 0; g < G; g++)
+                if (!stage(g, st)) return false;
+            return mark(tstage, 1, st);
+        };
+        // The steady tick's pipeline, issued on st_main while it is captured:
+        // forward transforms group after group on cs_fwd; per group a chain
+        // (threshold, then inverse after the previous group's) on cs_chain[g];
+        // transfers group after group on cs_xfer; all joined back to st_main.
+        auto pipeline = [&] {
+            if (!cuda_ok(cudaEventRecord(ce_fork, st_main), "event record") ||
+                !cuda_ok(cudaStreamWaitEvent(cs_fwd, ce_fork, 0), "stream wait"))
+                return false;
+            for (int g = 0; g < G; g++)
+                if (!fwd0(g, cs_fwd) || !fwdl(g, cs_fwd) || !cuda_ok(cudaEventRecord(ce_f[g], cs_fwd), "event record"))
+                    return false;
+            for (int g = 0; g < G; g++) {
+                cudaStream_t cs = cs_chain[g];
+                if (!cuda_ok(cudaStreamWaitEvent(cs, ce_f[g], 0), "stream wait") || !thr(g, cs)) return false;
+                if (g > 0 && !cuda_ok(cudaStreamWaitEvent(cs, ce_i[g - 1], 0), "stream wait")) return false;
+                if (!invl(g, cs) || !inv0(g, cs) || !cuda_ok(cudaEventRecord(ce_i[g], cs), "event record"))
+                    return false;
             }
+            for (int g = 0; g < G; g++)
+                if (!cuda_ok(cudaStreamWaitEvent(cs_xfer, ce_i[g], 0), "stream wait") || !xfer(g, cs_xfer))
+                    return false;
+            int nj = 0;
+            auto join = [&](cudaStream_t st) {
+                return cuda_ok(cudaEventRecord(ce_join[nj], st), "event record") &&
+                       cuda_ok(cudaStreamWaitEvent(st_main, ce_join[nj++], 0), "stream wait");
+            };
+            if (!join(cs_fwd) || !join(cs_xfer)) return false;
+            for (int g = 0; g < G; g++)
+                if (!join(cs_chain[g])) return false;
+            return true;
+        };
+
+        bool first_frames = false;
+        for (int g = 0; g < G; g++)
+            first_frames |= L[g][L_IIR].n() || L[g][L_IIR_PRESEED].n() || L[g][L_THR_PART].n() || L[g][L_THR_PREFIX].n();
+        const bool steady = use_graphs && !timing && !first_frames;
+        if (steady) {
+            // what the graph holds: the table, every launch's blocks and offsets,
+            // the device's kernel variants
+            std::vector<long long> sig = {(long long)(uintptr_t)t.dev, dwt_variant(device, 0), dwt_variant(device, 1), G};
+            for (int g = 0; g < G; g++)
+                for (const Launch& l : L[g]) {
+                    sig.push_back(l.total);
+                    sig.push_back((long long)l.params_off);
+                    sig.push_back((long long)l.map_off);
+                }
             if (sig != t.sig) {
                 drop_graphs(t);
                 const long long before = launches;
-                if (!capture(st_main, &t.g_fwd, fwd_thr) || !capture(st_main, &t.g_inv, inverse) ||
-                    !capture(st_xfer, &t.g_xfer, transfer)) {
+                if (!capture(st_main, &t.g_tick, pipeline)) {
                     drop_graphs(t);
                     return false;
                 }
-                per_graph_launches = launches - before;
+                t.graph_launches = launches - before;
                 launches = before;
                 t.sig = sig;
             }
-            launches += per_graph_launches;
-            if (!cuda_ok(cudaGraphLaunch(t.g_fwd, st_main), "graph launch")) return false;
-            // the previous tick's transfer still reads its reconstructed luma
+            launches += t.graph_launches;
+            // a transfer outside the graphs (an earlier tick's) still reads its reconstructed luma
             if (xfer_pending && !cuda_ok(cudaStreamWaitEvent(st_main, ev_xfer, 0), "stream wait")) return false;
-            if (!cuda_ok(cudaGraphLaunch(t.g_inv, st_main), "graph launch")) return false;
+            if (!cuda_ok(cudaGraphLaunch(t.g_tick, st_main), "graph launch")) return false;
             if (!cuda_ok(cudaEventRecord(ev_inv, st_main), "event record")) return false;
             if (!cuda_ok(cudaStreamWaitEvent(st_xfer, ev_inv, 0), "stream wait")) return false;
-            if (!cuda_ok(cudaGraphLaunch(t.g_xfer, st_xfer), "graph launch")) return false;
         } else {
             // forward, then the filter (first frames) beside the threshold
-            if (!fwd()) return false;
+            if (!all(fwd0, T_FWD0, st_main) || !all(fwdl, T_FWD, st_main)) return false;
             if (!cuda_ok(cudaEventRecord(ev_fwd, st_main), "event record")) return false;
-            if (!thr()) return false;
+            if (!all(thr, T_THR, st_main)) return false;
             if (!cuda_ok(cudaStreamWaitEvent(st_iir, ev_fwd, 0), "stream wait")) return false;
-            if (!mark(T_IIR, 0, st_iir)) return false;
-            if (!go(L_IIR_PRESEED, [&] { return launch_iir_multi(P(L_IIR_PRESEED), M(L_IIR_PRESEED), L[L_IIR_PRESEED].total, 1, st_iir); }, "IIR preseed"))
-                return false;
-            if (!go(L_IIR, [&] { return launch_iir_multi(P(L_IIR), M(L_IIR), L[L_IIR].total, 0, st_iir); }, "IIR"))
-                return false;
-            if (!mark(T_IIR, 1, st_iir)) return false;
+            if (!all(iir, T_IIR, st_iir)) return false;
             if (!cuda_ok(cudaEventRecord(ev_iir, st_iir), "event record")) return false;
             if (!cuda_ok(cudaStreamWaitEvent(st_main, ev_iir, 0), "stream wait")) return false;
             // the previous tick's transfer still reads its reconstructed luma
             if (xfer_pending && !cuda_ok(cudaStreamWaitEvent(st_main, ev_xfer, 0), "stream wait")) return false;
-            if (!inverse()) return false;
+            if (!all(invl, T_INV, st_main) || !all(inv0, T_INV0, st_main)) return false;
             // the transfer on its own stream, so the next tick's forward half overlaps it
             if (!cuda_ok(cudaEventRecord(ev_inv, st_main), "event record")) return false;
             if (!cuda_ok(cudaStreamWaitEvent(st_xfer, ev_inv, 0), "stream wait")) return false;
-            if (!transfer()) return false;
+            if (!all(xfer, T_XFER, st_xfer)) return false;
         }
         if (!cuda_ok(cudaEventRecord(ev_xfer, st_xfer), "event record")) return false;
         xfer_pending = true;

@@ -51,11 +51,13 @@ __device__ __forceinline__ int prow(int y) { return (y & 1) * 32 + (y >> 1); }
 __device__ __forceinline__ int pcol(int x) { return (x & 1) * ODD_COL + (x >> 1); }
 
 // Forward lifting of one line: lane holds samples s = g0 + 2*lane (even) and
-// s + 1 of a line of n samples.
+// s + 1 of a line of n samples.  EDGE false: every lane's neighbours lie in
+// the line (1 <= g0 and g0 + 64 < n), so the border mirror's selects go.
+template <bool EDGE>
 __device__ __forceinline__ void lift_fwd(float& e, float& o, int s, int n) {
-    const bool r_ok = s + 2 < n;     // predict: right even neighbour s+2
-    const bool l_ok = s >= 1;        // update: left odd neighbour s-1
-    const bool ro_ok = s + 1 < n;    // update: right odd neighbour s+1
+    const bool r_ok = !EDGE || s + 2 < n;     // predict: right even neighbour s+2
+    const bool l_ok = !EDGE || s >= 1;        // update: left odd neighbour s-1
+    const bool ro_ok = !EDGE || s + 1 < n;    // update: right odd neighbour s+1
     float t;
 #define WEMA_PREDICT(C)                                    \
     t = __shfl_down_sync(FULL, e, 1);                       \
@@ -73,10 +75,11 @@ __device__ __forceinline__ void lift_fwd(float& e, float& o, int s, int n) {
 
 // Inverse lifting of one line (dwt.c:109-170): unscale, then the steps in
 // reverse order with negated constants.
+template <bool EDGE>
 __device__ __forceinline__ void lift_inv(float& e, float& o, int s, int n) {
-    const bool r_ok = s + 2 < n;
-    const bool l_ok = s >= 1;
-    const bool ro_ok = s + 1 < n;
+    const bool r_ok = !EDGE || s + 2 < n;
+    const bool l_ok = !EDGE || s >= 1;
+    const bool ro_ok = !EDGE || s + 1 < n;
     float t;
     e = __fmul_rn(e, kK);
     o = __fmul_rn(o, kKInv);
@@ -93,20 +96,30 @@ __device__ __forceinline__ void lift_inv(float& e, float& o, int s, int n) {
 // interleaves them.  b[u] is line u's base (a valid line even when
 // act[u] is false - then nothing is stored); ei / oi address this lane's even
 // and odd sample, s is its even sample's global index, n the line length, lim
-// the staged length.
+// the staged length.  s0 is lane 0's s: a segment away from both ends of
+// the line (s0 >= 1, s0 + 64 < n) lifts without the border selects.
 template <bool FWD, int LPW>
 __device__ __forceinline__ void liftN(float* const (&b)[LPW], const bool (&act)[LPW], int ei, int oi,
-                                      int s, int n, int lim, int lane) {
+                                      int s0, int n, int lim, int lane) {
+    const int s = s0 + 2 * lane;
     float e[LPW], o[LPW];
 #pragma unroll
     for (int u = 0; u < LPW; u++) {
         e[u] = b[u][ei];
         o[u] = b[u][oi];
     }
+    if (s0 >= 1 && s0 + SEG < n) {
 #pragma unroll
-    for (int u = 0; u < LPW; u++) {
-        if (FWD) lift_fwd(e[u], o[u], s, n);
-        else lift_inv(e[u], o[u], s, n);
+        for (int u = 0; u < LPW; u++) {
+            if (FWD) lift_fwd<false>(e[u], o[u], s, n);
+            else lift_inv<false>(e[u], o[u], s, n);
+        }
+    } else {
+#pragma unroll
+        for (int u = 0; u < LPW; u++) {
+            if (FWD) lift_fwd<true>(e[u], o[u], s, n);
+            else lift_inv<true>(e[u], o[u], s, n);
+        }
     }
 #pragma unroll
     for (int u = 0; u < LPW; u++) {
@@ -180,7 +193,6 @@ template <int C, int MODE, int LPW>
 __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, int by, int bz) {
     extern __shared__ __align__(16) float dyn[];
     float* planes = dyn;                                   // [C][PLANE]
-    float* lut = dyn + C * PLANE;                          // [256]
     const int ch0 = (C == 1 && MODE == kSrcPlanes) ? bz : 0;
     const int iw = p.iw, ih = p.ih, sw = p.sw, sh = p.sh;
     const int px0 = bx * TP, py0 = by * TP;
@@ -193,10 +205,6 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
     if (C == 1 && p.iir_state[ch0]) prefetch_state_rows(p, ch0, px0, py0);
 
     // ---- staging: one warp per region row
-    if (MODE == kSrcRgbU8) {
-        for (int i = threadIdx.x; i < 256; i += DWT_THREADS) lut[i] = __fdiv_rn((float)i, 255.0f);
-        __syncthreads();
-    }
     // every load of the warp's rows is issued before any is used
     constexpr int RPW = SEG / NWARP;   // region rows per warp
     if (MODE == kSrcPlanes) {
@@ -255,9 +263,9 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
                         hi = w + 1 < 32 ? h0 : h1;
                     }
                     const uint32_t x = __funnelshift_r(lo, hi, 8 * (b & 3));
-                    rgb[r][h][0] = lut[x & 0xFFu];
-                    rgb[r][h][1] = lut[(x >> 8) & 0xFFu];
-                    rgb[r][h][2] = lut[(x >> 16) & 0xFFu];
+                    rgb[r][h][0] = byte_of(x, 0);      // fl(byte / 255)
+                    rgb[r][h][1] = byte_of(x, 1);
+                    rgb[r][h][2] = byte_of(x, 2);
                 }
             }
         } else {
@@ -323,7 +331,7 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
                     act[u] = ly < RH;
                     b[u] = planes + cc * PLANE + prow(min(ly, RH - 1)) * RS;
                 }
-                liftN<true, LPW>(b, act, lane, ODD_COL + lane, rx0 + 2 * lane, iw, RW, lane);
+                liftN<true, LPW>(b, act, lane, ODD_COL + lane, rx0, iw, RW, lane);
             }
         __syncthreads();
     }
@@ -340,7 +348,7 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
                     act[u] = lx < cx1;
                     b[u] = planes + cc * PLANE + pcol(min(lx, cx1 - 1));
                 }
-                liftN<true, LPW>(b, act, lane * RS, (32 + lane) * RS, ry0 + 2 * lane, ih, RH, lane);
+                liftN<true, LPW>(b, act, lane * RS, (32 + lane) * RS, ry0, ih, RH, lane);
             }
         __syncthreads();
     }
@@ -452,7 +460,7 @@ __device__ __forceinline__ void dwt_inv_body(const InvLevelParams& p, int bx, in
                     act[u] = lx < RW;
                     b[u] = planes + cc * PLANE + pcol(min(lx, RW - 1));
                 }
-                liftN<false, LPW>(b, act, lane * RS, (32 + lane) * RS, ry0 + 2 * lane, oh, RH, lane);
+                liftN<false, LPW>(b, act, lane * RS, (32 + lane) * RS, ry0, oh, RH, lane);
             }
         __syncthreads();
     }
@@ -470,7 +478,7 @@ __device__ __forceinline__ void dwt_inv_body(const InvLevelParams& p, int bx, in
                     act[u] = ly < ty1;
                     b[u] = planes + cc * PLANE + prow(min(ly, ty1 - 1)) * RS;
                 }
-                liftN<false, LPW>(b, act, lane, ODD_COL + lane, rx0 + 2 * lane, ow, RW, lane);
+                liftN<false, LPW>(b, act, lane, ODD_COL + lane, rx0, ow, RW, lane);
             }
         __syncthreads();
     }
@@ -572,7 +580,7 @@ void dwt_variant_shape(int v, int* minb, int* lpw) {
 
 // ----------------------------------------------------------------- launch
 
-static size_t fwd_smem(int C) { return (size_t)C * PLANE * sizeof(float) + 256 * sizeof(float); }
+static size_t fwd_smem(int C) { return (size_t)C * PLANE * sizeof(float); }
 static size_t inv_smem(int C) { return (size_t)C * PLANE * sizeof(float); }
 size_t dwt_smem_bytes(int C) { return fwd_smem(C); }
 

@@ -110,6 +110,7 @@ def lib() -> C.CDLL:
         L.wema_cuda_batch_set_timing.argtypes = [vp, i]
         L.wema_cuda_batch_set_host_overlap.argtypes = [vp, i]
         L.wema_cuda_batch_set_graphs.argtypes = [vp, i]
+        L.wema_cuda_batch_set_groups.argtypes = [vp, i]
         L.wema_cuda_batch_stage_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
         L.wema_cuda_batch_stats.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                                             C.POINTER(i)]
@@ -349,6 +350,9 @@ class Batch:
 
     def set_graphs(self, enable: bool):
         _check(lib().wema_cuda_batch_set_graphs(self.h, int(bool(enable))), "set_graphs")
+
+    def set_groups(self, groups: int):
+        _check(lib().wema_cuda_batch_set_groups(self.h, int(groups)), "set_groups")
 
     def set_host_overlap(self, enable: bool):
         _check(lib().wema_cuda_batch_set_host_overlap(self.h, int(bool(enable))), "set_host_overlap")
