@@ -5,6 +5,23 @@
 
 #include "batch.h"
 
+namespace wema {
+
+__global__ void k_table_copy(uint4* __restrict__ dst, const uint4* __restrict__ src, size_t n16) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n16; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+cudaError_t launch_table_copy(void* dst, const void* host_mapped, size_t bytes, cudaStream_t st) {
+    const size_t n16 = (bytes + 15) / 16;
+    if (n16 == 0) return cudaSuccess;
+    const unsigned blocks = (unsigned)std::min<size_t>((n16 + 255) / 256, 148);
+    k_table_copy<<<blocks, 256, 0, st>>>(static_cast<uint4*>(dst), static_cast<const uint4*>(host_mapped), n16);
+    return cudaGetLastError();
+}
+
+}  // namespace wema
+
 // ===================================================================== C ABI
 using namespace wema;
 

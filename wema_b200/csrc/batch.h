@@ -104,6 +104,7 @@ public:
     static constexpr int NBUF = 3;
     struct Table {
         char* host = nullptr;
+        char* host_dev = nullptr;         // host's device-mapped address
         char* dev = nullptr;
         size_t cap = 0;
         cudaEvent_t done = nullptr;
@@ -143,14 +144,13 @@ public:
     } hs[3];
     cudaStream_t st_h2d = nullptr, st_d2h = nullptr;
     int hcur = 0;
-    // on: copies in wait only for their staging set's previous tick (three
-    // ticks back), so they overlap the previous tick's kernels and copies
-    // out.  Off (the default): they also wait for the previous tick to
-    // finish, and run beside the previous tick's copies out while the GPU is
-    // otherwise idle - measured faster on B200 hosts (9.8 vs 9.2 Gpix-frames/s
-    // on the 48-stream mix): copies beside the tick's kernels ran well below
-    // the host link's rate
-    bool host_overlap = false;
+    // on (the default): copies in wait only for their staging set's previous
+    // tick (three ticks back), so they overlap the previous tick's kernels and
+    // copies out - 12.7 Gpix-frames/s on the 48-stream mix on a B200 host,
+    // against 9.7 with them after the previous tick (off).  This needs the
+    // tick's parameter table to go in by a kernel: a table copy queued on
+    // the copy engine behind the next tick's frames held each tick back
+    bool host_overlap = true;
     int cur = 0;
     long long launches = 0;
     long long ticks = 0;
@@ -621,14 +621,17 @@ public:
             t.dev = nullptr;
             t.cap = 0;
             const size_t cap = std::max<size_t>(image.size() * 2, 1 << 16);
-            if (!cuda_ok(cudaMallocHost(&t.host, cap), "cudaMallocHost(table)")) return false;
+            if (!cuda_ok(cudaHostAlloc(&t.host, cap, cudaHostAllocMapped), "cudaHostAlloc(table)")) return false;
+            if (!cuda_ok(cudaHostGetDevicePointer((void**)&t.host_dev, t.host, 0), "table mapping")) return false;
             if (!cuda_ok(cudaMalloc(&t.dev, cap), "cudaMalloc(table)")) return false;
             t.cap = cap;
         }
         memcpy(t.host, image.data(), image.size());
         if (wait && !cuda_ok(cudaStreamWaitEvent(st_main, wait, 0), "stream wait")) return false;
-        if (!cuda_ok(cudaMemcpyAsync(t.dev, t.host, image.size(), cudaMemcpyHostToDevice, st_main), "table copy"))
-            return false;
+        // the table by a kernel, not a copy engine: with host ticks the H2D engine
+        // may be busy with the next tick's frames
+        launches += 1;
+        if (!cuda_ok(launch_table_copy(t.dev, t.host_dev, image.size(), st_main), "table copy")) return false;
         auto P = [&](int g, int k) { return (const void*)(t.dev + L[g][k].params_off); };
         auto M = [&](int g, int k) { return (const int*)(t.dev + L[g][k].map_off); };
         auto ok = [&](cudaError_t e, const char* what) {

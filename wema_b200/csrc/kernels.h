@@ -183,5 +183,9 @@ bool guided_set_rows(int dev, int rows);
 cudaError_t guided_autotune(int dev, const int* cand, int nc, float* ms, int* chosen);
 cudaError_t launch_transfer_multi(int edge_aware, const TransferParams* d_params, const int* d_map,
                                   unsigned blocks, cudaStream_t st);
+// a tick's parameter table from pinned host memory (its device-mapped
+// address) into device memory, read by a kernel over the host link: no copy
+// engine, so it never queues behind a frame copy; bytes rounded up to 16
+cudaError_t launch_table_copy(void* dst, const void* host_mapped, size_t bytes, cudaStream_t st);
 
 }  // namespace wema
