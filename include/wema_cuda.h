@@ -304,13 +304,14 @@ int wema_cuda_server_stats(wema_cuda_server *srv, int reset, wema_cuda_serve_sta
  *     thread (a 2^23-position trial plane) and keeps the fastest (4, the
  *     default, unless another is more than 3% faster);
  *   - the batched guided filter's sweep at 64, 128 and 256 output rows per
- *     segment (a 3840x8640 trial frame) and keeps the fastest (128 until then);
+ *     segment (a 3840x8640 trial frame) and keeps the fastest (64 until then);
  *   - the batched luma DWT level-0 kernels, forward and inverse, in nine
  *     variants each: CTAs per SM asked of the register allocator {1 (the
  *     compiler's choice), 3, 4} x lines lifted per warp at a time {2, 4, 8}
- *     (variant = 3 * index + index; a 3840x4320 trial frame) and keeps the
- *     fastest of each (forward 3x4, inverse 1x4 until then);
- * allocating ~550 MB for the trials (one at a time) and freeing it.  Every
+ *     (variant = 3 * index + index; a 3840x4320 trial frame, the forward
+ *     with the temporal filter's step inside as steady batched ticks run it)
+ *     and keeps the fastest of each (forward 4x4, inverse 4x8 until then);
+ * allocating ~950 MB for the trials (one at a time) and freeing it.  Every
  * later launch on the device uses the choices.  Returns the positions per
  * thread (or -1) and writes the timings to `report` (may be NULL; 1 KiB is
  * enough).  Results do not depend on any choice - each position's and each

@@ -78,6 +78,7 @@ struct Launch {
 enum {
     L_FWD0_LUMA, L_FWD0_COLOR, L_FWD1, L_FWD2, L_FWD3,
     L_THR_PART, L_THR_PREFIX, L_THR_MON, L_THR_WALK, L_THR16,
+    L_THR_MON0,                         // monoids of the level-0 sub-chunks, split off
     L_IIR_PRESEED, L_IIR,
     L_INV3, L_INV2, L_INV1, L_INV0_LUMA, L_INV0_COLOR,
     L_XFER_GUIDED, L_XFER_GAUSS,
@@ -100,7 +101,7 @@ public:
     // captured into a graph on st_main from another thread must not see it
     cudaStream_t st_alloc = nullptr;
     cudaEvent_t ev_fwd = nullptr, ev_iir = nullptr, ev_inv = nullptr, ev_xfer = nullptr;
-    bool xfer_pending = false;            // ev_xfer marks a transfer tick t+1 must wait for
+    bool xfer_pending = false;            // ev_xfer marks a transfer on st_xfer tick t+1 must wait for
     static constexpr int NBUF = 3;
     struct Table {
         char* host = nullptr;
@@ -122,7 +123,7 @@ public:
     static constexpr int MAXG = 4;
     int groups = 1;
     cudaStream_t cs_fwd = nullptr, cs_xfer = nullptr, cs_chain[MAXG] = {};
-    cudaEvent_t ce_fork = nullptr, ce_f[MAXG] = {}, ce_i[MAXG] = {}, ce_join[MAXG + 2] = {};
+    cudaEvent_t ce_fork = nullptr, ce_f0[MAXG] = {}, ce_f[MAXG] = {}, ce_i[MAXG] = {}, ce_join[MAXG + 2] = {};
     bool timing = false;
     double stage_ms[T_COUNT] = {};
     long long ticks_timed = 0;
@@ -182,6 +183,8 @@ public:
             if (e) cudaEventDestroy(e);
         for (cudaEvent_t e : ce_f)
             if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : ce_f0)
+            if (e) cudaEventDestroy(e);
         for (cudaEvent_t e : ce_i)
             if (e) cudaEventDestroy(e);
         for (cudaEvent_t e : ce_join)
@@ -228,6 +231,7 @@ public:
             if (!cuda_ok(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate")) return false;
         for (int g = 0; g < MAXG; g++)
             if (!cuda_ok(cudaEventCreateWithFlags(&ce_f[g], cudaEventDisableTiming), "cudaEventCreate") ||
+                !cuda_ok(cudaEventCreateWithFlags(&ce_f0[g], cudaEventDisableTiming), "cudaEventCreate") ||
                 !cuda_ok(cudaEventCreateWithFlags(&ce_i[g], cudaEventDisableTiming), "cudaEventCreate"))
                 return false;
         for (cudaEvent_t& e : ce_join)
@@ -473,7 +477,7 @@ public:
             LG[L_FWD0_LUMA].reset(sizeof(FwdLevelParams));
             LG[L_FWD0_COLOR].reset(sizeof(FwdLevelParams));
             for (int l = 1; l <= 3; l++) LG[L_FWD0_COLOR + l].reset(sizeof(FwdLevelParams));
-            for (int k = L_THR_PART; k <= L_THR16; k++) LG[k].reset(thr_args_bytes());
+            for (int k = L_THR_PART; k <= L_THR_MON0; k++) LG[k].reset(thr_args_bytes());
             LG[L_IIR_PRESEED].reset(iir_args_bytes());
             LG[L_IIR].reset(iir_args_bytes());
             for (int k = L_INV3; k <= L_INV0_COLOR; k++) LG[k].reset(sizeof(InvLevelParams));
@@ -482,16 +486,18 @@ public:
         }
         std::vector<char> targs(thr_args_bytes()), iargs(iir_args_bytes());
 
-        // the pipeline's groups: streams largest first, each to the group with the
+        // streams largest first: every launch lists its tasks in that order, so
+        // the blocks of the longest tasks (a 4K stream's threshold walk lanes)
+        // start in the first wave instead of trailing the launch; the pipeline's
+        // groups take the streams in the same order, each to the group with the
         // fewest pixels so far
         const int G = std::max(1, std::min(groups, n));
-        std::vector<int> grp(n, 0);
+        std::vector<int> grp(n, 0), order(n);
+        for (int k = 0; k < n; k++) order[k] = k;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+            return streams[ids[a]]->g.pixels > streams[ids[b]]->g.pixels;
+        });
         {
-            std::vector<int> order(n);
-            for (int k = 0; k < n; k++) order[k] = k;
-            std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-                return streams[ids[a]]->g.pixels > streams[ids[b]]->g.pixels;
-            });
             long long load[MAXG] = {};
             for (int k : order) {
                 int best = 0;
@@ -502,7 +508,7 @@ public:
             }
         }
 
-        for (int k = 0; k < n; k++) {
+        for (const int k : order) {
             Session& S = *streams[ids[k]];
             Launch* const LK = L[grp[k]];
             const Geom& g = S.g;
@@ -546,9 +552,21 @@ public:
                                        S.cfg.threshold_form, S.thr_hist ? 1 : 0, grids),
                          "threshold setup"))
                 return false;
+            // with a binade history the monoids of the sub-chunks wholly in level 0
+            // go in a launch of their own, which a steady tick runs beside the
+            // forward transform's levels 1-3
+            const int split = S.thr_hist && !S.cfg.planes_fp16 ? thr_level0_subchunks(views[0]) : 0;
             for (int st = 0; st < 5; st++) {
                 if ((st == 4) != (S.cfg.planes_fp16 != 0)) continue;   // FP16 planes: one kernel
                 if (st < 2 && S.thr_hist) continue;   // partial sums + prefix: first frame only
+                if (st == 2 && split > 0) {
+                    std::vector<char> part(targs);
+                    const unsigned b0 = thr_args_monoid_part(part.data(), 0, split);
+                    LK[L_THR_MON0].add(part.data(), b0, grids[st][1], b0 * grids[st][1]);
+                    const unsigned b1 = thr_args_monoid_part(part.data(), split, -1);
+                    LK[L_THR_MON].add(part.data(), b1, grids[st][1], b1 * grids[st][1]);
+                    continue;
+                }
                 LK[L_THR_PART + st].add(targs.data(), grids[st][0], grids[st][1],
                                        grids[st][0] * grids[st][1]);
             }
@@ -661,12 +679,22 @@ public:
                     return false;
             return true;
         };
-        auto thr = [&](int g, cudaStream_t st) {
-            for (int k = L_THR_PART; k <= L_THR16; k++)
-                if (!go(g, k, [&] { return launch_threshold_multi(k - L_THR_PART, P(g, k), M(g, k), L[g][k].total, st); }, "threshold"))
+        // threshold launches in order: partials, prefix, level-0 monoids, other
+        // monoids, walk, FP16 sum (a launch with no tasks is skipped); thr_a / thr_b
+        // are the parts before and after the forward transform's levels 1-3
+        auto thr_range = [&](int g, cudaStream_t st, int i0, int i1) {
+            static const int kind[6] = {L_THR_PART, L_THR_PREFIX, L_THR_MON0, L_THR_MON, L_THR_WALK, L_THR16};
+            static const int stage[6] = {0, 1, 2, 2, 3, 4};
+            for (int i = i0; i < i1; i++) {
+                const int k = kind[i];
+                if (!go(g, k, [&] { return launch_threshold_multi(stage[i], P(g, k), M(g, k), L[g][k].total, st); }, "threshold"))
                     return false;
+            }
             return true;
         };
+        auto thr = [&](int g, cudaStream_t st) { return thr_range(g, st, 0, 6); };
+        auto thr_a = [&](int g, cudaStream_t st) { return thr_range(g, st, 2, 3); };
+        auto thr_b = [&](int g, cudaStream_t st) { return thr_range(g, st, 0, 2) && thr_range(g, st, 3, 6); };
         auto iir = [&](int g, cudaStream_t st) {
             return go(g, L_IIR_PRESEED, [&] { return launch_iir_multi(P(g, L_IIR_PRESEED), M(g, L_IIR_PRESEED), L[g][L_IIR_PRESEED].total, 1, st); }, "IIR preseed") &&
                    go(g, L_IIR, [&] { return launch_iir_multi(P(g, L_IIR), M(g, L_IIR), L[g][L_IIR].total, 0, st); }, "IIR");
@@ -701,11 +729,14 @@ public:
                 !cuda_ok(cudaStreamWaitEvent(cs_fwd, ce_fork, 0), "stream wait"))
                 return false;
             for (int g = 0; g < G; g++)
-                if (!fwd0(g, cs_fwd) || !fwdl(g, cs_fwd) || !cuda_ok(cudaEventRecord(ce_f[g], cs_fwd), "event record"))
+                if (!fwd0(g, cs_fwd) || !cuda_ok(cudaEventRecord(ce_f0[g], cs_fwd), "event record") ||
+                    !fwdl(g, cs_fwd) || !cuda_ok(cudaEventRecord(ce_f[g], cs_fwd), "event record"))
                     return false;
             for (int g = 0; g < G; g++) {
                 cudaStream_t cs = cs_chain[g];
-                if (!cuda_ok(cudaStreamWaitEvent(cs, ce_f[g], 0), "stream wait") || !thr(g, cs)) return false;
+                // level-0 monoids beside levels 1-3 of the forward transform
+                if (!cuda_ok(cudaStreamWaitEvent(cs, ce_f0[g], 0), "stream wait") || !thr_a(g, cs)) return false;
+                if (!cuda_ok(cudaStreamWaitEvent(cs, ce_f[g], 0), "stream wait") || !thr_b(g, cs)) return false;
                 if (g > 0 && !cuda_ok(cudaStreamWaitEvent(cs, ce_i[g - 1], 0), "stream wait")) return false;
                 if (!invl(g, cs) || !inv0(g, cs) || !cuda_ok(cudaEventRecord(ce_i[g], cs), "event record"))
                     return false;
@@ -750,7 +781,8 @@ public:
                 t.sig = sig;
             }
             launches += t.graph_launches;
-            // a transfer outside the graphs (an earlier tick's) still reads its reconstructed luma
+            // a transfer outside the graphs (an earlier unsteady tick's, on st_xfer) may still
+            // read its reconstructed luma; a steady tick's transfer is in st_main's order
             if (xfer_pending && !cuda_ok(cudaStreamWaitEvent(st_main, ev_xfer, 0), "stream wait")) return false;
             if (!cuda_ok(cudaGraphLaunch(t.g_tick, st_main), "graph launch")) return false;
             if (!cuda_ok(cudaEventRecord(ev_inv, st_main), "event record")) return false;
@@ -773,7 +805,9 @@ public:
             if (!all(xfer, T_XFER, st_xfer)) return false;
         }
         if (!cuda_ok(cudaEventRecord(ev_xfer, st_xfer), "event record")) return false;
-        xfer_pending = true;
+        // only a transfer issued on st_xfer makes the next tick wait for ev_xfer (so a
+        // host callback queued on st_xfer after a steady tick never holds the next back)
+        xfer_pending = !steady;
         t.timed = timing;
         if (!cuda_ok(cudaEventRecord(t.done, st_xfer), "event record")) return false;
         if (done && !cuda_ok(cudaEventRecord(done, st_xfer), "event record")) return false;

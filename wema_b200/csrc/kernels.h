@@ -165,6 +165,12 @@ cudaError_t thr_args_fill(void* dst, const PyrView* views, int nch, const ThrScr
                           float* thr, float* sums, int batch_form, int use_hist, unsigned grids[5][2]);
 cudaError_t launch_threshold_multi(int stage, const void* d_args, const int* d_map, unsigned blocks,
                                    cudaStream_t st);
+// sub-chunks of the 6-slot array that lie wholly in level 0 (0: one level):
+// their monoids (stage 2) can run as soon as level 0's forward transform is done
+int thr_level0_subchunks(const PyrView& v);
+// sets the monoid launch of an args blob to sub-chunks sub0 .. sub1-1 (sub1 < 0:
+// to the end); its block count per channel
+unsigned thr_args_monoid_part(void* args, int sub0, int sub1);
 size_t iir_args_bytes();
 unsigned iir_args_fill(void* dst, const IirParams& p, const float* coef, void* state, int fp64, float* delta,
                        int warmup);   // returns the task's block count
@@ -176,7 +182,7 @@ cudaError_t iir_autotune(int dev, float ms[3], int* chosen);
 cudaError_t launch_iir_multi(const void* d_args, const int* d_map, unsigned blocks, int preseed,
                              cudaStream_t st);
 unsigned transfer_grid(TransferParams& p, unsigned& gx, unsigned& gy);
-// guided filter rows per sweep segment on a device (default 128)
+// guided filter rows per sweep segment on a device (default 64)
 int guided_rows(int dev);
 bool guided_set_rows(int dev, int rows);
 // times the sweep at each candidate segment height, keeps the fastest

@@ -84,7 +84,7 @@ constexpr int GS_OUT = GS_IN - 4 * GR;  // output columns per strip
 constexpr int GS_RING = 2 * GR + 1;     // rows in each ring
 constexpr int GS_WARPS = 2;             // strips per CTA (one per warp)
 constexpr int GS_THREADS = 32 * GS_WARPS;
-constexpr int GS_ROWS_DEFAULT = 128;
+constexpr int GS_ROWS_DEFAULT = 64;       // the autotuner's usual choice on B200
 constexpr float kEps = 0.01f;           // wema.c:315
 constexpr unsigned kFull = 0xffffffffu;
 

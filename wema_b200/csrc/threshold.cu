@@ -227,6 +227,7 @@ struct ThrArgs {
     float* sums;
     int batch_form;
     int use_hist;
+    int sub0;                   // monoids: first sub-chunk of this launch (a split launch)
 };
 
 // ---- FP64 partial sums: thread (lane j, block tb) covers EPT lane-elements
@@ -316,6 +317,9 @@ __device__ __forceinline__ void thr_prefix_body(const ThrArgs& a, int bx, int by
 // lane_monoids; small CTAs free their slot as soon as their own warps finish
 // instead of holding it for the slowest of eight.
 constexpr int MON_WARPS = 2;
+// CTAs per SM asked of the register allocator: 10 x 2 warps at 96 registers
+// (8 would allow 128 registers but only 16 warps per SM for a latency-bound kernel)
+constexpr int MON_MINB = 10;
 
 __device__ __forceinline__ void sub_candidates(const ThrArgs& a, const ThrScratch& sc,
                                                const ThrGeom& g, long long row, int sub,
@@ -438,11 +442,11 @@ __device__ __forceinline__ void thr_monoids_body(const ThrArgs& a, int bx, int b
     __shared__ PyrView sv;
     if (threadIdx.x == 0) {
         sv = v;
-        if (bx == 0) *sc.counter = 0u;   // the walk's lane counter
+        if (bx == 0 && a.sub0 == 0) *sc.counter = 0u;   // the walk's lane counter
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5, ln = threadIdx.x & 31;
-    const int sub = bx * MON_WARPS + warp;
+    const int sub = a.sub0 + bx * MON_WARPS + warp;
     if (sub >= g.nsub) return;   // whole warps only; no block barrier follows
     const int half = ln & 1;     // this thread's lanes: 4 * half + i
     const long long i0 = (long long)sub * (8 * G);
@@ -1123,10 +1127,10 @@ __global__ void __launch_bounds__(THR_THREADS) k_thr_partials(ThrArgs a) {
 __global__ void __launch_bounds__(THR_THREADS) k_thr_prefix(ThrArgs a) {
     thr_prefix_body(a, blockIdx.x, blockIdx.y);
 }
-__global__ void __launch_bounds__(32 * MON_WARPS, 16 / MON_WARPS) k_thr_monoids(ThrArgs a) {
+__global__ void __launch_bounds__(32 * MON_WARPS, MON_MINB) k_thr_monoids(ThrArgs a) {
     thr_monoids_body(a, blockIdx.x, blockIdx.y);
 }
-__global__ void __launch_bounds__(THR_THREADS, 1) k_thr_walk(ThrArgs a) {
+__global__ void __launch_bounds__(THR_THREADS, 2) k_thr_walk(ThrArgs a) {
     thr_walk_body(a, blockIdx.x, blockIdx.y);
 }
 // batched: task = one stream's ThrArgs
@@ -1140,12 +1144,12 @@ __global__ void __launch_bounds__(THR_THREADS)
     const TaskBlock t = task_block(map, blockIdx.x);
     thr_prefix_body(as[t.task], t.x, t.y);
 }
-__global__ void __launch_bounds__(32 * MON_WARPS, 16 / MON_WARPS)
+__global__ void __launch_bounds__(32 * MON_WARPS, MON_MINB)
     k_thr_monoids_multi(const ThrArgs* __restrict__ as, const int* __restrict__ map) {
     const TaskBlock t = task_block(map, blockIdx.x);
     thr_monoids_body(as[t.task], t.x, t.y);
 }
-__global__ void __launch_bounds__(THR_THREADS, 1)
+__global__ void __launch_bounds__(THR_THREADS, 2)
     k_thr_walk_multi(const ThrArgs* __restrict__ as, const int* __restrict__ map) {
     const TaskBlock t = task_block(map, blockIdx.x);
     thr_walk_body(as[t.task], t.x, t.y);
@@ -1157,11 +1161,19 @@ cudaError_t thr_prepare_device() {
     if (e != cudaSuccess) return e;
     static std::atomic<unsigned char> done[64];
     if (dev >= 0 && dev < 64 && done[dev].load(std::memory_order_acquire)) return cudaSuccess;
+    // the walk: two CTAs per SM (about 101 KB of shared memory and at most 128
+    // registers each), so a batch's lanes x streams take fewer waves
     e = cudaFuncSetAttribute(k_thr_walk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(WalkSmem));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_thr_walk_multi, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)sizeof(WalkSmem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_thr_walk, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_thr_walk_multi, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
     if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev].store(1, std::memory_order_release);
     return e;
 }
@@ -1222,6 +1234,22 @@ cudaError_t thr_args_fill(void* dst, const PyrView* views, int nch, const ThrScr
     for (int k = 0; k < 5; k++) grids[k][1] = (unsigned)nch;
     if (nsub == 0) grids[0][0] = 0;
     return cudaSuccess;
+}
+
+int thr_level0_subchunks(const PyrView& v) {
+    if (v.levels < 2) return 0;
+    const ThrGeom g = thr_geom(v.off6[v.levels]);
+    return (int)std::min<long long>(v.off6[1] / (LANES * G), g.nsub);
+}
+
+unsigned thr_args_monoid_part(void* args, int sub0, int sub1) {
+    ThrArgs a;
+    memcpy(&a, args, sizeof a);
+    if (sub1 < 0)
+        for (int c = 0; c < 3; c++) sub1 = max(sub1, thr_geom(a.v[c].off6[a.v[c].levels]).nsub);
+    a.sub0 = sub0;
+    memcpy(args, &a, sizeof a);
+    return (unsigned)((sub1 - sub0 + MON_WARPS - 1) / MON_WARPS);
 }
 
 cudaError_t launch_threshold_multi(int stage, const void* d_args, const int* d_map, unsigned blocks,
