@@ -189,7 +189,9 @@ __device__ __forceinline__ void prefetch_state_rows(const FwdLevelParams& p, int
 // ----------------------------------------------------------------- forward
 // C == 3: level 0 of a colour frame, all channels in one CTA, grid (tx, ty, 1).
 // C == 1: channel blockIdx.z (planes in), or the luma of an RGB frame.
-template <int C, int MODE, int LPW>
+// H16: the planes_fp16 variant's FP16 coefficient planes (p.h16), a
+// compile-time constant so the FP32 path carries no FP16 selects
+template <int C, int MODE, int LPW, bool H16>
 __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, int by, int bz) {
     extern __shared__ __align__(16) float dyn[];
     float* planes = dyn;                                   // [C][PLANE]
@@ -373,7 +375,7 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
             const int j = py0 + jj, ry = qy0 + jj;
             const int o = j * sw + i;
             const bool hy = 2 * j + 1 < ih;
-            const bool h = p.h16;
+            constexpr bool h = H16;
             float v[3];                                                                         // LH, HH, HL
             v[0] = hy ? pl[(32 + ry) * RS] : (prev ? pl_ld(prev, o, h) : 0.0f);
             v[1] = (hx && hy) ? pl[(32 + ry) * RS + ODD_COL] : (prev ? pl_ld(prev, pn + o, h) : 0.0f);
@@ -389,7 +391,9 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
 // ----------------------------------------------------------------- inverse
 // C == 1: grid (tiles_x, tiles_y, channels), planes out.
 // C == 3: one CTA per tile does all three channels (YCbCr -> RGB at level 0).
-template <int C, int OUT, int LPW>
+// H16: FP16 coefficient / delta planes and (p.out16) FP16 output planes,
+// a compile-time constant as in the forward body
+template <int C, int OUT, int LPW, bool H16>
 __device__ __forceinline__ void dwt_inv_body(const InvLevelParams& p, int bx, int by, int bz) {
     extern __shared__ __align__(16) float dyn[];
     float* planes = dyn;   // [C][PLANE]
@@ -414,16 +418,16 @@ __device__ __forceinline__ void dwt_inv_body(const InvLevelParams& p, int bx, in
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const int boff = q == 1 ? 2 * n : (q == 2 ? 0 : n);   // HL 2, LH 0, HH 1
-            const float* src = q == 0 ? p.ll[ch] : plane_at(p.coef[ch], boff, p.h16);
-            const float* dsrc = plane_at(p.delta[ch], boff, p.h16);
+            const float* src = q == 0 ? p.ll[ch] : plane_at(p.coef[ch], boff, H16);
+            const float* dsrc = plane_at(p.delta[ch], boff, H16);
             const bool okx = 2 * lane + (q & 1) < RW;
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 const int qy = warp + NWARP * u;
                 const bool ok = okx && 2 * qy + (q >> 1) < RH;
                 const int o = o0 + qy * sw;
-                xv[cc][q][u] = ok ? pl_ld(src, o, q != 0 && p.h16) : 0.0f;
-                if (q != 0) dv[cc][q - 1][u] = ok ? pl_ld(dsrc, o, p.h16) : 0.0f;
+                xv[cc][q][u] = ok ? pl_ld(src, o, q != 0 && H16) : 0.0f;
+                if (q != 0) dv[cc][q - 1][u] = ok ? pl_ld(dsrc, o, H16) : 0.0f;
             }
         }
     }
@@ -483,6 +487,7 @@ __device__ __forceinline__ void dwt_inv_body(const InvLevelParams& p, int bx, in
         __syncthreads();
     }
     // ---- output: one warp per tile row, lanes along x
+    const bool out16 = H16 && p.out16;
     for (int ly = ty0 + warp; ly < ty1; ly += NWARP) {
         const int rowpix = (ry0 + ly) * ow + rx0;
         const int pr = prow(ly) * RS;
@@ -494,15 +499,15 @@ __device__ __forceinline__ void dwt_inv_body(const InvLevelParams& p, int bx, in
             const int idx = pr + pcol(lx);
             if (OUT == kOutPlanes) {
 #pragma unroll
-                for (int cc = 0; cc < C; cc++) pl_st(p.out_planes[c0 + cc], pi, planes[cc * PLANE + idx], p.out16);
+                for (int cc = 0; cc < C; cc++) pl_st(p.out_planes[c0 + cc], pi, planes[cc * PLANE + idx], out16);
             } else {
                 const float y = planes[idx];
                 const float cb = planes[(C > 1 ? PLANE : 0) + idx];
                 const float cr = planes[(C > 2 ? 2 * PLANE : 0) + idx];
                 if (p.out_planes[0]) {
-                    pl_st(p.out_planes[0], pi, y, p.out16);
-                    pl_st(p.out_planes[1], pi, cb, p.out16);
-                    pl_st(p.out_planes[2], pi, cr, p.out16);
+                    pl_st(p.out_planes[0], pi, y, out16);
+                    pl_st(p.out_planes[1], pi, cb, out16);
+                    pl_st(p.out_planes[2], pi, cr, out16);
                 }
                 float r, g, b;
                 ycbcr_to_rgb(y, cb, cr, r, g, b);
@@ -531,27 +536,35 @@ __device__ __forceinline__ void dwt_inv_body(const InvLevelParams& p, int bx, in
 // LPW lines per warp in flight (2, 4 or 8); every variant computes the same
 // coefficients, bit for bit.
 constexpr int LPW_DEF = 4;
+// a launch's FP32 and FP16-plane tasks take the body compiled for each (the
+// branch is uniform over a CTA)
 template <int C, int MODE>
 __global__ void __launch_bounds__(DWT_THREADS, 3) k_dwt_fwd(FwdLevelParams p) {
-    dwt_fwd_body<C, MODE, LPW_DEF>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+    if (p.h16) dwt_fwd_body<C, MODE, LPW_DEF, true>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+    else dwt_fwd_body<C, MODE, LPW_DEF, false>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <int C, int MODE, int MINB, int LPW>
 __global__ void __launch_bounds__(DWT_THREADS, MINB)
     k_dwt_fwd_multi(const FwdLevelParams* __restrict__ ps, const int* __restrict__ map) {
     const TaskBlock t = task_block(map, blockIdx.x);
-    dwt_fwd_body<C, MODE, LPW>(ps[t.task], t.x, t.y, t.z);
+    const FwdLevelParams& p = ps[t.task];
+    if (p.h16) dwt_fwd_body<C, MODE, LPW, true>(p, t.x, t.y, t.z);
+    else dwt_fwd_body<C, MODE, LPW, false>(p, t.x, t.y, t.z);
 }
 // one channel: 4 CTAs per SM (measured in the batched form: 40% faster than the
 // compiler's 82-register choice, which leaves 2); colour: the compiler's choice
 template <int C, int OUT>
 __global__ void __launch_bounds__(DWT_THREADS, C == 1 ? 4 : 1) k_dwt_inv(InvLevelParams p) {
-    dwt_inv_body<C, OUT, LPW_DEF>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+    if (p.h16) dwt_inv_body<C, OUT, LPW_DEF, true>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+    else dwt_inv_body<C, OUT, LPW_DEF, false>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <int C, int OUT, int MINB, int LPW>
 __global__ void __launch_bounds__(DWT_THREADS, MINB)
     k_dwt_inv_multi(const InvLevelParams* __restrict__ ps, const int* __restrict__ map) {
     const TaskBlock t = task_block(map, blockIdx.x);
-    dwt_inv_body<C, OUT, LPW>(ps[t.task], t.x, t.y, t.z);
+    const InvLevelParams& p = ps[t.task];
+    if (p.h16) dwt_inv_body<C, OUT, LPW, true>(p, t.x, t.y, t.z);
+    else dwt_inv_body<C, OUT, LPW, false>(p, t.x, t.y, t.z);
 }
 
 // ---- tuning of the batched luma kernels, per device: variant index
