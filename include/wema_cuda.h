@@ -310,7 +310,7 @@ int wema_cuda_server_stats(wema_cuda_server *srv, int reset, wema_cuda_serve_sta
  *     compiler's choice), 3, 4} x lines lifted per warp at a time {2, 4, 8}
  *     (variant = 3 * index + index; a 3840x4320 trial frame, the forward
  *     with the temporal filter's step inside as steady batched ticks run it)
- *     and keeps the fastest of each (forward 4x4, inverse 4x8 until then);
+ *     and keeps the fastest of each (4x4 for both until then);
  * allocating ~950 MB for the trials (one at a time) and freeing it.  Every
  * later launch on the device uses the choices.  Returns the positions per
  * thread (or -1) and writes the timings to `report` (may be NULL; 1 KiB is

@@ -580,9 +580,9 @@ static int dwt_dev_now() {
 }
 int dwt_variant(int dev, int inverse) {
     const int v = (dev >= 0 && dev < 64) ? g_dwt_var[dev][inverse ? 1 : 0].load() : 0;
-    // defaults until tuned: the autotuner's usual choices on B200 - forward 4 CTAs
-    // per SM x 4 lines per warp, inverse 4 CTAs per SM x 8 lines per warp
-    return v > 0 ? v - 1 : (inverse ? 2 * 3 + 2 : 2 * 3 + 1);
+    // defaults until tuned: the fastest in a 48-stream tick on B200 - 4 CTAs per
+    // SM x 4 lines per warp, forward and inverse
+    return v > 0 ? v - 1 : 2 * 3 + 1;
 }
 bool dwt_set_variant(int dev, int inverse, int v) {
     if (dev < 0 || dev >= 64 || v < 0 || v >= kDwtVariants) return false;
