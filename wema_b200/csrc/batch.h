@@ -322,10 +322,6 @@ public:
         return true;
     }
 
-    // fn(arg) on a driver thread once everything issued so far has completed
-    bool after_last_tick(cudaHostFn_t fn, void* arg) {
-        return cuda_ok(cudaLaunchHostFunc(st_xfer, fn, arg), "cudaLaunchHostFunc");
-    }
 
     bool sync() {
         if (!cuda_ok(cudaStreamSynchronize(st_h2d), "sync")) return false;
@@ -805,8 +801,8 @@ public:
             if (!all(xfer, T_XFER, st_xfer)) return false;
         }
         if (!cuda_ok(cudaEventRecord(ev_xfer, st_xfer), "event record")) return false;
-        // only a transfer issued on st_xfer makes the next tick wait for ev_xfer (so a
-        // host callback queued on st_xfer after a steady tick never holds the next back)
+        // only a transfer issued on st_xfer makes the next tick wait for ev_xfer (a
+        // steady tick's transfer is in st_main's order already)
         xfer_pending = !steady;
         t.timed = timing;
         if (!cuda_ok(cudaEventRecord(t.done, st_xfer), "event record")) return false;

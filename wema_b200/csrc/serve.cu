@@ -71,7 +71,12 @@ public:
         std::vector<int> sids;
         std::vector<double> t_submit;
         double t_issue = 0, t_done = -1;
+        cudaEvent_t ev = nullptr;          // recorded when the tick's outputs are written
     };
+    // completion events for ticks, reused; the dispatcher polls them (no host
+    // callback sits in a stream, where it could hold back later launches that
+    // share its hardware queue)
+    std::vector<cudaEvent_t> ev_pool;
 
     Batch batch;
     size_t budget = 0, used = 0;
@@ -106,7 +111,11 @@ public:
         if (th.joinable()) th.join();
         if (th_alloc.joinable()) th_alloc.join();
         batch.sync();
-        for (Tick* t : inflight) delete t;
+        for (Tick* t : inflight) {
+            if (t->ev) cudaEventDestroy(t->ev);
+            delete t;
+        }
+        for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
         for (auto& m : made) delete m.second;
     }
 
@@ -168,14 +177,14 @@ public:
         }
     }
 
-    static void CUDART_CB on_done(void* arg) {
-        Tick* t = static_cast<Tick*>(arg);
-        Server* s = t->srv;
-        {
-            std::lock_guard<std::mutex> lk(s->mu);
-            t->t_done = now_ms();
+    cudaEvent_t take_event() {
+        if (!ev_pool.empty()) {
+            cudaEvent_t e = ev_pool.back();
+            ev_pool.pop_back();
+            return e;
         }
-        s->cv.notify_all();
+        cudaEvent_t e = nullptr;
+        return cuda_ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate") ? e : nullptr;
     }
 
     int live() const {
@@ -190,9 +199,17 @@ public:
     }
 
     void reap() {
-        while (!inflight.empty() && inflight.front()->t_done >= 0) {
+        bool any = false;
+        while (!inflight.empty()) {
             Tick* t = inflight.front();
+            if (t->t_done < 0) {
+                const cudaError_t q = cudaEventQuery(t->ev);
+                if (q == cudaErrorNotReady) break;
+                t->t_done = now_ms();
+                if (q != cudaSuccess && err.empty()) err = std::string("tick: ") + cudaGetErrorString(q);
+            }
             inflight.pop_front();
+            any = true;
             const double span = t->t_done - t->t_issue;
             span_sum += span;
             span_max = std::max(span_max, span);
@@ -205,8 +222,10 @@ public:
                 mpix_done += (double)s.cfg.width * s.cfg.height * 1e-6;
                 lat_ms.push_back((float)(t->t_done - t->t_submit[k]));
             }
+            ev_pool.push_back(t->ev);
             delete t;
         }
+        if (any) cv.notify_all();   // drain() and submitters wait on progress
     }
 
     // (sess may grow while the lock is released: entries are re-indexed after)
@@ -283,6 +302,12 @@ public:
             if ((int)inflight.size() < max_inflight && err.empty() && !hold) {
                 Tick* t = new Tick();
                 t->srv = this;
+                t->ev = take_event();
+                if (!t->ev) {
+                    fail("tick event");
+                    delete t;
+                    continue;
+                }
                 ids.clear();
                 in.clear();
                 out.clear();
@@ -303,9 +328,8 @@ public:
                     ticks++;
                     t->t_issue = now_ms();
                     lk.unlock();
-                    bool ok = batch.tick(ids.data(), in.data(), out.data(), (int)ids.size(), nullptr, nullptr);
+                    bool ok = batch.tick(ids.data(), in.data(), out.data(), (int)ids.size(), nullptr, t->ev);
                     const std::string why = ok ? "" : last_error();
-                    ok = ok && batch.after_last_tick(on_done, t);
                     const double dt = now_ms() - t->t_issue;
                     lk.lock();
                     host_sum += dt;
@@ -316,9 +340,12 @@ public:
                     }
                     continue;
                 }
+                ev_pool.push_back(t->ev);
                 delete t;
             }
-            cv.wait_for(lk, std::chrono::milliseconds(2));
+            // ticks in flight: poll their events often; else wait for work
+            if (inflight.empty()) cv.wait_for(lk, std::chrono::milliseconds(2));
+            else cv.wait_for(lk, std::chrono::microseconds(50));
         }
     }
 
