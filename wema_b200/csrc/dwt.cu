@@ -488,6 +488,31 @@ __device__ __forceinline__ void dwt_inv_body(const InvLevelParams& p, int bx, in
     }
     // ---- output: one warp per tile row, lanes along x
     const bool out16 = H16 && p.out16;
+    if (OUT == kOutPlanes) {
+        // two adjacent pixels per lane: the even one from the row's even half in
+        // shared memory, the odd one ODD_COL further (tx0 is even), one index
+        // computation for both and, on an even pixel index, one 8-byte store
+        for (int ly = ty0 + warp; ly < ty1; ly += NWARP) {
+            const int lx = tx0 + 2 * lane;
+            if (lx >= tx1) continue;
+            const int pi = (ry0 + ly) * ow + rx0 + lx;
+            const int ie = prow(ly) * RS + (lx >> 1);
+            const bool two = lx + 1 < tx1;
+#pragma unroll
+            for (int cc = 0; cc < C; cc++) {
+                float* o = p.out_planes[c0 + cc];
+                const float ve = planes[cc * PLANE + ie];
+                const float vo = two ? planes[cc * PLANE + ie + ODD_COL] : 0.0f;
+                if (!out16 && two && !(pi & 1)) {
+                    *reinterpret_cast<float2*>(o + pi) = make_float2(ve, vo);
+                } else {
+                    pl_st(o, pi, ve, out16);
+                    if (two) pl_st(o, pi + 1, vo, out16);
+                }
+            }
+        }
+        return;
+    }
     for (int ly = ty0 + warp; ly < ty1; ly += NWARP) {
         const int rowpix = (ry0 + ly) * ow + rx0;
         const int pr = prow(ly) * RS;
