@@ -27,6 +27,7 @@
 // reference's: x = fma(left + right, c, x), scalings as separate multiplies
 // (dwt.c:45-170 as GCC -Ofast evaluates it), so coefficients are bit-exact.
 #include <atomic>
+#include <type_traits>
 
 #include "cascade.cuh"
 #include "common.cuh"
@@ -134,8 +135,10 @@ __device__ __forceinline__ void liftN(float* const (&b)[LPW], const bool (&act)[
 // the forward transform writes them: the filter reads the coefficient as
 // stored (FP16-rounded in the planes_fp16 variant), so the deltas equal
 // those of the separate filter kernel bit for bit.  All state loads first.
+// all_simd: no coefficient of the CTA's tile takes the scalar-tail form
+// (uniform over the CTA), so the per-coefficient test and select drop out.
 __device__ __forceinline__ void temporal_step3(const FwdLevelParams& p, int ch, void* st, int o, int n,
-                                               const float (&v)[3], bool h) {
+                                               const float (&v)[3], bool h, bool all_simd) {
     float x[3];
 #pragma unroll
     for (int b = 0; b < 3; b++) x[b] = h ? __half2float(__float2half_rn(v[b])) : v[b];
@@ -145,28 +148,37 @@ __device__ __forceinline__ void temporal_step3(const FwdLevelParams& p, int ch, 
         double2 hp[3], lp[3];
 #pragma unroll
         for (int b = 0; b < 3; b++) {
-            const long long u = (long long)b * n + o;
-            hp[b] = __ldcs(s2 + 2 * u);
-            lp[b] = __ldcs(s2 + 2 * u + 1);
+            const int u = b * n + o;
+            hp[b] = __ldcs(s2 + 2 * (long long)u);
+            lp[b] = __ldcs(s2 + 2 * (long long)u + 1);
         }
 #pragma unroll
         for (int b = 0; b < 3; b++) {
-            const long long u = (long long)b * n + o;
+            const int u = b * n + o;
             pl_st(dl, u, cascade64(p.iir_c, hp[b], lp[b], x[b]), h);
-            __stcs(s2 + 2 * u, hp[b]);
-            __stcs(s2 + 2 * u + 1, lp[b]);
+            __stcs(s2 + 2 * (long long)u, hp[b]);
+            __stcs(s2 + 2 * (long long)u + 1, lp[b]);
         }
     } else {
         float4* s4 = static_cast<float4*>(st);
         float4 sv[3];
 #pragma unroll
-        for (int b = 0; b < 3; b++) sv[b] = __ldcs(s4 + (long long)b * n + o);   // touched once: evict first
+        for (int b = 0; b < 3; b++) sv[b] = __ldcs(s4 + (b * n + o));   // touched once: evict first
+        if (all_simd) {   // the whole tile before the scalar-tail positions (uniform)
 #pragma unroll
-        for (int b = 0; b < 3; b++) {
-            const long long u = (long long)b * n + o;
-            const bool tail = p.iir_off6 + u >= p.iir_simd_end;
-            pl_st(dl, u, cascade(p.iir_c, sv[b], x[b], tail), h);
-            __stcs(s4 + u, sv[b]);
+            for (int b = 0; b < 3; b++) {
+                const int u = b * n + o;
+                pl_st(dl, u, cascade(p.iir_c, sv[b], x[b], false), h);
+                __stcs(s4 + u, sv[b]);
+            }
+        } else {
+#pragma unroll
+            for (int b = 0; b < 3; b++) {
+                const int u = b * n + o;
+                const bool tail = p.iir_off6 + u >= p.iir_simd_end;
+                pl_st(dl, u, cascade(p.iir_c, sv[b], x[b], tail), h);
+                __stcs(s4 + u, sv[b]);
+            }
         }
     }
 }
@@ -289,35 +301,42 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
 #pragma unroll
         for (int cc = 0; cc < C; cc++) pout[cc] = p.plane_out[cc];
         const long long vec_end = p.vec_end;
+        // ALL: the whole staged region lies in the vector body (every tile but
+        // the frame's last ones), so no pixel needs the epilogue's form
+        auto convert = [&](auto all) {
+            constexpr bool ALL = decltype(all)::value;
 #pragma unroll
-        for (int r = 0; r < RPW; r++) {
-            const int ly = warp + r * NWARP;
-            if (ly >= RH) continue;
-            const int rowpix = (ry0 + ly) * iw + rx0;
-            const bool rowvec = rowpix + RW <= vec_end;   // the whole staged row in the vector body
-            float* dst = planes + prow(ly) * RS;
+            for (int r = 0; r < RPW; r++) {
+                const int ly = warp + r * NWARP;
+                if (ly >= RH) continue;
+                const int rowpix = (ry0 + ly) * iw + rx0;
+                const bool rowvec = ALL || rowpix + RW <= vec_end;   // the whole staged row in the vector body
+                float* dst = planes + prow(ly) * RS;
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const int lx = lane + 32 * h;
-                if (lx >= RW) continue;
-                const int pi = rowpix + lx;
-                const bool vec = rowvec || pi < vec_end;
-                const float rr = rgb[r][h][0], gg = rgb[r][h][1], bb = rgb[r][h][2];
-                float out[3];
-                if (C == 1) {
-                    out[0] = vec ? luma_vec(rr, gg, bb) : luma_tail(rr, gg, bb);
-                } else if (vec) {
-                    ycbcr_vec(rr, gg, bb, out[0], out[1], out[2]);
-                } else {
-                    ycbcr_tail(rr, gg, bb, out[0], out[1], out[2]);
-                }
+                for (int h = 0; h < 2; h++) {
+                    const int lx = lane + 32 * h;
+                    if (lx >= RW) continue;
+                    const int pi = rowpix + lx;
+                    const bool vec = rowvec || pi < vec_end;
+                    const float rr = rgb[r][h][0], gg = rgb[r][h][1], bb = rgb[r][h][2];
+                    float out[3];
+                    if (C == 1) {
+                        out[0] = (ALL || vec) ? luma_vec(rr, gg, bb) : luma_tail(rr, gg, bb);
+                    } else if (ALL || vec) {
+                        ycbcr_vec(rr, gg, bb, out[0], out[1], out[2]);
+                    } else {
+                        ycbcr_tail(rr, gg, bb, out[0], out[1], out[2]);
+                    }
 #pragma unroll
-                for (int cc = 0; cc < C; cc++) {
-                    dst[cc * PLANE + pcol(lx)] = out[cc];
-                    if (pout[cc]) pout[cc][pi] = out[cc];
+                    for (int cc = 0; cc < C; cc++) {
+                        dst[cc * PLANE + pcol(lx)] = out[cc];
+                        if (pout[cc]) pout[cc][pi] = out[cc];
+                    }
                 }
             }
-        }
+        };
+        if ((long long)(ry0 + RH - 1) * iw + rx0 + RW <= vec_end) convert(std::true_type{});
+        else convert(std::false_type{});
     }
     __syncthreads();
 
@@ -362,6 +381,9 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
     const int i = px0 + lane;
     const bool hx = 2 * i + 1 < iw;
     const int n = (int)p.n, pn = (int)p.prev_n;
+    // every coefficient of the tile lies before the scalar-tail positions of
+    // the 6-slot array (all but the last tiles of a frame's last level)
+    const bool all_simd = p.iir_off6 + 2 * p.n + (long long)(py0 + nj - 1) * sw + px0 + ni - 1 < p.iir_simd_end;
 #pragma unroll
     for (int cc = 0; cc < C; cc++) {
         const int ch = ch0 + cc;
@@ -383,7 +405,7 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
             ll[o] = pl[ry * RS];
 #pragma unroll
             for (int b = 0; b < 3; b++) pl_st(bands, b * n + o, v[b], h);
-            if (st) temporal_step3(p, ch, st, o, n, v, h);
+            if (st) temporal_step3(p, ch, st, o, n, v, h, all_simd);
         }
     }
 }

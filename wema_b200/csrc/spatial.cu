@@ -190,13 +190,20 @@ struct RowLoad {
                 gy[j] = gv[j];
             }
         }
+        float Iv[4];
+        if (pi0 + 3 < p.vec_end) {   // all four in the vector body (every row but the last)
+#pragma unroll
+            for (int j = 0; j < 4; j++) Iv[j] = luma_vec(rr[j], gg[j], bb[j]);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                Iv[j] = pi0 + j < p.vec_end ? luma_vec(rr[j], gg[j], bb[j]) : luma_tail(rr[j], gg[j], bb[j]);
+        }
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             const bool in = any && (FAST || (cx + j >= 0 && cx + j < p.w));
-            const float Iv = pi0 + j < p.vec_end ? luma_vec(rr[j], gg[j], bb[j])
-                                                 : luma_tail(rr[j], gg[j], bb[j]);
-            I[j] = in ? Iv : 0.f;
-            P[j] = in ? __fadd_rn(gy[j], -Iv) : 0.f;
+            I[j] = in ? Iv[j] : 0.f;
+            P[j] = in ? __fadd_rn(gy[j], -Iv[j]) : 0.f;
         }
     }
 };
