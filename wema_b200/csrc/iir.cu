@@ -117,17 +117,18 @@ __device__ __forceinline__ void iir_body64(const IirDev& a, int block, int nbloc
     }
 }
 
-template <int U>
-__device__ __forceinline__ void iir_body(const IirDev& a, int block, int nblocks) {
-    if (a.fp64) {
-        iir_body64<(U > 4 ? 4 : U)>(a, block, nblocks);   // double state: at most 4 in registers
-        return;
-    }
+// H16: FP16 coefficient / delta planes (planes_fp16), a compile-time constant
+template <int U, bool H16>
+__device__ __forceinline__ void iir_body_t(const IirDev& a, int block, int nblocks) {
     const long long pu = a.p.uoff[a.p.levels];
     const long long B = (long long)nblocks * IIR_THREADS;
     const float* __restrict__ coef = a.coef;
     float4* __restrict__ state = static_cast<float4*>(a.state);
     float* __restrict__ dout = a.delta_out;
+    // a position's 6-slot index is u + uoff[its level] <= u + uoff[last level]:
+    // below this bound (and pu) every position exists and none takes the
+    // scalar-tail form
+    const long long no_tail = min(a.p.simd_end - a.p.uoff[a.p.levels > 0 ? a.p.levels - 1 : 0], pu);
     for (long long u0 = block * (long long)IIR_THREADS + threadIdx.x; u0 < pu; u0 += U * B) {
         float x[U];
         float4 st[U];
@@ -135,9 +136,18 @@ __device__ __forceinline__ void iir_body(const IirDev& a, int block, int nblocks
         for (int j = 0; j < U; j++) {
             const long long u = u0 + j * B;
             if (u < pu) {
-                x[j] = pl_ld(coef, u, a.p.h16);
+                x[j] = pl_ld(coef, u, H16);
                 st[j] = __ldcs(state + u);          // touched once per frame: evict first
             }
+        }
+        if (u0 + (U - 1) * B < no_tail) {           // (uniform but for one grid-stride step)
+#pragma unroll
+            for (int j = 0; j < U; j++) {
+                const long long u = u0 + j * B;
+                pl_st(dout, u, cascade(a.p.c, st[j], x[j], false), H16);
+                __stcs(state + u, st[j]);
+            }
+            continue;
         }
 #pragma unroll
         for (int j = 0; j < U; j++) {
@@ -145,11 +155,18 @@ __device__ __forceinline__ void iir_body(const IirDev& a, int block, int nblocks
             if (u < pu) {
                 bool tail;
                 level_of(a.p, u, tail);
-                pl_st(dout, u, cascade(a.p.c, st[j], x[j], tail), a.p.h16);
+                pl_st(dout, u, cascade(a.p.c, st[j], x[j], tail), H16);
                 __stcs(state + u, st[j]);
             }
         }
     }
+}
+
+template <int U>
+__device__ __forceinline__ void iir_body(const IirDev& a, int block, int nblocks) {
+    if (a.fp64) iir_body64<(U > 4 ? 4 : U)>(a, block, nblocks);   // double state: at most 4 in registers
+    else if (a.p.h16) iir_body_t<U, true>(a, block, nblocks);
+    else iir_body_t<U, false>(a, block, nblocks);
 }
 
 __global__ void __launch_bounds__(IIR_THREADS) k_iir_preseed(IirDev a) {
