@@ -533,21 +533,16 @@ __device__ __forceinline__ void dwt_inv_body(const InvLevelParams& p, int bx, in
                 }
             }
         }
-        return;
-    }
-    for (int ly = ty0 + warp; ly < ty1; ly += NWARP) {
-        const int rowpix = (ry0 + ly) * ow + rx0;
-        const int pr = prow(ly) * RS;
+    } else {   // RGB out (colour level 0)
+        for (int ly = ty0 + warp; ly < ty1; ly += NWARP) {
+            const int rowpix = (ry0 + ly) * ow + rx0;
+            const int pr = prow(ly) * RS;
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int lx = tx0 + lane + 32 * h;
-            if (lx >= tx1) continue;
-            const int pi = rowpix + lx;
-            const int idx = pr + pcol(lx);
-            if (OUT == kOutPlanes) {
-#pragma unroll
-                for (int cc = 0; cc < C; cc++) pl_st(p.out_planes[c0 + cc], pi, planes[cc * PLANE + idx], out16);
-            } else {
+            for (int h = 0; h < 2; h++) {
+                const int lx = tx0 + lane + 32 * h;
+                if (lx >= tx1) continue;
+                const int pi = rowpix + lx;
+                const int idx = pr + pcol(lx);
                 const float y = planes[idx];
                 const float cb = planes[(C > 1 ? PLANE : 0) + idx];
                 const float cr = planes[(C > 2 ? 2 * PLANE : 0) + idx];
