@@ -70,16 +70,15 @@ WORKLOADS = {
 }
 METRIC = "Mpix-frames/s"
 
-# DRAM bytes (read + write) per frame of a stage's kernels from one ncu
-# capture each, keyed by (workload, stage); stages not captured report null.
-# profiles/k_thr_monoids_plain_fullhd_color.txt, k_thr_walk_plain_fullhd_color.txt
-# and batched_kernels_16streams.md hold the captures and the commands that made them.
-# DRAM bytes (read + written) per launch from ncu captures (profiles/).  The
-# batched kernels were captured on a tick of 16 streams (8 x 640x480 +
-# 8 x 1920x1080, 19.05 Mpix) and are scaled by pixels to the 77.72 Mpix of the
-# 48-stream tick; the threshold of the plain workload is monoids + walk.
+# DRAM bytes (read + written) per launch of a stage's kernels from ncu
+# captures (summaries and commands in profiles/), keyed by (workload, stage);
+# stages not captured report null.  The batched kernels were captured on a
+# tick of 16 streams (8 x 640x480 + 8 x 1920x1080, 19.05 Mpix,
+# `--workload profile_batch16`) and are scaled by pixels to the 77.72 Mpix of
+# the 48-stream tick; the threshold of the plain workload is monoids + walk.
 _MIX = 77.722 / 19.046
 TRAFFIC_NCU = {
+    ("mixed_streams_48", "fwd_dwt_level0"): int((288116224 + 304738048) * _MIX),
     ("mixed_streams_48", "luma_transfer"): int((148669184 + 34321152) * _MIX),
     ("mixed_streams_48", "inv_dwt_level0"): int((133352960 + 47001344) * _MIX),
     ("plain_fullhd_color", "threshold"): 25081088 + 2323456,
