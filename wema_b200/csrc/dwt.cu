@@ -240,47 +240,38 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
         }
     } else {
         float rgb[RPW][2][3];
+        // lane k holds pixels 2k and 2k + 1 of each of its rows (rgb[r][0], [1])
         if (MODE == kSrcRgbU8) {
-            // a row's bytes through aligned 32-bit words (an aligned word
-            // that holds a byte of the frame is mapped memory)
-            uint32_t wv[RPW][2];
-            int offs[RPW];
+            // the lane's 6 bytes at byte off + 6k of the row: the (at most 3)
+            // aligned 32-bit words holding them, loaded directly (neighbouring
+            // lanes share words through L1; an aligned word that holds a byte of
+            // the frame is mapped memory, words past the row's last are not read)
+            uint32_t wv[RPW][3];
+            int sh[RPW];
 #pragma unroll
             for (int r = 0; r < RPW; r++) {
                 const int ly = warp + r * NWARP;
                 const uintptr_t a0 = reinterpret_cast<uintptr_t>(
                     p.src_u8 + 3 * ((ry0 + min(ly, RH - 1)) * iw + rx0));
                 const uint32_t* w0 = reinterpret_cast<const uint32_t*>(a0 & ~(uintptr_t)3);
-                offs[r] = (int)(a0 & 3);
-                const int nw = (offs[r] + 3 * RW + 3) >> 2;
-                wv[r][0] = (ly < RH && lane < nw) ? __ldg(w0 + lane) : 0u;
-                wv[r][1] = (ly < RH && lane + 32 < nw) ? __ldg(w0 + lane + 32) : 0u;
+                const int off = (int)(a0 & 3);
+                const int nw = (off + 3 * RW + 3) >> 2;
+                const int wb = (off + 6 * lane) >> 2;
+                sh[r] = 8 * ((off + 6 * lane) & 3);
+                const bool row = ly < RH && 2 * lane < RW;
+#pragma unroll
+                for (int k = 0; k < 3; k++) wv[r][k] = (row && wb + k < nw) ? __ldg(w0 + wb + k) : 0u;
             }
-            // pixel lx's bytes start at byte off + 3 lx of the row's words:
-            // fetch that word and the next by shuffles, funnel-shift them out
 #pragma unroll
             for (int r = 0; r < RPW; r++) {
-#pragma unroll
-                for (int h = 0; h < 2; h++) {
-                    const int b = offs[r] + 3 * (lane + 32 * h);
-                    const int w = b >> 2;           // 0 .. 48
-                    uint32_t lo, hi;
-                    if (h == 0) {                   // w <= 24: both words in the low half
-                        lo = __shfl_sync(FULL, wv[r][0], w);
-                        hi = __shfl_sync(FULL, wv[r][0], w + 1);
-                    } else {
-                        const uint32_t l0 = __shfl_sync(FULL, wv[r][0], w & 31);
-                        const uint32_t l1 = __shfl_sync(FULL, wv[r][1], w & 31);
-                        const uint32_t h0 = __shfl_sync(FULL, wv[r][0], (w + 1) & 31);
-                        const uint32_t h1 = __shfl_sync(FULL, wv[r][1], (w + 1) & 31);
-                        lo = w < 32 ? l0 : l1;
-                        hi = w + 1 < 32 ? h0 : h1;
-                    }
-                    const uint32_t x = __funnelshift_r(lo, hi, 8 * (b & 3));
-                    rgb[r][h][0] = byte_of(x, 0);      // fl(byte / 255)
-                    rgb[r][h][1] = byte_of(x, 1);
-                    rgb[r][h][2] = byte_of(x, 2);
-                }
+                const uint32_t x0 = __funnelshift_r(wv[r][0], wv[r][1], sh[r]);   // bytes 0-3
+                const uint32_t x1 = __funnelshift_r(wv[r][1], wv[r][2], sh[r]);   // bytes 4-7
+                rgb[r][0][0] = byte_of(x0, 0);      // fl(byte / 255)
+                rgb[r][0][1] = byte_of(x0, 1);
+                rgb[r][0][2] = byte_of(x0, 2);
+                rgb[r][1][0] = byte_of(x0, 3);
+                rgb[r][1][1] = byte_of(x1, 0);
+                rgb[r][1][2] = byte_of(x1, 1);
             }
         } else {
 #pragma unroll
@@ -288,7 +279,7 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
                 const int ly = warp + r * NWARP;
 #pragma unroll
                 for (int h = 0; h < 2; h++) {
-                    const int lx = lane + 32 * h;
+                    const int lx = 2 * lane + h;
                     const bool ok = ly < RH && lx < RW;
                     const float* q = p.src_f32 + 3 * ((ry0 + (ok ? ly : 0)) * iw + rx0 + (ok ? lx : 0));
                     rgb[r][h][0] = q[0];
@@ -314,7 +305,7 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
                 float* dst = planes + prow(ly) * RS;
 #pragma unroll
                 for (int h = 0; h < 2; h++) {
-                    const int lx = lane + 32 * h;
+                    const int lx = 2 * lane + h;
                     if (lx >= RW) continue;
                     const int pi = rowpix + lx;
                     const bool vec = rowvec || pi < vec_end;
