@@ -56,6 +56,7 @@ struct Launch {
     std::vector<int> gx, gy, nblk;
     unsigned total = 0;
     size_t params_off = 0, map_off = 0;   // device offsets in the tick's table
+    bool any16 = false;                   // some task has FP16 planes (planes_fp16)
     void reset(size_t e) {
         elem = e;
         params.clear();
@@ -63,6 +64,7 @@ struct Launch {
         gy.clear();
         nblk.clear();
         total = 0;
+        any16 = false;
     }
     void add(const void* p, unsigned x, unsigned y, unsigned blocks) {
         if (blocks == 0) return;
@@ -532,13 +534,10 @@ public:
                 p.prev_n = l > 0 ? g.n[l - 1] : 0;
                 if (S.frames_processed > 0) S.fill_temporal(p, l);   // the filter's step inside the transform
                 unsigned gx, gy;
-                if (l == 0) {
-                    const unsigned b = dwt_fwd_grid(p, 1, gx, gy);
-                    LK[nch == 3 ? L_FWD0_COLOR : L_FWD0_LUMA].add(&p, gx, gy, b);
-                } else {
-                    const unsigned b = dwt_fwd_grid(p, nch, gx, gy);
-                    LK[L_FWD0_COLOR + l].add(&p, gx, gy, b);
-                }
+                Launch& lf = LK[l == 0 ? (nch == 3 ? L_FWD0_COLOR : L_FWD0_LUMA) : L_FWD0_COLOR + l];
+                const unsigned b = dwt_fwd_grid(p, l == 0 ? 1 : nch, gx, gy);
+                lf.add(&p, gx, gy, b);
+                lf.any16 |= h;
             }
             // ---- threshold
             PyrView views[3];
@@ -597,14 +596,11 @@ public:
                     iq.out_planes[c] = (l > 0 || nch == 1) ? q.rec[c][l] : nullptr;
                 }
                 unsigned gx, gy;
-                if (l == 0 && nch == 3) {
-                    iq.out_u8 = out[k];
-                    const unsigned b = dwt_inv_grid(iq, 1, gx, gy);
-                    LK[L_INV0_COLOR].add(&iq, gx, gy, b);
-                } else {
-                    const unsigned b = dwt_inv_grid(iq, nch, gx, gy);
-                    LK[l == 0 ? L_INV0_LUMA : L_INV1 - (l - 1)].add(&iq, gx, gy, b);
-                }
+                if (l == 0 && nch == 3) iq.out_u8 = out[k];
+                Launch& li = LK[l == 0 ? (nch == 3 ? L_INV0_COLOR : L_INV0_LUMA) : L_INV1 - (l - 1)];
+                const unsigned b = dwt_inv_grid(iq, l == 0 && nch == 3 ? 1 : nch, gx, gy);
+                li.add(&iq, gx, gy, b);
+                li.any16 |= iq.h16 != 0;
             }
             if (nch == 1) {
                 TransferParams tp{};
@@ -666,12 +662,12 @@ public:
 
         // the stages of one group on one stream
         auto fwd0 = [&](int g, cudaStream_t st) {
-            return go(g, L_FWD0_LUMA, [&] { return launch_dwt_fwd_multi(kSrcRgbU8, 1, (const FwdLevelParams*)P(g, L_FWD0_LUMA), M(g, L_FWD0_LUMA), L[g][L_FWD0_LUMA].total, st); }, "forward DWT") &&
-                   go(g, L_FWD0_COLOR, [&] { return launch_dwt_fwd_multi(kSrcRgbU8, 3, (const FwdLevelParams*)P(g, L_FWD0_COLOR), M(g, L_FWD0_COLOR), L[g][L_FWD0_COLOR].total, st); }, "forward DWT");
+            return go(g, L_FWD0_LUMA, [&] { return launch_dwt_fwd_multi(kSrcRgbU8, 1, (const FwdLevelParams*)P(g, L_FWD0_LUMA), M(g, L_FWD0_LUMA), L[g][L_FWD0_LUMA].total, L[g][L_FWD0_LUMA].any16, st); }, "forward DWT") &&
+                   go(g, L_FWD0_COLOR, [&] { return launch_dwt_fwd_multi(kSrcRgbU8, 3, (const FwdLevelParams*)P(g, L_FWD0_COLOR), M(g, L_FWD0_COLOR), L[g][L_FWD0_COLOR].total, L[g][L_FWD0_COLOR].any16, st); }, "forward DWT");
         };
         auto fwdl = [&](int g, cudaStream_t st) {
             for (int k = L_FWD1; k <= L_FWD3; k++)
-                if (!go(g, k, [&] { return launch_dwt_fwd_multi(kSrcPlanes, 1, (const FwdLevelParams*)P(g, k), M(g, k), L[g][k].total, st); }, "forward DWT"))
+                if (!go(g, k, [&] { return launch_dwt_fwd_multi(kSrcPlanes, 1, (const FwdLevelParams*)P(g, k), M(g, k), L[g][k].total, L[g][k].any16, st); }, "forward DWT"))
                     return false;
             return true;
         };
@@ -697,13 +693,13 @@ public:
         };
         auto invl = [&](int g, cudaStream_t st) {
             for (int k = L_INV3; k <= L_INV1; k++)
-                if (!go(g, k, [&] { return launch_dwt_inv_multi(1, kOutPlanes, (const InvLevelParams*)P(g, k), M(g, k), L[g][k].total, st); }, "inverse DWT"))
+                if (!go(g, k, [&] { return launch_dwt_inv_multi(1, kOutPlanes, (const InvLevelParams*)P(g, k), M(g, k), L[g][k].total, L[g][k].any16, st); }, "inverse DWT"))
                     return false;
             return true;
         };
         auto inv0 = [&](int g, cudaStream_t st) {
-            return go(g, L_INV0_LUMA, [&] { return launch_dwt_inv_multi(1, kOutPlanes, (const InvLevelParams*)P(g, L_INV0_LUMA), M(g, L_INV0_LUMA), L[g][L_INV0_LUMA].total, st); }, "inverse DWT") &&
-                   go(g, L_INV0_COLOR, [&] { return launch_dwt_inv_multi(3, kOutRgb, (const InvLevelParams*)P(g, L_INV0_COLOR), M(g, L_INV0_COLOR), L[g][L_INV0_COLOR].total, st); }, "inverse DWT");
+            return go(g, L_INV0_LUMA, [&] { return launch_dwt_inv_multi(1, kOutPlanes, (const InvLevelParams*)P(g, L_INV0_LUMA), M(g, L_INV0_LUMA), L[g][L_INV0_LUMA].total, L[g][L_INV0_LUMA].any16, st); }, "inverse DWT") &&
+                   go(g, L_INV0_COLOR, [&] { return launch_dwt_inv_multi(3, kOutRgb, (const InvLevelParams*)P(g, L_INV0_COLOR), M(g, L_INV0_COLOR), L[g][L_INV0_COLOR].total, L[g][L_INV0_COLOR].any16, st); }, "inverse DWT");
         };
         auto xfer = [&](int g, cudaStream_t st) {
             return go(g, L_XFER_GUIDED, [&] { return launch_transfer_multi(1, (const TransferParams*)P(g, L_XFER_GUIDED), M(g, L_XFER_GUIDED), L[g][L_XFER_GUIDED].total, st); }, "luma transfer") &&
@@ -764,6 +760,7 @@ public:
                     sig.push_back(l.total);
                     sig.push_back((long long)l.params_off);
                     sig.push_back((long long)l.map_off);
+                    sig.push_back(l.any16);
                 }
             if (sig != t.sig) {
                 drop_graphs(t);

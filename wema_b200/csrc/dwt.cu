@@ -569,34 +569,35 @@ __device__ __forceinline__ void dwt_inv_body(const InvLevelParams& p, int bx, in
 // LPW lines per warp in flight (2, 4 or 8); every variant computes the same
 // coefficients, bit for bit.
 constexpr int LPW_DEF = 4;
-// a launch's FP32 and FP16-plane tasks take the body compiled for each (the
-// branch is uniform over a CTA)
-template <int C, int MODE>
+// Plane type (FP32, or the planes_fp16 variant's FP16): one stream's kernel
+// is compiled for its type (H16, chosen at launch); a batched launch whose
+// tasks are all FP32 takes the FP32-only kernel, one with FP16-plane tasks
+// (ANY16) the kernel holding both bodies, chosen per CTA.  A kernel holding
+// both is allocated registers for both, which slowed the FP32 colour path.
+template <int C, int MODE, bool H16>
 __global__ void __launch_bounds__(DWT_THREADS, 3) k_dwt_fwd(FwdLevelParams p) {
-    if (p.h16) dwt_fwd_body<C, MODE, LPW_DEF, true>(p, blockIdx.x, blockIdx.y, blockIdx.z);
-    else dwt_fwd_body<C, MODE, LPW_DEF, false>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+    dwt_fwd_body<C, MODE, LPW_DEF, H16>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
-template <int C, int MODE, int MINB, int LPW>
+template <int C, int MODE, int MINB, int LPW, bool ANY16>
 __global__ void __launch_bounds__(DWT_THREADS, MINB)
     k_dwt_fwd_multi(const FwdLevelParams* __restrict__ ps, const int* __restrict__ map) {
     const TaskBlock t = task_block(map, blockIdx.x);
     const FwdLevelParams& p = ps[t.task];
-    if (p.h16) dwt_fwd_body<C, MODE, LPW, true>(p, t.x, t.y, t.z);
+    if (ANY16 && p.h16) dwt_fwd_body<C, MODE, LPW, true>(p, t.x, t.y, t.z);
     else dwt_fwd_body<C, MODE, LPW, false>(p, t.x, t.y, t.z);
 }
 // one channel: 4 CTAs per SM (measured in the batched form: 40% faster than the
 // compiler's 82-register choice, which leaves 2); colour: the compiler's choice
-template <int C, int OUT>
+template <int C, int OUT, bool H16>
 __global__ void __launch_bounds__(DWT_THREADS, C == 1 ? 4 : 1) k_dwt_inv(InvLevelParams p) {
-    if (p.h16) dwt_inv_body<C, OUT, LPW_DEF, true>(p, blockIdx.x, blockIdx.y, blockIdx.z);
-    else dwt_inv_body<C, OUT, LPW_DEF, false>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+    dwt_inv_body<C, OUT, LPW_DEF, H16>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
-template <int C, int OUT, int MINB, int LPW>
+template <int C, int OUT, int MINB, int LPW, bool ANY16>
 __global__ void __launch_bounds__(DWT_THREADS, MINB)
     k_dwt_inv_multi(const InvLevelParams* __restrict__ ps, const int* __restrict__ map) {
     const TaskBlock t = task_block(map, blockIdx.x);
     const InvLevelParams& p = ps[t.task];
-    if (p.h16) dwt_inv_body<C, OUT, LPW, true>(p, t.x, t.y, t.z);
+    if (ANY16 && p.h16) dwt_inv_body<C, OUT, LPW, true>(p, t.x, t.y, t.z);
     else dwt_inv_body<C, OUT, LPW, false>(p, t.x, t.y, t.z);
 }
 
@@ -642,11 +643,16 @@ static cudaError_t allow_smem(K k, size_t bytes) {
 
 // kernels above the 48 KB default; call once per device
 cudaError_t dwt_prepare_device() {
-    cudaError_t e = allow_smem(k_dwt_inv<3, kOutRgb>, inv_smem(3));
-    if (e == cudaSuccess) e = allow_smem(k_dwt_fwd<3, kSrcRgbU8>, fwd_smem(3));
-    if (e == cudaSuccess) e = allow_smem(k_dwt_fwd<3, kSrcRgbF32>, fwd_smem(3));
-    if (e == cudaSuccess) e = allow_smem(k_dwt_inv_multi<3, kOutRgb, 1, LPW_DEF>, inv_smem(3));
-    if (e == cudaSuccess) e = allow_smem(k_dwt_fwd_multi<3, kSrcRgbU8, 3, LPW_DEF>, fwd_smem(3));
+    cudaError_t e = allow_smem(k_dwt_inv<3, kOutRgb, false>, inv_smem(3));
+    if (e == cudaSuccess) e = allow_smem(k_dwt_inv<3, kOutRgb, true>, inv_smem(3));
+    if (e == cudaSuccess) e = allow_smem(k_dwt_fwd<3, kSrcRgbU8, false>, fwd_smem(3));
+    if (e == cudaSuccess) e = allow_smem(k_dwt_fwd<3, kSrcRgbU8, true>, fwd_smem(3));
+    if (e == cudaSuccess) e = allow_smem(k_dwt_fwd<3, kSrcRgbF32, false>, fwd_smem(3));
+    if (e == cudaSuccess) e = allow_smem(k_dwt_fwd<3, kSrcRgbF32, true>, fwd_smem(3));
+    if (e == cudaSuccess) e = allow_smem(k_dwt_inv_multi<3, kOutRgb, 1, LPW_DEF, false>, inv_smem(3));
+    if (e == cudaSuccess) e = allow_smem(k_dwt_inv_multi<3, kOutRgb, 1, LPW_DEF, true>, inv_smem(3));
+    if (e == cudaSuccess) e = allow_smem(k_dwt_fwd_multi<3, kSrcRgbU8, 3, LPW_DEF, false>, fwd_smem(3));
+    if (e == cudaSuccess) e = allow_smem(k_dwt_fwd_multi<3, kSrcRgbU8, 3, LPW_DEF, true>, fwd_smem(3));
     return e;
 }
 
@@ -663,10 +669,11 @@ unsigned dwt_inv_grid(const InvLevelParams& p, int channels_z, unsigned& gx, uns
 }
 
 cudaError_t launch_dwt_fwd_multi(int mode, int channels, const FwdLevelParams* d_params,
-                                 const int* d_map, unsigned blocks, cudaStream_t st) {
+                                 const int* d_map, unsigned blocks, bool any16, cudaStream_t st) {
     if (blocks == 0) return cudaSuccess;
     if (mode == kSrcRgbU8 && channels == 3) {
-        k_dwt_fwd_multi<3, kSrcRgbU8, 3, LPW_DEF><<<blocks, DWT_THREADS, fwd_smem(3), st>>>(d_params, d_map);
+        if (any16) k_dwt_fwd_multi<3, kSrcRgbU8, 3, LPW_DEF, true><<<blocks, DWT_THREADS, fwd_smem(3), st>>>(d_params, d_map);
+        else k_dwt_fwd_multi<3, kSrcRgbU8, 3, LPW_DEF, false><<<blocks, DWT_THREADS, fwd_smem(3), st>>>(d_params, d_map);
         return cudaGetLastError();
     }
     if ((mode != kSrcPlanes && mode != kSrcRgbU8) || channels != 1) return cudaErrorInvalidValue;
@@ -674,8 +681,13 @@ cudaError_t launch_dwt_fwd_multi(int mode, int channels, const FwdLevelParams* d
     const size_t sm = fwd_smem(1);
 #define WEMA_FWD_CASE(I, MB, LP)                                                                        \
     case I:                                                                                             \
-        if (mode == kSrcPlanes) k_dwt_fwd_multi<1, kSrcPlanes, MB, LP><<<blocks, DWT_THREADS, sm, st>>>(d_params, d_map); \
-        else k_dwt_fwd_multi<1, kSrcRgbU8, MB, LP><<<blocks, DWT_THREADS, sm, st>>>(d_params, d_map);     \
+        if (mode == kSrcPlanes) {                                                                       \
+            if (any16) k_dwt_fwd_multi<1, kSrcPlanes, MB, LP, true><<<blocks, DWT_THREADS, sm, st>>>(d_params, d_map); \
+            else k_dwt_fwd_multi<1, kSrcPlanes, MB, LP, false><<<blocks, DWT_THREADS, sm, st>>>(d_params, d_map); \
+        } else {                                                                                        \
+            if (any16) k_dwt_fwd_multi<1, kSrcRgbU8, MB, LP, true><<<blocks, DWT_THREADS, sm, st>>>(d_params, d_map); \
+            else k_dwt_fwd_multi<1, kSrcRgbU8, MB, LP, false><<<blocks, DWT_THREADS, sm, st>>>(d_params, d_map); \
+        }                                                                                               \
         break;
     switch (v) {
         WEMA_FWD_CASE(0, 1, 2) WEMA_FWD_CASE(1, 1, 4) WEMA_FWD_CASE(2, 1, 8)
@@ -688,17 +700,21 @@ cudaError_t launch_dwt_fwd_multi(int mode, int channels, const FwdLevelParams* d
 }
 
 cudaError_t launch_dwt_inv_multi(int channels, int out_mode, const InvLevelParams* d_params,
-                                 const int* d_map, unsigned blocks, cudaStream_t st) {
+                                 const int* d_map, unsigned blocks, bool any16, cudaStream_t st) {
     if (blocks == 0) return cudaSuccess;
     if (out_mode == kOutRgb && channels == 3) {
-        k_dwt_inv_multi<3, kOutRgb, 1, LPW_DEF><<<blocks, DWT_THREADS, inv_smem(3), st>>>(d_params, d_map);
+        if (any16) k_dwt_inv_multi<3, kOutRgb, 1, LPW_DEF, true><<<blocks, DWT_THREADS, inv_smem(3), st>>>(d_params, d_map);
+        else k_dwt_inv_multi<3, kOutRgb, 1, LPW_DEF, false><<<blocks, DWT_THREADS, inv_smem(3), st>>>(d_params, d_map);
         return cudaGetLastError();
     }
     if (out_mode != kOutPlanes) return cudaErrorInvalidValue;
     const int v = dwt_variant(dwt_dev_now(), 1);
     const size_t sm = inv_smem(1);
 #define WEMA_INV_CASE(I, MB, LP)                                                                        \
-    case I: k_dwt_inv_multi<1, kOutPlanes, MB, LP><<<blocks, DWT_THREADS, sm, st>>>(d_params, d_map); break;
+    case I:                                                                                             \
+        if (any16) k_dwt_inv_multi<1, kOutPlanes, MB, LP, true><<<blocks, DWT_THREADS, sm, st>>>(d_params, d_map); \
+        else k_dwt_inv_multi<1, kOutPlanes, MB, LP, false><<<blocks, DWT_THREADS, sm, st>>>(d_params, d_map); \
+        break;
     switch (v) {
         WEMA_INV_CASE(0, 1, 2) WEMA_INV_CASE(1, 1, 4) WEMA_INV_CASE(2, 1, 8)
         WEMA_INV_CASE(3, 3, 2) WEMA_INV_CASE(4, 3, 4) WEMA_INV_CASE(5, 3, 8)
@@ -713,13 +729,18 @@ cudaError_t launch_dwt_fwd(int mode, int channels, const FwdLevelParams& p, cuda
     if (channels != 1 && channels != 3) return cudaErrorInvalidValue;
     const unsigned tx = tiles_of(p.sw), ty = tiles_of(p.sh);
     if (mode == kSrcPlanes) {
-        k_dwt_fwd<1, kSrcPlanes><<<dim3(tx, ty, channels), DWT_THREADS, fwd_smem(1), st>>>(p);
+        if (p.h16) k_dwt_fwd<1, kSrcPlanes, true><<<dim3(tx, ty, channels), DWT_THREADS, fwd_smem(1), st>>>(p);
+        else k_dwt_fwd<1, kSrcPlanes, false><<<dim3(tx, ty, channels), DWT_THREADS, fwd_smem(1), st>>>(p);
     } else if (mode == kSrcRgbU8) {
-        if (channels == 3) k_dwt_fwd<3, kSrcRgbU8><<<dim3(tx, ty, 1), DWT_THREADS, fwd_smem(3), st>>>(p);
-        else k_dwt_fwd<1, kSrcRgbU8><<<dim3(tx, ty, 1), DWT_THREADS, fwd_smem(1), st>>>(p);
+        if (channels == 3 && p.h16) k_dwt_fwd<3, kSrcRgbU8, true><<<dim3(tx, ty, 1), DWT_THREADS, fwd_smem(3), st>>>(p);
+        else if (channels == 3) k_dwt_fwd<3, kSrcRgbU8, false><<<dim3(tx, ty, 1), DWT_THREADS, fwd_smem(3), st>>>(p);
+        else if (p.h16) k_dwt_fwd<1, kSrcRgbU8, true><<<dim3(tx, ty, 1), DWT_THREADS, fwd_smem(1), st>>>(p);
+        else k_dwt_fwd<1, kSrcRgbU8, false><<<dim3(tx, ty, 1), DWT_THREADS, fwd_smem(1), st>>>(p);
     } else if (mode == kSrcRgbF32) {
-        if (channels == 3) k_dwt_fwd<3, kSrcRgbF32><<<dim3(tx, ty, 1), DWT_THREADS, fwd_smem(3), st>>>(p);
-        else k_dwt_fwd<1, kSrcRgbF32><<<dim3(tx, ty, 1), DWT_THREADS, fwd_smem(1), st>>>(p);
+        if (channels == 3 && p.h16) k_dwt_fwd<3, kSrcRgbF32, true><<<dim3(tx, ty, 1), DWT_THREADS, fwd_smem(3), st>>>(p);
+        else if (channels == 3) k_dwt_fwd<3, kSrcRgbF32, false><<<dim3(tx, ty, 1), DWT_THREADS, fwd_smem(3), st>>>(p);
+        else if (p.h16) k_dwt_fwd<1, kSrcRgbF32, true><<<dim3(tx, ty, 1), DWT_THREADS, fwd_smem(1), st>>>(p);
+        else k_dwt_fwd<1, kSrcRgbF32, false><<<dim3(tx, ty, 1), DWT_THREADS, fwd_smem(1), st>>>(p);
     } else {
         return cudaErrorInvalidValue;
     }
@@ -729,9 +750,11 @@ cudaError_t launch_dwt_fwd(int mode, int channels, const FwdLevelParams& p, cuda
 cudaError_t launch_dwt_inv(int channels, int out_mode, const InvLevelParams& p, cudaStream_t st) {
     const unsigned tx = tiles_of((p.ow + 1) / 2), ty = tiles_of((p.oh + 1) / 2);
     if (out_mode == kOutPlanes && (channels == 1 || channels == 3))
-        k_dwt_inv<1, kOutPlanes><<<dim3(tx, ty, channels), DWT_THREADS, inv_smem(1), st>>>(p);
+        if (p.h16) k_dwt_inv<1, kOutPlanes, true><<<dim3(tx, ty, channels), DWT_THREADS, inv_smem(1), st>>>(p);
+        else k_dwt_inv<1, kOutPlanes, false><<<dim3(tx, ty, channels), DWT_THREADS, inv_smem(1), st>>>(p);
     else if (out_mode == kOutRgb && channels == 3)
-        k_dwt_inv<3, kOutRgb><<<dim3(tx, ty, 1), DWT_THREADS, inv_smem(3), st>>>(p);
+        if (p.h16) k_dwt_inv<3, kOutRgb, true><<<dim3(tx, ty, 1), DWT_THREADS, inv_smem(3), st>>>(p);
+        else k_dwt_inv<3, kOutRgb, false><<<dim3(tx, ty, 1), DWT_THREADS, inv_smem(3), st>>>(p);
     else
         return cudaErrorInvalidValue;
     return cudaGetLastError();
@@ -825,8 +848,8 @@ cudaError_t dwt_autotune(int dev, float fwd_ms[9], float inv_ms[9], int* fwd_bes
             dwt_set_variant(dev, inv, v);
             for (int rep = 0; rep < 6; rep++) {
                 if (rep == 1 && (e = cudaEventRecord(e0, st)) != cudaSuccess) return done(e);
-                e = inv ? launch_dwt_inv_multi(1, kOutPlanes, (const InvLevelParams*)dpi, map, iblocks, st)
-                        : launch_dwt_fwd_multi(kSrcRgbU8, 1, (const FwdLevelParams*)dp, map, fblocks, st);
+                e = inv ? launch_dwt_inv_multi(1, kOutPlanes, (const InvLevelParams*)dpi, map, iblocks, false, st)
+                        : launch_dwt_fwd_multi(kSrcRgbU8, 1, (const FwdLevelParams*)dp, map, fblocks, false, st);
                 if (e != cudaSuccess) return done(e);
             }
             if ((e = cudaEventRecord(e1, st)) != cudaSuccess) return done(e);

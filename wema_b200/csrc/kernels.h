@@ -155,10 +155,12 @@ cudaError_t launch_window(const WindowParams& wp, const void* ring, float* delta
 // (multi.cuh); `blocks` is the sum of the tasks' grids.
 unsigned dwt_fwd_grid(const FwdLevelParams& p, int channels_z, unsigned& gx, unsigned& gy);
 unsigned dwt_inv_grid(const InvLevelParams& p, int channels_z, unsigned& gx, unsigned& gy);
+// any16: some task has FP16 planes (planes_fp16); false selects the kernel
+// compiled for FP32 planes only
 cudaError_t launch_dwt_fwd_multi(int mode, int channels, const FwdLevelParams* d_params,
-                                 const int* d_map, unsigned blocks, cudaStream_t st);
+                                 const int* d_map, unsigned blocks, bool any16, cudaStream_t st);
 cudaError_t launch_dwt_inv_multi(int channels, int out_mode, const InvLevelParams* d_params,
-                                 const int* d_map, unsigned blocks, cudaStream_t st);
+                                 const int* d_map, unsigned blocks, bool any16, cudaStream_t st);
 size_t thr_args_bytes();
 // grids[stage] = {x, y} for stage 0 partials, 1 prefix, 2 monoids, 3 walk
 cudaError_t thr_args_fill(void* dst, const PyrView* views, int nch, const ThrScratch* scratch,
