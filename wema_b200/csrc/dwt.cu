@@ -587,9 +587,9 @@ __global__ void __launch_bounds__(DWT_THREADS, MINB)
     else dwt_fwd_body<C, MODE, LPW, false>(p, t.x, t.y, t.z);
 }
 // one channel: 4 CTAs per SM (measured in the batched form: 40% faster than the
-// compiler's 82-register choice, which leaves 2); colour: the compiler's choice
+// compiler's 82-register choice, which leaves 2); colour: 3 CTAs per SM
 template <int C, int OUT, bool H16>
-__global__ void __launch_bounds__(DWT_THREADS, C == 1 ? 4 : 1) k_dwt_inv(InvLevelParams p) {
+__global__ void __launch_bounds__(DWT_THREADS, C == 1 ? 4 : 3) k_dwt_inv(InvLevelParams p) {
     dwt_inv_body<C, OUT, LPW_DEF, H16>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <int C, int OUT, int MINB, int LPW, bool ANY16>
@@ -649,8 +649,8 @@ cudaError_t dwt_prepare_device() {
     if (e == cudaSuccess) e = allow_smem(k_dwt_fwd<3, kSrcRgbU8, true>, fwd_smem(3));
     if (e == cudaSuccess) e = allow_smem(k_dwt_fwd<3, kSrcRgbF32, false>, fwd_smem(3));
     if (e == cudaSuccess) e = allow_smem(k_dwt_fwd<3, kSrcRgbF32, true>, fwd_smem(3));
-    if (e == cudaSuccess) e = allow_smem(k_dwt_inv_multi<3, kOutRgb, 1, LPW_DEF, false>, inv_smem(3));
-    if (e == cudaSuccess) e = allow_smem(k_dwt_inv_multi<3, kOutRgb, 1, LPW_DEF, true>, inv_smem(3));
+    if (e == cudaSuccess) e = allow_smem(k_dwt_inv_multi<3, kOutRgb, 3, LPW_DEF, false>, inv_smem(3));
+    if (e == cudaSuccess) e = allow_smem(k_dwt_inv_multi<3, kOutRgb, 3, LPW_DEF, true>, inv_smem(3));
     if (e == cudaSuccess) e = allow_smem(k_dwt_fwd_multi<3, kSrcRgbU8, 3, LPW_DEF, false>, fwd_smem(3));
     if (e == cudaSuccess) e = allow_smem(k_dwt_fwd_multi<3, kSrcRgbU8, 3, LPW_DEF, true>, fwd_smem(3));
     return e;
@@ -703,8 +703,8 @@ cudaError_t launch_dwt_inv_multi(int channels, int out_mode, const InvLevelParam
                                  const int* d_map, unsigned blocks, bool any16, cudaStream_t st) {
     if (blocks == 0) return cudaSuccess;
     if (out_mode == kOutRgb && channels == 3) {
-        if (any16) k_dwt_inv_multi<3, kOutRgb, 1, LPW_DEF, true><<<blocks, DWT_THREADS, inv_smem(3), st>>>(d_params, d_map);
-        else k_dwt_inv_multi<3, kOutRgb, 1, LPW_DEF, false><<<blocks, DWT_THREADS, inv_smem(3), st>>>(d_params, d_map);
+        if (any16) k_dwt_inv_multi<3, kOutRgb, 3, LPW_DEF, true><<<blocks, DWT_THREADS, inv_smem(3), st>>>(d_params, d_map);
+        else k_dwt_inv_multi<3, kOutRgb, 3, LPW_DEF, false><<<blocks, DWT_THREADS, inv_smem(3), st>>>(d_params, d_map);
         return cudaGetLastError();
     }
     if (out_mode != kOutPlanes) return cudaErrorInvalidValue;
