@@ -405,15 +405,20 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
 // C == 1: grid (tiles_x, tiles_y, channels), planes out.
 // C == 3: one CTA per tile does all three channels (YCbCr -> RGB at level 0).
 // H16: FP16 coefficient / delta planes and (p.out16) FP16 output planes,
-// a compile-time constant as in the forward body
-template <int C, int OUT, int LPW, bool H16>
+// a compile-time constant as in the forward body.  FULL: the staged region is
+// a whole 64 x 64 inside the level (every tile but those at the far edges),
+// so its extent is a constant and the bounds tests fold away.
+__device__ __forceinline__ bool inv_full(const InvLevelParams& p, int bx, int by) {
+    return p.ow - seg_start(bx * TP) >= SEG && p.oh - seg_start(by * TP) >= SEG;
+}
+template <int C, int OUT, int LPW, bool H16, bool FULL>
 __device__ __forceinline__ void dwt_inv_body(const InvLevelParams& p, int bx, int by, int bz) {
     extern __shared__ __align__(16) float dyn[];
     float* planes = dyn;   // [C][PLANE]
     const int ow = p.ow, oh = p.oh, sw = p.sw, sh = p.sh;
     const int px0 = bx * TP, py0 = by * TP;
     const int rx0 = seg_start(px0), ry0 = seg_start(py0);
-    const int RW = min(SEG, ow - rx0), RH = min(SEG, oh - ry0);
+    const int RW = FULL ? SEG : min(SEG, ow - rx0), RH = FULL ? SEG : min(SEG, oh - ry0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int c0 = (C == 1) ? bz : 0;
     const int gx0 = rx0 >> 1, gy0 = ry0 >> 1;   // region's first pair
@@ -481,8 +486,8 @@ __device__ __forceinline__ void dwt_inv_body(const InvLevelParams& p, int bx, in
             }
         __syncthreads();
     }
-    const int ty0 = 2 * py0 - ry0, ty1 = min(2 * (py0 + TP), oh) - ry0;
-    const int tx0 = 2 * px0 - rx0, tx1 = min(2 * (px0 + TP), ow) - rx0;
+    const int ty0 = 2 * py0 - ry0, ty1 = FULL ? ty0 + 2 * TP : min(2 * (py0 + TP), oh) - ry0;
+    const int tx0 = 2 * px0 - rx0, tx1 = FULL ? tx0 + 2 * TP : min(2 * (px0 + TP), ow) - rx0;
     if (ow >= 2) {   // rows of the tile
 #pragma unroll
         for (int cc = 0; cc < C; cc++)
@@ -590,15 +595,18 @@ __global__ void __launch_bounds__(DWT_THREADS, MINB)
 // compiler's 82-register choice, which leaves 2); colour: 3 CTAs per SM
 template <int C, int OUT, bool H16>
 __global__ void __launch_bounds__(DWT_THREADS, C == 1 ? 4 : 3) k_dwt_inv(InvLevelParams p) {
-    dwt_inv_body<C, OUT, LPW_DEF, H16>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+    if (!H16 && inv_full(p, blockIdx.x, blockIdx.y))
+        dwt_inv_body<C, OUT, LPW_DEF, false, true>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+    else dwt_inv_body<C, OUT, LPW_DEF, H16, false>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <int C, int OUT, int MINB, int LPW, bool ANY16>
 __global__ void __launch_bounds__(DWT_THREADS, MINB)
     k_dwt_inv_multi(const InvLevelParams* __restrict__ ps, const int* __restrict__ map) {
     const TaskBlock t = task_block(map, blockIdx.x);
     const InvLevelParams& p = ps[t.task];
-    if (ANY16 && p.h16) dwt_inv_body<C, OUT, LPW, true>(p, t.x, t.y, t.z);
-    else dwt_inv_body<C, OUT, LPW, false>(p, t.x, t.y, t.z);
+    if (ANY16 && p.h16) dwt_inv_body<C, OUT, LPW, true, false>(p, t.x, t.y, t.z);
+    else if (inv_full(p, t.x, t.y)) dwt_inv_body<C, OUT, LPW, false, true>(p, t.x, t.y, t.z);
+    else dwt_inv_body<C, OUT, LPW, false, false>(p, t.x, t.y, t.z);
 }
 
 // ---- tuning of the batched luma kernels, per device: variant index
