@@ -203,7 +203,13 @@ __device__ __forceinline__ void prefetch_state_rows(const FwdLevelParams& p, int
 // C == 1: channel blockIdx.z (planes in), or the luma of an RGB frame.
 // H16: the planes_fp16 variant's FP16 coefficient planes (p.h16), a
 // compile-time constant so the FP32 path carries no FP16 selects
-template <int C, int MODE, int LPW, bool H16>
+// FULL: the staged region is a whole 64 x 64 inside the level, as in the
+// inverse (inv_full), so the tile is a whole 27 x 27 pairs with every odd
+// sample present and the bounds tests fold away.
+__device__ __forceinline__ bool fwd_full(const FwdLevelParams& p, int bx, int by) {
+    return p.iw - seg_start(bx * TP) >= SEG && p.ih - seg_start(by * TP) >= SEG;
+}
+template <int C, int MODE, int LPW, bool H16, bool FULL>
 __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, int by, int bz) {
     extern __shared__ __align__(16) float dyn[];
     float* planes = dyn;                                   // [C][PLANE]
@@ -211,7 +217,7 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
     const int iw = p.iw, ih = p.ih, sw = p.sw, sh = p.sh;
     const int px0 = bx * TP, py0 = by * TP;
     const int rx0 = seg_start(px0), ry0 = seg_start(py0);
-    const int RW = min(SEG, iw - rx0), RH = min(SEG, ih - ry0);
+    const int RW = FULL ? SEG : min(SEG, iw - rx0), RH = FULL ? SEG : min(SEG, ih - ry0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
     // the IIR state rows this tile's write-out will update: bulk prefetches
@@ -367,10 +373,10 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
 
     // quadrants: LL (even,even), HL (odd x), LH (odd y), HH; stale entries of
     // odd-sized levels take the previous level's value at the same index
-    const int ni = min(TP, sw - px0), nj = min(TP, sh - py0);
+    const int ni = FULL ? TP : min(TP, sw - px0), nj = FULL ? TP : min(TP, sh - py0);
     const int qx0 = px0 - (rx0 >> 1), qy0 = py0 - (ry0 >> 1);   // tile's first pair in the region
     const int i = px0 + lane;
-    const bool hx = 2 * i + 1 < iw;
+    const bool hx = FULL || 2 * i + 1 < iw;
     const int n = (int)p.n, pn = (int)p.prev_n;
     // every coefficient of the tile lies before the scalar-tail positions of
     // the 6-slot array (all but the last tiles of a frame's last level)
@@ -387,7 +393,7 @@ __device__ __forceinline__ void dwt_fwd_body(const FwdLevelParams& p, int bx, in
             if (lane >= ni) continue;
             const int j = py0 + jj, ry = qy0 + jj;
             const int o = j * sw + i;
-            const bool hy = 2 * j + 1 < ih;
+            const bool hy = FULL || 2 * j + 1 < ih;
             constexpr bool h = H16;
             float v[3];                                                                         // LH, HH, HL
             v[0] = hy ? pl[(32 + ry) * RS] : (prev ? pl_ld(prev, o, h) : 0.0f);
@@ -581,15 +587,18 @@ constexpr int LPW_DEF = 4;
 // both is allocated registers for both, which slowed the FP32 colour path.
 template <int C, int MODE, bool H16>
 __global__ void __launch_bounds__(DWT_THREADS, 3) k_dwt_fwd(FwdLevelParams p) {
-    dwt_fwd_body<C, MODE, LPW_DEF, H16>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+    if (!H16 && fwd_full(p, blockIdx.x, blockIdx.y))
+        dwt_fwd_body<C, MODE, LPW_DEF, false, true>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+    else dwt_fwd_body<C, MODE, LPW_DEF, H16, false>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <int C, int MODE, int MINB, int LPW, bool ANY16>
 __global__ void __launch_bounds__(DWT_THREADS, MINB)
     k_dwt_fwd_multi(const FwdLevelParams* __restrict__ ps, const int* __restrict__ map) {
     const TaskBlock t = task_block(map, blockIdx.x);
     const FwdLevelParams& p = ps[t.task];
-    if (ANY16 && p.h16) dwt_fwd_body<C, MODE, LPW, true>(p, t.x, t.y, t.z);
-    else dwt_fwd_body<C, MODE, LPW, false>(p, t.x, t.y, t.z);
+    if (ANY16 && p.h16) dwt_fwd_body<C, MODE, LPW, true, false>(p, t.x, t.y, t.z);
+    else if (fwd_full(p, t.x, t.y)) dwt_fwd_body<C, MODE, LPW, false, true>(p, t.x, t.y, t.z);
+    else dwt_fwd_body<C, MODE, LPW, false, false>(p, t.x, t.y, t.z);
 }
 // one channel: 4 CTAs per SM (measured in the batched form: 40% faster than the
 // compiler's 82-register choice, which leaves 2); colour: 3 CTAs per SM
