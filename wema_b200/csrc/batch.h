@@ -22,9 +22,11 @@
 // g's threshold beside group g+1's forward transform, its inverse beside group
 // g+1's threshold, its transfer beside group g+1's inverse; threshold and
 // inverse launches at the highest priority, the transfer at the lowest); one
-// group is the default - on the 48-stream mix one graph per tick measured
-// 2.56 ms, two to four groups 2.64-2.69 ms, and the earlier three graphs per
-// tick with the transfer beside the next tick's forward 2.65 ms.  Other ticks
+// group is the default - on the 48-stream mix one group measured 2.19 ms per
+// tick, two to four groups 2.32-2.36 ms (an earlier build: one graph 2.56 ms
+// against three graphs per tick, with the transfer beside the next tick's
+// forward, 2.65 ms).  The level-0 threshold monoids run on a branch of the
+// graph beside the forward levels 1-3.  Other ticks
 // (first frames, stage timing, graphs off) issue the stages in turn over all
 // groups on streams: the luma transfer of tick t on its own lower-priority
 // stream while tick t+1's forward, threshold and IIR run; tick t+1's inverse
