@@ -135,11 +135,21 @@ struct RowLoad {
     float4 g;
     float rgb[12];                      // generic path: decoded RGB
     float gv[4];
+    uint32_t ow[3];                     // FAST: RGB words of row r - 2 GR, the step's output row
     bool any;
 
     __device__ __forceinline__ void issue(const TransferParams& p, int r, int cx) {
         any = r >= 0 && r < p.h && cx + 3 >= 0 && cx < p.w;
         if (FAST) {
+            // the output row's words (loaded as input 2 GR rows earlier, so mostly
+            // cache hits), issued a row ahead of their use like the input
+            const int y = r - 2 * GR;
+            if (y >= 0 && y < p.h && cx >= 0 && cx < p.w) {
+                const uint32_t* q = reinterpret_cast<const uint32_t*>(p.src_u8) + 3 * (((long long)y * p.w + cx) >> 2);
+                ow[0] = __ldg(q);
+                ow[1] = __ldg(q + 1);
+                ow[2] = __ldg(q + 2);
+            }
             if (any) {
                 const long long pi = (long long)r * p.w + cx;
                 const uint32_t* q = reinterpret_cast<const uint32_t*>(p.src_u8) + 3 * (pi >> 2);
@@ -209,13 +219,13 @@ struct RowLoad {
 };
 
 // out = clamp01(RGB + dy) of a lane's 4 output pixels of row y
+// (FAST: w holds the row's 3 RGB words of the lane's 4 pixels, loaded ahead)
 template <bool FAST>
-__device__ __forceinline__ void put_row(const TransferParams& p, int y, int cx, const float dy[4]) {
+__device__ __forceinline__ void put_row(const TransferParams& p, int y, int cx, const float dy[4],
+                                        const uint32_t (&w)[3]) {
     const long long pi0 = (long long)y * p.w + cx;
     if (FAST) {
         if (cx < 0 || cx >= p.w) return;
-        const uint32_t* q = reinterpret_cast<const uint32_t*>(p.src_u8) + 3 * (pi0 >> 2);
-        const uint32_t w[3] = {__ldg(q), __ldg(q + 1), __ldg(q + 2)};
         float v[12];
         uint32_t qb[12];
 #pragma unroll
@@ -392,7 +402,7 @@ __device__ __forceinline__ void guided_sweep(const TransferParams& p, SweepRing&
             const float inv = __fmul_rn(icx[j], icy);
             dy[j] = __fmaf_rn(__fmul_rn(uA[j], inv), Iv[j], __fmul_rn(uB[j], inv));
         }
-        put_row<FAST>(p, y, cx, dy);
+        put_row<FAST>(p, y, cx, dy, in.ow);
     };
 
     // two load buffers in turn, so a row's loads are in flight while the
