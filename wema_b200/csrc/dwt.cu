@@ -591,6 +591,32 @@ __global__ void __launch_bounds__(DWT_THREADS, 3) k_dwt_fwd(FwdLevelParams p) {
         dwt_fwd_body<C, MODE, LPW_DEF, false, true>(p, blockIdx.x, blockIdx.y, blockIdx.z);
     else dwt_fwd_body<C, MODE, LPW_DEF, H16, false>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
+// A batched one-channel CTA works on channel z of its task: the task's
+// parameters copied into registers with that channel's fields at index 0, the
+// body run as channel 0, so every array index in it is a constant (a copy
+// indexed by a run-time channel goes to the stack).  Levels 1-3 forward:
+// spills about 108 -> 60 bytes, 0.2445 -> 0.239 ms per tick; inverse levels
+// 0.119 -> 0.116 and level 0 0.276 -> 0.272 ms; bit-identical.
+__device__ __forceinline__ FwdLevelParams fwd_chan(const FwdLevelParams& g, int z) {
+    FwdLevelParams q = g;
+    q.src_planes[0] = g.src_planes[z];
+    q.coef[0] = g.coef[z];
+    q.prev[0] = g.prev[z];
+    q.ll_out[0] = g.ll_out[z];
+    q.iir_state[0] = g.iir_state[z];
+    q.iir_delta[0] = g.iir_delta[z];
+    return q;
+}
+__device__ __forceinline__ InvLevelParams inv_chan(const InvLevelParams& g, int z) {
+    InvLevelParams q = g;
+    q.ll[0] = g.ll[z];
+    q.coef[0] = g.coef[z];
+    q.delta[0] = g.delta[z];
+    q.thr = g.thr + z;
+    q.alpha[0] = g.alpha[z];
+    q.out_planes[0] = g.out_planes[z];
+    return q;
+}
 template <int C, int MODE, int LPW, bool ANY16>
 __device__ __forceinline__ void dwt_fwd_task(const FwdLevelParams& p, const TaskBlock& t) {
     if (ANY16 && p.h16) dwt_fwd_body<C, MODE, LPW, true, false>(p, t.x, t.y, t.z);
@@ -606,10 +632,12 @@ __global__ void __launch_bounds__(DWT_THREADS, MINB)
         // reference into the table, a field is loaded again after stores that
         // may alias the table as far as the compiler knows; the copy cut the
         // spills (about 120 to 28 bytes) and the level's time (0.646 -> 0.615 ms
-        // per tick on the 48-stream mix).  The other levels and the inverse keep
-        // the reference: there the copy raised the spills or went to the stack.
+        // per tick on the 48-stream mix).
         const FwdLevelParams p = ps[t.task];
         dwt_fwd_task<C, MODE, LPW, ANY16>(p, t);
+    } else if constexpr (C == 1) {
+        const FwdLevelParams p = fwd_chan(ps[t.task], t.z);
+        dwt_fwd_task<C, MODE, LPW, ANY16>(p, TaskBlock{t.task, t.x, t.y, 0});
     } else {
         dwt_fwd_task<C, MODE, LPW, ANY16>(ps[t.task], t);
     }
@@ -626,10 +654,17 @@ template <int C, int OUT, int MINB, int LPW, bool ANY16>
 __global__ void __launch_bounds__(DWT_THREADS, MINB)
     k_dwt_inv_multi(const InvLevelParams* __restrict__ ps, const int* __restrict__ map) {
     const TaskBlock t = task_block(map, blockIdx.x);
-    const InvLevelParams& p = ps[t.task];
-    if (ANY16 && p.h16) dwt_inv_body<C, OUT, LPW, true, false>(p, t.x, t.y, t.z);
-    else if (inv_full(p, t.x, t.y)) dwt_inv_body<C, OUT, LPW, false, true>(p, t.x, t.y, t.z);
-    else dwt_inv_body<C, OUT, LPW, false, false>(p, t.x, t.y, t.z);
+    if constexpr (C == 1) {
+        const InvLevelParams p = inv_chan(ps[t.task], t.z);
+        if (ANY16 && p.h16) dwt_inv_body<C, OUT, LPW, true, false>(p, t.x, t.y, 0);
+        else if (inv_full(p, t.x, t.y)) dwt_inv_body<C, OUT, LPW, false, true>(p, t.x, t.y, 0);
+        else dwt_inv_body<C, OUT, LPW, false, false>(p, t.x, t.y, 0);
+    } else {
+        const InvLevelParams& p = ps[t.task];
+        if (ANY16 && p.h16) dwt_inv_body<C, OUT, LPW, true, false>(p, t.x, t.y, t.z);
+        else if (inv_full(p, t.x, t.y)) dwt_inv_body<C, OUT, LPW, false, true>(p, t.x, t.y, t.z);
+        else dwt_inv_body<C, OUT, LPW, false, false>(p, t.x, t.y, t.z);
+    }
 }
 
 // ---- tuning of the batched luma kernels, per device: variant index
