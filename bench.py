@@ -132,6 +132,12 @@ class ClockSampler:
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+        # the sampler's start-up (NVML initialisation) before the timed region:
+        # wait, at most 3 s, for its first sample
+        t_end = time.time() + 3.0
+        while self.proc and self.proc.poll() is None and time.time() < t_end \
+                and os.path.getsize(self.path) == 0:
+            time.sleep(0.02)
         return self
 
     def __exit__(self, *a):
