@@ -41,3 +41,30 @@ def test_reference_arm_line():
 def test_served_reference_arm_is_unavailable(workload):
     line = run("--impl", "reference", "--workload", workload)
     assert line["impl"] == "reference" and "unavailable" in line
+
+
+def test_clock_sampler_samples_before_the_timed_region(tmp_path, monkeypatch):
+    """The clock sampler's nvidia-smi is started and has written its first
+    sample before the timed region begins; its summary gives the median SM
+    clock, the max clock and the active throttle reasons (a fake nvidia-smi
+    on PATH, no GPU)."""
+    fake = tmp_path / "nvidia-smi"
+    fake.write_text(
+        "#!/bin/sh\n"
+        "sleep 0.3\n"
+        "while true; do\n"
+        "  echo '0, 1965, 1965, 700.0, 0x0000000000000004, Not Active, Not Active, Not Active, Active'\n"
+        "  sleep 0.05\n"
+        "done\n")
+    fake.chmod(0o755)
+    monkeypatch.setenv("PATH", f"{tmp_path}{os.pathsep}{os.environ.get('PATH', '')}")
+    sys.path.insert(0, ROOT)
+    try:
+        import bench
+    finally:
+        sys.path.remove(ROOT)
+    with bench.ClockSampler(0) as c:
+        assert c.proc is not None and os.path.getsize(c.path) > 0   # first sample already in
+    s = c.summary()
+    assert s["sm_mhz"] == 1965.0 and s["sm_max_mhz"] == 1965.0
+    assert s["reasons"] == ["sw_power_cap"] and s["samples"] >= 1
